@@ -1,0 +1,337 @@
+// C ABI entry points (include/alpine_gpu.h).
+#include "context.cuh"
+#include "trace.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+using ag::DeviceBuffer;
+
+namespace {
+
+const char* kNoError = "";
+
+std::string cuda_msg(const char* what, cudaError_t e)
+{
+    return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+std::string status_msg(uint32_t bits)
+{
+    std::string m = "device-side limit:";
+    if (bits & ag::kErrStackOverflow) m += " traversal stack overflow;";
+    if (bits & ag::kErrBadIndex) m += " node/triangle index out of range;";
+    if (bits & ag::kErrIterations) m += " traversal visit cap reached;";
+    if (bits & ag::kErrBuildDepth) m += " BVH build level cap reached;";
+    if (bits & ag::kErrQueueOverflow) m += " wavefront queue overflow;";
+    return m;
+}
+
+// Reads and clears the device status word (stream must be idle).
+int check_status(alpine_gpu_ctx* c)
+{
+    cudaError_t e = cudaMemcpyAsync(c->hStatus, c->dStatus, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("status readback", e));
+    if (*c->hStatus) {
+        uint32_t bits = *c->hStatus;
+        cudaMemsetAsync(c->dStatus, 0, sizeof(uint32_t), c->stream);
+        cudaStreamSynchronize(c->stream);
+        return c->fail(ALPINE_GPU_ERR_LIMIT, status_msg(bits));
+    }
+    return ALPINE_GPU_OK;
+}
+
+int upload_geometry(alpine_gpu_ctx* c)
+{
+    if (!c->geometryDirty) return ALPINE_GPU_OK;
+    size_t vb = c->verts.size() * sizeof(float), ib = c->idx.size() * sizeof(uint32_t);
+    if (!c->dVerts.reserve(vb) || !c->dIdx.reserve(ib))
+        return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "geometry upload: cudaMalloc failed");
+    cudaError_t e = cudaSuccess;
+    if (vb) e = cudaMemcpyAsync(c->dVerts.ptr, c->verts.data(), vb, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && ib) e = cudaMemcpyAsync(c->dIdx.ptr, c->idx.data(), ib, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("geometry upload", e));
+    c->geometryDirty = false;
+    return ALPINE_GPU_OK;
+}
+
+ag::BvhView view(const alpine_gpu_ctx* c)
+{
+    ag::BvhView v;
+    v.nodes = c->dNodes.as<ag::WideNode>();
+    v.tris = c->dTris.as<ag::TriRecord>();
+    v.nodeCount = c->nodeCount;
+    v.triCount = c->triCount;
+    return v;
+}
+
+int require_bvh(alpine_gpu_ctx* c)
+{
+    if (c->bvhDirty) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "geometry changed since the last alpine_gpu_build");
+    return ALPINE_GPU_OK;
+}
+
+bool is_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host-memory query: pinned buffers go through a chunked copy/compute
+// pipeline over several streams; pageable buffers are staged whole.
+template <bool kAny>
+int host_query(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, void* out)
+{
+    if (!c || (n && (!rays || !out))) return c ? c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "null buffer") : -1;
+    if (int rc = require_bvh(c)) return rc;
+    if (n == 0) return ALPINE_GPU_OK;
+    const size_t outSize = kAny ? 1 : sizeof(alpine_gpu_hit);
+    if (!c->dRays.reserve(n * sizeof(alpine_gpu_ray)) || !c->dOut.reserve(n * outSize))
+        return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "ray staging: cudaMalloc failed");
+    ag::BvhView v = view(c);
+    cudaError_t e = cudaSuccess;
+    if (is_pinned(rays) && is_pinned(out)) {
+        const uint64_t kMinChunk = 1ull << 16;
+        uint64_t chunk = (n + 15) / 16;
+        if (chunk < kMinChunk) chunk = kMinChunk;
+        int k = 0;
+        for (uint64_t s = 0; s < n && e == cudaSuccess; s += chunk, ++k) {
+            uint64_t m = n - s < chunk ? n - s : chunk;
+            cudaStream_t st = c->copyStreams[k % ag::kCopyStreams];
+            const char* src = reinterpret_cast<const char*>(rays) + s * sizeof(alpine_gpu_ray);
+            char* dr = c->dRays.as<char>() + s * sizeof(alpine_gpu_ray);
+            char* dout = c->dOut.as<char>() + s * outSize;
+            e = cudaMemcpyAsync(dr, src, m * sizeof(alpine_gpu_ray), cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) break;
+            if (kAny) ag::launch_occluded(v, dr, m, reinterpret_cast<uint8_t*>(dout), c->dStatus, st);
+            else ag::launch_trace(v, dr, m, dout, c->dStatus, st);
+            e = cudaMemcpyAsync(static_cast<char*>(out) + s * outSize, dout, m * outSize, cudaMemcpyDeviceToHost, st);
+        }
+        for (int i = 0; i < ag::kCopyStreams; ++i) {
+            cudaError_t e2 = cudaStreamSynchronize(c->copyStreams[i]);
+            if (e == cudaSuccess) e = e2;
+        }
+    } else {
+        e = cudaMemcpyAsync(c->dRays.ptr, rays, n * sizeof(alpine_gpu_ray), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) {
+            if (kAny) ag::launch_occluded(v, c->dRays.ptr, n, c->dOut.as<uint8_t>(), c->dStatus, c->stream);
+            else ag::launch_trace(v, c->dRays.ptr, n, c->dOut.ptr, c->dStatus, c->stream);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, c->dOut.ptr, n * outSize, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg(kAny ? "occluded" : "trace", e));
+    return check_status(c);
+}
+
+template <bool kAny>
+int device_query(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, void* out, void* stream)
+{
+    if (!c || (n && (!rays || !out))) return c ? c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "null buffer") : -1;
+    if (int rc = require_bvh(c)) return rc;
+    if (n == 0) return ALPINE_GPU_OK;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    ag::BvhView v = view(c);
+    if (kAny) ag::launch_occluded(v, rays, n, static_cast<uint8_t*>(out), c->dStatus, st);
+    else ag::launch_trace(v, rays, n, out, c->dStatus, st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("launch", e));
+    return ALPINE_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alpine_gpu_create(const alpine_gpu_config* cfg, alpine_gpu_ctx** out)
+{
+    if (!cfg || !out) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || cfg->device < 0 || cfg->device >= n) {
+        cudaGetLastError();
+        return ALPINE_GPU_ERR_CUDA;
+    }
+    auto* c = new (std::nothrow) alpine_gpu_ctx;
+    if (!c) return ALPINE_GPU_ERR_OUT_OF_MEMORY;
+    c->cfg = *cfg;
+    c->device = cfg->device;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < ag::kCopyStreams && e == cudaSuccess; ++i)
+        e = cudaStreamCreateWithFlags(&c->copyStreams[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dStatus, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->hStatus, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(c->dStatus, 0, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        alpine_gpu_destroy(c);
+        return ALPINE_GPU_ERR_CUDA;
+    }
+    *out = c;
+    return ALPINE_GPU_OK;
+}
+
+void alpine_gpu_destroy(alpine_gpu_ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& s : c->copyStreams)
+        if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->dStatus) cudaFree(c->dStatus);
+    if (c->hStatus) cudaFreeHost(c->hStatus);
+    delete c;
+}
+
+const char* alpine_gpu_last_error(const alpine_gpu_ctx* c) { return c ? c->error.c_str() : kNoError; }
+
+int alpine_gpu_reset_scene(alpine_gpu_ctx* c)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    c->verts.clear();
+    c->idx.clear();
+    c->shapeVertBase.clear();
+    c->shapeVertCount.clear();
+    c->shapeTriBase.clear();
+    c->shapeTriCount.clear();
+    c->geometryDirty = true;
+    c->bvhDirty = true;
+    c->nodeCount = 0;
+    c->triCount = 0;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_add_mesh(alpine_gpu_ctx* c, const float* vertices, uint32_t vcount, const uint32_t* indices,
+                        uint32_t tcount, uint32_t* shape_id)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if ((vcount && !vertices) || (tcount && !indices))
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_mesh: null array");
+    uint64_t totalTris = c->idx.size() / 3 + (uint64_t)tcount;
+    uint64_t totalVerts = c->verts.size() / 3 + (uint64_t)vcount;
+    if (totalTris >= 0x7fffffffull || totalVerts >= 0x7fffffffull)
+        return c->fail(ALPINE_GPU_ERR_LIMIT, "add_mesh: more than 2^31 - 1 triangles or vertices");
+    for (uint64_t i = 0; i < 3ull * tcount; ++i)
+        if (indices[i] >= vcount) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_mesh: vertex index out of range");
+    uint32_t vbase = (uint32_t)(c->verts.size() / 3);
+    c->shapeVertBase.push_back(vbase);
+    c->shapeVertCount.push_back(vcount);
+    c->shapeTriBase.push_back((uint32_t)(c->idx.size() / 3));
+    c->shapeTriCount.push_back(tcount);
+    c->verts.insert(c->verts.end(), vertices, vertices + 3ull * vcount);
+    c->idx.reserve(c->idx.size() + 3ull * tcount);
+    for (uint64_t i = 0; i < 3ull * tcount; ++i) c->idx.push_back(indices[i] + vbase);
+    c->geometryDirty = true;
+    c->bvhDirty = true;
+    if (shape_id) *shape_id = (uint32_t)(c->shapeVertBase.size() - 1);
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_update_vertices(alpine_gpu_ctx* c, uint32_t shape, const float* vertices)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (shape >= c->shapeVertBase.size() || !vertices)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "update_vertices: bad shape id or null array");
+    std::memcpy(c->verts.data() + 3ull * c->shapeVertBase[shape], vertices,
+                3ull * c->shapeVertCount[shape] * sizeof(float));
+    c->geometryDirty = true;
+    c->bvhDirty = true;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_build(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (int rc = upload_geometry(c)) return rc;
+    uint32_t n = (uint32_t)(c->idx.size() / 3);
+    if (!c->dNodes.reserve((size_t(n) + 1) * sizeof(ag::WideNode)) || !c->dTris.reserve(size_t(n) * sizeof(ag::TriRecord)))
+        return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "build: cudaMalloc failed");
+    ag::BuildStats bs;
+    char err[256] = {0};
+    int rc = c->builder.build(c->dVerts.as<float>(), c->dIdx.as<uint32_t>(), n, c->dNodes.as<ag::WideNode>(),
+                              c->dTris.as<ag::TriRecord>(), c->dStatus, c->stream, &bs, err, sizeof err);
+    if (rc) {
+        c->nodeCount = 0;
+        c->triCount = 0;
+        int code = rc == -2 ? ALPINE_GPU_ERR_CUDA : (rc == -5 ? ALPINE_GPU_ERR_OUT_OF_MEMORY : ALPINE_GPU_ERR_LIMIT);
+        return c->fail(code, err);
+    }
+    c->nodeCount = n ? bs.wideNodes : 0;
+    c->triCount = n;
+    c->bvhDirty = false;
+    c->stats.triangles = n;
+    c->stats.binary_nodes = bs.binaryNodes;
+    c->stats.binary_levels = bs.binaryLevels;
+    c->stats.wide_nodes = bs.wideNodes;
+    c->stats.wide_depth = bs.wideDepth;
+    c->stats.sah_cost = bs.sahCost;
+    c->stats.build_ms = bs.buildMs;
+    if (stats) *stats = c->stats;
+    return check_status(c);
+}
+
+int alpine_gpu_trace(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, alpine_gpu_hit* hits)
+{
+    return host_query<false>(c, rays, n, hits);
+}
+
+int alpine_gpu_occluded(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, uint8_t* occ)
+{
+    return host_query<true>(c, rays, n, occ);
+}
+
+int alpine_gpu_trace_device(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, alpine_gpu_hit* hits,
+                            void* stream)
+{
+    return device_query<false>(c, rays, n, hits, stream);
+}
+
+int alpine_gpu_occluded_device(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, uint8_t* occ,
+                               void* stream)
+{
+    return device_query<true>(c, rays, n, occ, stream);
+}
+
+int alpine_gpu_traversal_stats(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, int any,
+                               uint64_t* nodeVisits, uint64_t* triVisits)
+{
+    if (!c || (n && !rays) || !nodeVisits || !triVisits)
+        return c ? c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "traversal_stats: null argument") : -1;
+    if (int rc = require_bvh(c)) return rc;
+    DeviceBuffer counts;
+    if (!counts.reserve(2 * sizeof(unsigned long long)))
+        return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "traversal_stats: cudaMalloc failed");
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemsetAsync(counts.ptr, 0, sizeof h, c->stream);
+    if (e == cudaSuccess && n) {
+        ag::launch_trace_count(view(c), rays, n, any != 0, counts.as<unsigned long long>(), c->dStatus, c->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, counts.ptr, sizeof h, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("traversal_stats", e));
+    *nodeVisits = h[0];
+    *triVisits = h[1];
+    return check_status(c);
+}
+
+int alpine_gpu_synchronize(alpine_gpu_ctx* c)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("synchronize", e));
+    return check_status(c);
+}
+
+}  // extern "C"

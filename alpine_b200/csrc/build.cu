@@ -1,0 +1,1153 @@
+// GPU BVH builder (see build.cuh).
+//
+// Binary phase: level-synchronous top-down binned SAH over primitive
+// references. Every level processes all active tasks (node ranges) at once:
+//   * big tasks (> kSmallMax references) are binned by blocks of kChunk
+//     references with shared-memory bins merged into per-task global bins,
+//     split by one warp per task, and partitioned stably by chunk;
+//   * small tasks are binned, split and partitioned by one warp each with
+//     warp-private shared-memory bins.
+// Children are compacted in a deterministic order with prefix sums, so a build
+// is a pure function of its input (the float min/max merges and integer counts
+// are order independent).
+//
+// Wide phase: breadth-first greedy collapse to 8 slots (open the internal
+// child of largest surface area, as src/accelerators/wide_bvh.cpp:200-243
+// does), quantised child boxes, octant-ordered slots, triangle records in leaf
+// order (src/accelerators/wide_bvh.cpp:430-472 packs TriangleN likewise).
+#include "build.cuh"
+#include "scan.cuh"
+
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace ag {
+namespace {
+
+constexpr uint32_t kSmallMax = 512;  // tasks up to this size are handled by one warp
+constexpr uint32_t kChunk = 1024;    // references per block for big tasks
+constexpr int kChunkThreads = 256;   // kChunk / 4
+constexpr int kBinWords = 13;        // lo3 hi3 clo3 chi3 count
+constexpr int kAxisBinWords = kSahBins * kBinWords;
+constexpr int kTaskBinWords = 3 * kAxisBinWords;
+constexpr int kSmallWarps = 4;       // warps per block in the small-task kernel
+constexpr uint32_t kMaxLevels = 1024;
+
+struct alignas(16) Task {
+    float clo[3];
+    uint32_t node;
+    float chi[3];
+    uint32_t begin;
+    uint32_t count;
+    uint32_t pad[3];
+};
+
+struct alignas(16) Cand {
+    float lo[3];
+    uint32_t begin;
+    float hi[3];
+    uint32_t count;
+    float clo[3];
+    uint32_t big;    // 1 when count > kSmallMax
+    float chi[3];
+    uint32_t chunks; // ceil(count / kChunk) for big candidates, else 0
+};
+
+struct BigSplit {
+    int axis;
+    int bin;
+    int mode;  // 0 = SAH bin split, 1 = median (all centroids coincide)
+    uint32_t nL;
+};
+
+enum Counter { kCntTasks = 0, kCntBig, kCntChunks, kCntInt, kCntTri, kCntBounds = 8, kCntWords = 32 };
+
+// --------------------------------------------------------------------------
+// Binning arithmetic. Every kernel must compute identical bin indices, so all
+// float operations are explicitly rounded (no contraction into FMA).
+AG_D float centroid(float lo, float hi) { return __fmul_rn(0.5f, __fadd_rn(lo, hi)); }
+AG_D float axis_scale(float clo, float chi)
+{
+    float e = __fsub_rn(chi, clo);
+    return e > 0.0f ? __fdiv_rn(float(kSahBins), e) : 0.0f;
+}
+AG_D int bin_of(float c, float clo, float scale)
+{
+    int b = __float2int_rz(__fmul_rn(__fsub_rn(c, clo), scale));
+    return min(max(b, 0), kSahBins - 1);
+}
+
+AG_D void bin_init_word(uint32_t* w, int k)
+{
+    int f = k % kBinWords;
+    // min words (lo, clo) start at the largest key, max words (hi, chi) at 0.
+    *w = (f < 3 || (f >= 6 && f < 9)) ? 0xffffffffu : 0u;
+}
+
+AG_D float area_of(float lx, float ly, float lz, float hx, float hy, float hz)
+{
+    float ex = hx - lx, ey = hy - ly, ez = hz - lz;
+    return ex * ey + ey * ez + ez * ex;
+}
+
+// Inclusive warp scans for union-of-boxes and counts.
+template <bool kForward>
+AG_D float scan_min(float v)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        float y = kForward ? __shfl_up_sync(0xffffffffu, v, o) : __shfl_down_sync(0xffffffffu, v, o);
+        bool ok = kForward ? (lane_id() >= (uint32_t)o) : (lane_id() + o < 32);
+        if (ok) v = fminf(v, y);
+    }
+    return v;
+}
+template <bool kForward>
+AG_D float scan_max(float v)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        float y = kForward ? __shfl_up_sync(0xffffffffu, v, o) : __shfl_down_sync(0xffffffffu, v, o);
+        bool ok = kForward ? (lane_id() >= (uint32_t)o) : (lane_id() + o < 32);
+        if (ok) v = fmaxf(v, y);
+    }
+    return v;
+}
+template <bool kForward>
+AG_D uint32_t scan_add(uint32_t v)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = kForward ? __shfl_up_sync(0xffffffffu, v, o) : __shfl_down_sync(0xffffffffu, v, o);
+        bool ok = kForward ? (lane_id() >= (uint32_t)o) : (lane_id() + o < 32);
+        if (ok) v += y;
+    }
+    return v;
+}
+
+AG_D float warp_min(float v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+AG_D float warp_max(float v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Result of a warp-wide split search over the bins of one task.
+struct SplitChoice {
+    float cost;
+    int axis;
+    int bin;
+    uint32_t nL;
+    float L[12];  // lo3 hi3 clo3 chi3 of the left child
+    float R[12];
+};
+
+// Evaluate all 31 split planes of one axis from bins held one per lane
+// (lane = bin). `v` holds the lane's bin: lo3 hi3 clo3 chi3 as floats (empty
+// bins: lo = +FLT_MAX, hi = -FLT_MAX) and `cnt`. Updates `best` when a cheaper
+// split is found (ties keep the earlier axis / lower bin).
+AG_D void eval_axis(int axis, const float v[12], uint32_t cnt, bool withCentroids, SplitChoice& best)
+{
+    float Lv[12], Rv[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        Lv[k] = scan_min<true>(v[k]);
+        Lv[3 + k] = scan_max<true>(v[3 + k]);
+        Rv[k] = scan_min<false>(v[k]);
+        Rv[3 + k] = scan_max<false>(v[3 + k]);
+    }
+    if (withCentroids) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            Lv[6 + k] = scan_min<true>(v[6 + k]);
+            Lv[9 + k] = scan_max<true>(v[9 + k]);
+            Rv[6 + k] = scan_min<false>(v[6 + k]);
+            Rv[9 + k] = scan_max<false>(v[9 + k]);
+        }
+    }
+    uint32_t cL = scan_add<true>(cnt);
+    uint32_t cR = scan_add<false>(cnt);
+    // right side of the plane after bin k is bins k+1..31
+    float Rn[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) Rn[k] = __shfl_down_sync(0xffffffffu, Rv[k], 1);
+    uint32_t cRn = __shfl_down_sync(0xffffffffu, cR, 1);
+    bool valid = lane_id() < 31 && cL > 0 && cRn > 0;
+    float cost = FLT_MAX;
+    if (valid) {
+        cost = float(cL) * area_of(Lv[0], Lv[1], Lv[2], Lv[3], Lv[4], Lv[5]) +
+               float(cRn) * area_of(Rn[0], Rn[1], Rn[2], Rn[3], Rn[4], Rn[5]);
+    }
+    // warp argmin (cost, then lowest lane)
+    float bc = cost;
+    int bl = (int)lane_id();
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+        int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+        if (oc < bc || (oc == bc && ol < bl)) { bc = oc; bl = ol; }
+    }
+    if (bc < best.cost) {
+        best.cost = bc;
+        best.axis = axis;
+        best.bin = bl;
+        best.nL = __shfl_sync(0xffffffffu, cL, bl);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            best.L[k] = __shfl_sync(0xffffffffu, Lv[k], bl);
+            best.R[k] = __shfl_sync(0xffffffffu, Rn[k], bl);
+        }
+    }
+}
+
+AG_D void load_bin(const uint32_t* b, float v[12], uint32_t& cnt)
+{
+    cnt = b[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        bool isMin = (k < 3) || (k >= 6 && k < 9);
+        v[k] = cnt ? ord2f(b[k]) : (isMin ? FLT_MAX : -FLT_MAX);
+    }
+}
+
+AG_D void bin_accumulate(uint32_t* bin, float4 lo, float4 hi, float cx, float cy, float cz)
+{
+    atomicMin(bin + 0, f2ord(lo.x));
+    atomicMin(bin + 1, f2ord(lo.y));
+    atomicMin(bin + 2, f2ord(lo.z));
+    atomicMax(bin + 3, f2ord(hi.x));
+    atomicMax(bin + 4, f2ord(hi.y));
+    atomicMax(bin + 5, f2ord(hi.z));
+    atomicMin(bin + 6, f2ord(cx));
+    atomicMin(bin + 7, f2ord(cy));
+    atomicMin(bin + 8, f2ord(cz));
+    atomicMax(bin + 9, f2ord(cx));
+    atomicMax(bin + 10, f2ord(cy));
+    atomicMax(bin + 11, f2ord(cz));
+    atomicAdd(bin + 12, 1u);
+}
+
+AG_D void write_cand(Cand* c, const float* b, uint32_t begin, uint32_t count)
+{
+    Cand o;
+    o.lo[0] = b[0]; o.lo[1] = b[1]; o.lo[2] = b[2];
+    o.hi[0] = b[3]; o.hi[1] = b[4]; o.hi[2] = b[5];
+    o.clo[0] = b[6]; o.clo[1] = b[7]; o.clo[2] = b[8];
+    o.chi[0] = b[9]; o.chi[1] = b[10]; o.chi[2] = b[11];
+    o.begin = begin;
+    o.count = count;
+    o.big = count > kSmallMax ? 1u : 0u;
+    o.chunks = o.big ? (count + kChunk - 1) / kChunk : 0u;
+    *c = o;
+}
+
+// --------------------------------------------------------------------------
+// Preparation: primitive boxes and root bounds.
+__global__ void k_prep_prims(const float* __restrict__ verts, const uint32_t* __restrict__ idx, uint32_t n,
+                             float4* __restrict__ primLo, float4* __restrict__ primHi, uint32_t* __restrict__ refs,
+                             uint32_t* __restrict__ bounds)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float c[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, cmx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    if (i < n) {
+        const uint32_t* t = idx + 3ull * i;
+        float p[3][3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) p[v][k] = verts[3ull * t[v] + k];
+        float l[3], h[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            l[k] = fminf(fminf(p[0][k], p[1][k]), p[2][k]);
+            h[k] = fmaxf(fmaxf(p[0][k], p[1][k]), p[2][k]);
+            lo[k] = l[k];
+            hi[k] = h[k];
+            c[k] = cmx[k] = centroid(l[k], h[k]);
+        }
+        primLo[i] = make_float4(l[0], l[1], l[2], 0.0f);
+        primHi[i] = make_float4(h[0], h[1], h[2], 0.0f);
+        refs[i] = i;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = warp_min(lo[k]);
+        hi[k] = warp_max(hi[k]);
+        c[k] = warp_min(c[k]);
+        cmx[k] = warp_max(cmx[k]);
+    }
+    if (lane_id() == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(bounds + k, f2ord(lo[k]));
+            atomicMax(bounds + 3 + k, f2ord(hi[k]));
+            atomicMin(bounds + 6 + k, f2ord(c[k]));
+            atomicMax(bounds + 9 + k, f2ord(cmx[k]));
+        }
+    }
+}
+
+__global__ void k_init_bounds(uint32_t* bounds)
+{
+    int k = threadIdx.x;
+    if (k < 12) bounds[k] = (k < 3 || (k >= 6 && k < 9)) ? 0xffffffffu : 0u;
+}
+
+__global__ void k_root(uint32_t n, const uint32_t* __restrict__ bounds, Task* tasks, BinNode* bnodes,
+                       uint32_t* bigList, uint32_t* chunkOff, uint32_t* chunkTask, uint32_t nChunks)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        Task t;
+        for (int k = 0; k < 3; ++k) {
+            t.clo[k] = ord2f(bounds[6 + k]);
+            t.chi[k] = ord2f(bounds[9 + k]);
+        }
+        t.node = 0;
+        t.begin = 0;
+        t.count = n;
+        tasks[0] = t;
+        BinNode b;
+        b.lo = mk3(ord2f(bounds[0]), ord2f(bounds[1]), ord2f(bounds[2]));
+        b.hi = mk3(ord2f(bounds[3]), ord2f(bounds[4]), ord2f(bounds[5]));
+        b.begin = 0;
+        b.count = n;
+        b.left = -1;
+        b.right = -1;
+        bnodes[0] = b;
+        bigList[0] = 0;
+        chunkOff[0] = 0;
+    }
+    if (i < nChunks) chunkTask[i] = 0;
+}
+
+// --------------------------------------------------------------------------
+// Big tasks.
+__global__ void k_bins_clear(uint32_t* bins, uint32_t numBig)
+{
+    uint32_t* b = bins + size_t(blockIdx.x) * kTaskBinWords;
+    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(b + k, k);
+}
+
+struct ChunkRange {
+    uint32_t bi, t, begin, end, local;
+};
+
+AG_D ChunkRange chunk_range(uint32_t c, const Task* tasks, const uint32_t* bigList, const uint32_t* chunkOff,
+                            const uint32_t* chunkTask, Task& task)
+{
+    ChunkRange r;
+    r.bi = chunkTask[c];
+    r.t = bigList[r.bi];
+    task = tasks[r.t];
+    r.local = c - chunkOff[r.bi];
+    r.begin = task.begin + r.local * kChunk;
+    r.end = min(task.begin + task.count, r.begin + kChunk);
+    return r;
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_bin_big(const Task* __restrict__ tasks, const uint32_t* __restrict__ refs,
+                                                           const float4* __restrict__ primLo, const float4* __restrict__ primHi,
+                                                           const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
+                                                           const uint32_t* __restrict__ chunkTask, uint32_t* __restrict__ bigBins)
+{
+    __shared__ uint32_t sb[kTaskBinWords];
+    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(sb + k, k);
+    __syncthreads();
+    Task task;
+    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
+    float sc[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) sc[a] = axis_scale(task.clo[a], task.chi[a]);
+    for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) {
+        uint32_t p = refs[i];
+        float4 lo = primLo[p], hi = primHi[p];
+        float cx = centroid(lo.x, hi.x), cy = centroid(lo.y, hi.y), cz = centroid(lo.z, hi.z);
+        float cc[3] = {cx, cy, cz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (sc[a] == 0.0f) continue;
+            int b = bin_of(cc[a], task.clo[a], sc[a]);
+            bin_accumulate(sb + a * kAxisBinWords + b * kBinWords, lo, hi, cx, cy, cz);
+        }
+    }
+    __syncthreads();
+    uint32_t* g = bigBins + size_t(r.bi) * kTaskBinWords;
+    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) {
+        int binBase = k - k % kBinWords;
+        if (sb[binBase + 12] == 0) continue;  // empty bin: nothing to merge
+        int f = k % kBinWords;
+        if (f == 12) atomicAdd(g + k, sb[k]);
+        else if (f < 3 || (f >= 6 && f < 9)) atomicMin(g + k, sb[k]);
+        else atomicMax(g + k, sb[k]);
+    }
+}
+
+__global__ void k_split_big(const Task* __restrict__ tasks, const uint32_t* __restrict__ bigList,
+                            const uint32_t* __restrict__ bigBins, BigSplit* __restrict__ splits,
+                            Cand* __restrict__ cands, uint32_t* __restrict__ candFlag)
+{
+    uint32_t bi = blockIdx.x;
+    uint32_t t = bigList[bi];
+    Task task = tasks[t];
+    SplitChoice best;
+    best.cost = FLT_MAX;
+    best.axis = -1;
+    best.bin = 0;
+    best.nL = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (axis_scale(task.clo[a], task.chi[a]) == 0.0f) continue;
+        float v[12];
+        uint32_t cnt;
+        load_bin(bigBins + size_t(bi) * kTaskBinWords + a * kAxisBinWords + lane_id() * kBinWords, v, cnt);
+        eval_axis(a, v, cnt, true, best);
+    }
+    if (lane_id() == 0) {
+        BigSplit s;
+        if (best.axis >= 0) {
+            s.axis = best.axis;
+            s.bin = best.bin;
+            s.mode = 0;
+            s.nL = best.nL;
+            write_cand(cands + 2 * t, best.L, task.begin, best.nL);
+            write_cand(cands + 2 * t + 1, best.R, task.begin + best.nL, task.count - best.nL);
+        } else {
+            // All centroids coincide: split by position. The children inherit
+            // the parent's node box (a NaN in lo marks this for k_compact) and
+            // its point-sized centroid box.
+            float pb[12];
+            const float nan = __uint_as_float(0x7fc00000u);
+            for (int k = 0; k < 3; ++k) {
+                pb[k] = nan;
+                pb[3 + k] = nan;
+                pb[6 + k] = task.clo[k];
+                pb[9 + k] = task.chi[k];
+            }
+            s.axis = 0;
+            s.bin = 0;
+            s.mode = 1;
+            s.nL = task.count / 2;
+            write_cand(cands + 2 * t, pb, task.begin, s.nL);
+            write_cand(cands + 2 * t + 1, pb, task.begin + s.nL, task.count - s.nL);
+        }
+        splits[bi] = s;
+        candFlag[2 * t] = 1;
+        candFlag[2 * t + 1] = 1;
+    }
+}
+
+AG_D bool goes_left(const BigSplit& s, const Task& task, uint32_t i, uint32_t p, const float4* primLo,
+                    const float4* primHi)
+{
+    if (s.mode == 1) return (i - task.begin) < s.nL;
+    float lo = comp(make_float3(primLo[p].x, primLo[p].y, primLo[p].z), s.axis);
+    float hi = comp(make_float3(primHi[p].x, primHi[p].y, primHi[p].z), s.axis);
+    float c = centroid(lo, hi);
+    return bin_of(c, task.clo[s.axis], axis_scale(task.clo[s.axis], task.chi[s.axis])) <= s.bin;
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_part_count(const Task* __restrict__ tasks, const uint32_t* __restrict__ refs,
+                                                              const float4* __restrict__ primLo, const float4* __restrict__ primHi,
+                                                              const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
+                                                              const uint32_t* __restrict__ chunkTask, const BigSplit* __restrict__ splits,
+                                                              uint32_t* __restrict__ chunkLeft)
+{
+    Task task;
+    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
+    BigSplit s = splits[r.bi];
+    uint32_t c = 0;
+    for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) c += goes_left(s, task, i, refs[i], primLo, primHi);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ uint32_t ws[kChunkThreads / 32];
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s2 = 0;
+        for (int w = 0; w < kChunkThreads / 32; ++w) s2 += ws[w];
+        chunkLeft[blockIdx.x] = s2;
+    }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_part_scatter(const Task* __restrict__ tasks, const uint32_t* __restrict__ refs,
+                                                                uint32_t* __restrict__ refsNext,
+                                                                const float4* __restrict__ primLo, const float4* __restrict__ primHi,
+                                                                const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
+                                                                const uint32_t* __restrict__ chunkTask, const BigSplit* __restrict__ splits,
+                                                                const uint32_t* __restrict__ chunkLeftOff,
+                                                                uint32_t* __restrict__ status)
+{
+    Task task;
+    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
+    BigSplit s = splits[r.bi];
+    uint32_t leftBefore = chunkLeftOff[blockIdx.x] - chunkLeftOff[chunkOff[r.bi]];
+    uint32_t rightBefore = r.local * kChunk - leftBefore;
+    // each thread owns 4 consecutive references: stable order inside the chunk
+    uint32_t base = r.begin + threadIdx.x * 4;
+    uint32_t p[4];
+    bool f[4];
+    uint32_t nl = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint32_t i = base + k;
+        f[k] = false;
+        p[k] = 0;
+        if (i < r.end) {
+            p[k] = refs[i];
+            f[k] = goes_left(s, task, i, p[k], primLo, primHi);
+            nl += f[k];
+        }
+    }
+    uint32_t nvalid = base < r.end ? min(4u, r.end - base) : 0u;
+    // block exclusive scan of (left count, valid count)
+    __shared__ uint32_t wl[kChunkThreads / 32], wv[kChunkThreads / 32];
+    uint32_t il = nl, iv = nvalid;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t yl = __shfl_up_sync(0xffffffffu, il, o);
+        uint32_t yv = __shfl_up_sync(0xffffffffu, iv, o);
+        if (lane_id() >= (uint32_t)o) { il += yl; iv += yv; }
+    }
+    if (lane_id() == 31) { wl[threadIdx.x >> 5] = il; wv[threadIdx.x >> 5] = iv; }
+    __syncthreads();
+    uint32_t pl = 0, pv = 0;
+    for (uint32_t w = 0; w < (threadIdx.x >> 5); ++w) { pl += wl[w]; pv += wv[w]; }
+    uint32_t leftRank = pl + il - nl;
+    uint32_t rightRank = (pv + iv - nvalid) - leftRank;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint32_t i = base + k;
+        if (i >= r.end) break;
+        uint32_t dst = f[k] ? task.begin + leftBefore + leftRank++ : task.begin + s.nL + rightBefore + rightRank++;
+        if (dst >= task.begin + task.count) { atomicOr(status, kErrBadIndex); continue; }
+        refsNext[dst] = p[k];
+    }
+}
+
+// --------------------------------------------------------------------------
+// Small tasks: one warp does bin + split + partition.
+__global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restrict__ tasks, uint32_t numTasks,
+                                                          const uint32_t* __restrict__ refs, uint32_t* __restrict__ refsNext,
+                                                          const float4* __restrict__ primLo, const float4* __restrict__ primHi,
+                                                          const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
+                                                          uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order,
+                                                          uint32_t* __restrict__ status)
+{
+    __shared__ uint32_t sbins[kSmallWarps][kTaskBinWords];
+    uint32_t w = threadIdx.x >> 5;
+    uint32_t t = blockIdx.x * kSmallWarps + w;
+    if (t >= numTasks) return;
+    Task task = tasks[t];
+    if (task.count > kSmallMax) return;  // handled by the big-task kernels
+    uint32_t lane = lane_id();
+    const uint32_t b0 = task.begin, n = task.count;
+
+    auto make_leaf = [&]() {
+        for (uint32_t i = lane; i < n; i += 32) order[b0 + i] = refs[b0 + i];
+        if (lane == 0) { candFlag[2 * t] = 0; candFlag[2 * t + 1] = 0; }
+    };
+    if (n <= 1) { make_leaf(); return; }
+
+    // centroid bounds of this task
+    float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = lane; i < n; i += 32) {
+        uint32_t p = refs[b0 + i];
+        float4 lo = primLo[p], hi = primHi[p];
+        float c[3] = {centroid(lo.x, hi.x), centroid(lo.y, hi.y), centroid(lo.z, hi.z)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { clo[k] = fminf(clo[k], c[k]); chi[k] = fmaxf(chi[k], c[k]); }
+    }
+    float sc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        clo[k] = warp_min(clo[k]);
+        chi[k] = warp_max(chi[k]);
+        sc[k] = axis_scale(clo[k], chi[k]);
+    }
+
+    uint32_t* sb = sbins[w];
+    for (int k = lane; k < kTaskBinWords; k += 32) bin_init_word(sb + k, k);
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) {
+        uint32_t p = refs[b0 + i];
+        float4 lo = primLo[p], hi = primHi[p];
+        float cx = centroid(lo.x, hi.x), cy = centroid(lo.y, hi.y), cz = centroid(lo.z, hi.z);
+        float cc[3] = {cx, cy, cz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (sc[a] == 0.0f) continue;
+            bin_accumulate(sb + a * kAxisBinWords + bin_of(cc[a], clo[a], sc[a]) * kBinWords, lo, hi, cx, cy, cz);
+        }
+    }
+    __syncwarp();
+    SplitChoice best;
+    best.cost = FLT_MAX;
+    best.axis = -1;
+    best.bin = 0;
+    best.nL = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (sc[a] == 0.0f) continue;
+        float v[12];
+        uint32_t cnt;
+        load_bin(sb + a * kAxisBinWords + lane * kBinWords, v, cnt);
+        eval_axis(a, v, cnt, false, best);
+    }
+    const BinNode node = bnodes[task.node];
+    float nodeArea = area_of(node.lo.x, node.lo.y, node.lo.z, node.hi.x, node.hi.y, node.hi.z);
+    // SAH with unit traversal and intersection costs.
+    float leafCost = float(n) * nodeArea;
+    float splitCost = nodeArea + best.cost;
+    if (n <= (uint32_t)kMaxLeafTris && (best.axis < 0 || leafCost <= splitCost)) { make_leaf(); return; }
+
+    uint32_t nL;
+    float Lb[12], Rb[12];
+    bool median = best.axis < 0;
+    if (!median) {
+        nL = best.nL;
+        for (int k = 0; k < 12; ++k) { Lb[k] = best.L[k]; Rb[k] = best.R[k]; }
+    } else {
+        nL = n / 2;
+        // bounds of each half by warp reduction
+        float l0[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+        float l1[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (uint32_t i = lane; i < n; i += 32) {
+            uint32_t p = refs[b0 + i];
+            float4 lo = primLo[p], hi = primHi[p];
+            float* d = i < nL ? l0 : l1;
+            d[0] = fminf(d[0], lo.x); d[1] = fminf(d[1], lo.y); d[2] = fminf(d[2], lo.z);
+            d[3] = fmaxf(d[3], hi.x); d[4] = fmaxf(d[4], hi.y); d[5] = fmaxf(d[5], hi.z);
+        }
+        for (int k = 0; k < 3; ++k) {
+            Lb[k] = warp_min(l0[k]); Lb[3 + k] = warp_max(l0[3 + k]);
+            Rb[k] = warp_min(l1[k]); Rb[3 + k] = warp_max(l1[3 + k]);
+        }
+        for (int k = 0; k < 3; ++k) { Lb[6 + k] = Rb[6 + k] = clo[k]; Lb[9 + k] = Rb[9 + k] = chi[k]; }
+    }
+    // stable partition into refsNext
+    uint32_t leftSeen = 0, rightSeen = 0;
+    for (uint32_t base = 0; base < n; base += 32) {
+        uint32_t i = base + lane;
+        bool valid = i < n;
+        uint32_t p = valid ? refs[b0 + i] : 0;
+        bool left = false;
+        if (valid) {
+            if (median) left = i < nL;
+            else {
+                float4 lo = primLo[p], hi = primHi[p];
+                float c = centroid(comp(make_float3(lo.x, lo.y, lo.z), best.axis), comp(make_float3(hi.x, hi.y, hi.z), best.axis));
+                left = bin_of(c, clo[best.axis], sc[best.axis]) <= best.bin;
+            }
+        }
+        uint32_t bl = __ballot_sync(0xffffffffu, valid && left);
+        uint32_t br = __ballot_sync(0xffffffffu, valid && !left);
+        if (valid) {
+            uint32_t dst = left ? b0 + leftSeen + __popc(bl & lanemask_lt())
+                                : b0 + nL + rightSeen + __popc(br & lanemask_lt());
+            if (dst < b0 + n) refsNext[dst] = p;
+            else atomicOr(status, kErrBadIndex);
+        }
+        leftSeen += __popc(bl);
+        rightSeen += __popc(br);
+    }
+    if (lane == 0) {
+        write_cand(cands + 2 * t, Lb, b0, nL);
+        write_cand(cands + 2 * t + 1, Rb, b0 + nL, n - nL);
+        candFlag[2 * t] = 1;
+        candFlag[2 * t + 1] = 1;
+    }
+}
+
+// --------------------------------------------------------------------------
+// Compaction of the children into the next level's task list.
+__global__ void k_cand_keys(const Cand* __restrict__ cands, const uint32_t* __restrict__ candFlag, uint32_t n,
+                            uint32_t* __restrict__ bigFlag, uint32_t* __restrict__ chunkCnt)
+{
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    bool v = candFlag[j] != 0;
+    bigFlag[j] = v ? cands[j].big : 0u;
+    chunkCnt[j] = v ? cands[j].chunks : 0u;
+}
+
+__global__ void k_compact(const Task* __restrict__ tasks, const Cand* __restrict__ cands,
+                          const uint32_t* __restrict__ candFlag, const uint32_t* __restrict__ candPos,
+                          const uint32_t* __restrict__ bigPos, const uint32_t* __restrict__ chunkOffSparse, uint32_t n,
+                          uint32_t nodeBase, Task* __restrict__ next, BinNode* __restrict__ bnodes,
+                          uint32_t* __restrict__ bigList, uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ chunkTask)
+{
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n || !candFlag[j]) return;
+    Cand c = cands[j];
+    uint32_t p = candPos[j];
+    uint32_t node = nodeBase + p;
+    uint32_t parent = tasks[j >> 1].node;
+    if (j & 1) bnodes[parent].right = (int32_t)node;
+    else bnodes[parent].left = (int32_t)node;
+    BinNode b;
+    if (c.lo[0] != c.lo[0]) {  // median split of coincident centroids: inherit parent box
+        b.lo = bnodes[parent].lo;
+        b.hi = bnodes[parent].hi;
+    } else {
+        b.lo = mk3(c.lo[0], c.lo[1], c.lo[2]);
+        b.hi = mk3(c.hi[0], c.hi[1], c.hi[2]);
+    }
+    b.begin = c.begin;
+    b.count = c.count;
+    b.left = -1;
+    b.right = -1;
+    bnodes[node] = b;
+    Task t;
+    for (int k = 0; k < 3; ++k) { t.clo[k] = c.clo[k]; t.chi[k] = c.chi[k]; }
+    t.node = node;
+    t.begin = c.begin;
+    t.count = c.count;
+    next[p] = t;
+    if (c.big) {
+        uint32_t bi = bigPos[j];
+        bigList[bi] = p;
+        uint32_t off = chunkOffSparse[j];
+        chunkOff[bi] = off;
+        for (uint32_t k = 0; k < c.chunks; ++k) chunkTask[off + k] = bi;
+    }
+}
+
+// --------------------------------------------------------------------------
+// Collapse to the wide layout.
+AG_D float bn_area(const BinNode& b) { return area_of(b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z); }
+
+__global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
+                                  int32_t* __restrict__ slots, uint32_t* __restrict__ intCount,
+                                  uint32_t* __restrict__ triCount)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numItems) return;
+    uint32_t b = items[i].x;
+    int32_t ent[kWidth];
+    int n = 0;
+    const BinNode root = bnodes[b];
+    if (root.count <= (uint32_t)kMaxLeafTris || root.left < 0) {
+        ent[n++] = (int32_t)b;
+    } else {
+        ent[n++] = root.left;
+        ent[n++] = root.right;
+    }
+    // Open children until all 8 slots are used: first those too large for a
+    // leaf slot, then small internal ones (tighter leaf boxes are free since
+    // every slot box is tested anyway).
+    for (int phase = 0; phase < 2; ++phase) {
+        while (n < kWidth) {
+            int pick = -1;
+            float pa = -1.0f;
+            for (int k = 0; k < n; ++k) {
+                const BinNode& c = bnodes[ent[k]];
+                if (c.left < 0) continue;
+                bool large = c.count > (uint32_t)kMaxLeafTris;
+                if (phase == 0 ? !large : large) continue;
+                float a = bn_area(c);
+                if (a > pa) { pa = a; pick = k; }
+            }
+            if (pick < 0) break;
+            const BinNode& c = bnodes[ent[pick]];
+            ent[pick] = c.left;
+            ent[n++] = c.right;
+        }
+    }
+    // Octant slot assignment: slot s prefers the child whose centre lies
+    // toward corner s of the parent box (bit k of s set = + side of axis k).
+    float3 pc = 0.5f * (root.lo + root.hi);
+    float3 cen[kWidth];
+    for (int k = 0; k < n; ++k) {
+        const BinNode& c = bnodes[ent[k]];
+        cen[k] = 0.5f * (c.lo + c.hi) - pc;
+    }
+    int32_t slot[kWidth];
+    for (int s = 0; s < kWidth; ++s) slot[s] = -1;
+    uint32_t usedChild = 0, usedSlot = 0;
+    for (int it = 0; it < n; ++it) {
+        float bestV = -FLT_MAX;
+        int bc = -1, bs = -1;
+        for (int k = 0; k < n; ++k) {
+            if (usedChild & (1u << k)) continue;
+            for (int s = 0; s < kWidth; ++s) {
+                if (usedSlot & (1u << s)) continue;
+                float v = ((s & 1) ? cen[k].x : -cen[k].x) + ((s & 2) ? cen[k].y : -cen[k].y) +
+                          ((s & 4) ? cen[k].z : -cen[k].z);
+                if (v > bestV) { bestV = v; bc = k; bs = s; }
+            }
+        }
+        usedChild |= 1u << bc;
+        usedSlot |= 1u << bs;
+        slot[bs] = ent[bc];
+    }
+    uint32_t ni = 0, nt = 0;
+    for (int s = 0; s < kWidth; ++s) {
+        slots[size_t(i) * kWidth + s] = slot[s];
+        if (slot[s] < 0) continue;
+        uint32_t cnt = bnodes[slot[s]].count;
+        if (cnt <= (uint32_t)kMaxLeafTris) nt += cnt;
+        else ni += 1;
+    }
+    intCount[i] = ni;
+    triCount[i] = nt;
+}
+
+__host__ __device__ inline uint32_t quant_exponent(float extent)
+{
+    // smallest power of two q with 255 * q >= extent (biased exponent byte)
+    if (!(extent > 0.0f)) return 1u;
+    int e;
+    frexpf(extent / 255.0f, &e);
+    float q = ldexpf(1.0f, e);
+    if (255.0f * q < extent * 1.000001f) { e += 1; q *= 2.0f; }
+    int biased = e + 127;
+    biased = biased < 1 ? 1 : (biased > 253 ? 253 : biased);
+    return (uint32_t)biased;
+}
+
+__global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
+                                const int32_t* __restrict__ slots, const uint32_t* __restrict__ intOff,
+                                const uint32_t* __restrict__ triOff, uint32_t wideBase, uint32_t triBase0,
+                                const uint32_t* __restrict__ order, const float* __restrict__ verts,
+                                const uint32_t* __restrict__ idx, WideNode* __restrict__ nodes,
+                                TriRecord* __restrict__ tris, uint2* __restrict__ itemsNext, float* sahAccum,
+                                float rootAreaInv, uint32_t nodeCap, uint32_t triCap, uint32_t* __restrict__ status)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numItems) return;
+    uint2 it = items[i];
+    const BinNode nb = bnodes[it.x];
+    WideNode w;
+    w.px = nb.lo.x;
+    w.py = nb.lo.y;
+    w.pz = nb.lo.z;
+    uint32_t E[3] = {quant_exponent(nb.hi.x - nb.lo.x), quant_exponent(nb.hi.y - nb.lo.y),
+                     quant_exponent(nb.hi.z - nb.lo.z)};
+    float q[3], invq[3];
+    for (int k = 0; k < 3; ++k) {
+        q[k] = __uint_as_float(E[k] << 23);
+        invq[k] = __uint_as_float((254u - E[k]) << 23);  // exact 1/q
+    }
+    float p[3] = {w.px, w.py, w.pz};
+    uint32_t imask = 0;
+    uint32_t childBase = wideBase + intOff[i];
+    uint32_t triBase = triBase0 + triOff[i];
+    uint8_t meta[8], qlo[3][8], qhi[3][8];
+    uint32_t rank = 0, toff = 0;
+    float sah = bn_area(nb) * rootAreaInv;  // one node visit
+    for (int s = 0; s < kWidth; ++s) {
+        int32_t e = slots[size_t(i) * kWidth + s];
+        if (e < 0) {
+            meta[s] = 0;
+            for (int k = 0; k < 3; ++k) { qlo[k][s] = 0xff; qhi[k][s] = 0; }
+            continue;
+        }
+        const BinNode c = bnodes[e];
+        float clo[3] = {c.lo.x, c.lo.y, c.lo.z}, chi[3] = {c.hi.x, c.hi.y, c.hi.z};
+        for (int k = 0; k < 3; ++k) {
+            float fl = floorf((clo[k] - p[k]) * invq[k]);
+            float fh = ceilf((chi[k] - p[k]) * invq[k]);
+            int l = (int)fmaxf(0.0f, fminf(255.0f, fl));
+            int h = (int)fmaxf(0.0f, fminf(255.0f, fh));
+            while (l > 0 && p[k] + float(l) * q[k] > clo[k]) --l;
+            while (h < 255 && p[k] + float(h) * q[k] < chi[k]) ++h;
+            qlo[k][s] = (uint8_t)l;
+            qhi[k][s] = (uint8_t)h;
+        }
+        if (c.count <= (uint32_t)kMaxLeafTris) {
+            meta[s] = (uint8_t)((((1u << c.count) - 1u) << 5) | toff);
+            for (uint32_t k = 0; k < c.count; ++k) {
+                uint32_t prim = order[c.begin + k];
+                const uint32_t* ti = idx + 3ull * prim;
+                float v0[3], v1[3], v2[3];
+                for (int a = 0; a < 3; ++a) {
+                    v0[a] = verts[3ull * ti[0] + a];
+                    v1[a] = verts[3ull * ti[1] + a];
+                    v2[a] = verts[3ull * ti[2] + a];
+                }
+                TriRecord r;
+                r.v0 = make_float4(v0[0], v0[1], v0[2], __uint_as_float(prim));
+                r.e0 = make_float4(__fsub_rn(v1[0], v0[0]), __fsub_rn(v1[1], v0[1]), __fsub_rn(v1[2], v0[2]), 0.0f);
+                r.e1 = make_float4(__fsub_rn(v2[0], v0[0]), __fsub_rn(v2[1], v0[1]), __fsub_rn(v2[2], v0[2]), 0.0f);
+                if (triBase + toff + k < triCap) tris[triBase + toff + k] = r;
+                else atomicOr(status, kErrBadIndex);
+            }
+            toff += c.count;
+            sah += bn_area(c) * rootAreaInv * float(c.count);
+        } else {
+            meta[s] = (uint8_t)(0x20u | (24u + s));
+            imask |= 1u << s;
+            itemsNext[intOff[i] + rank] = make_uint2((uint32_t)e, childBase + rank);
+            ++rank;
+        }
+    }
+    w.e_imask = E[0] | (E[1] << 8) | (E[2] << 16) | (imask << 24);
+    w.childBase = childBase;
+    w.triBase = triBase;
+    w.meta[0] = meta[0] | (meta[1] << 8) | (meta[2] << 16) | ((uint32_t)meta[3] << 24);
+    w.meta[1] = meta[4] | (meta[5] << 8) | (meta[6] << 16) | ((uint32_t)meta[7] << 24);
+    for (int k = 0; k < 3; ++k) {
+        w.qlo[k][0] = qlo[k][0] | (qlo[k][1] << 8) | (qlo[k][2] << 16) | ((uint32_t)qlo[k][3] << 24);
+        w.qlo[k][1] = qlo[k][4] | (qlo[k][5] << 8) | (qlo[k][6] << 16) | ((uint32_t)qlo[k][7] << 24);
+        w.qhi[k][0] = qhi[k][0] | (qhi[k][1] << 8) | (qhi[k][2] << 16) | ((uint32_t)qhi[k][3] << 24);
+        w.qhi[k][1] = qhi[k][4] | (qhi[k][5] << 8) | (qhi[k][6] << 16) | ((uint32_t)qhi[k][7] << 24);
+    }
+    if (it.y < nodeCap) nodes[it.y] = w;
+    else atomicOr(status, kErrBadIndex);
+    atomicAdd(sahAccum, sah);
+}
+
+template <typename T>
+T* carve(char*& p, size_t count)
+{
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    T* r = reinterpret_cast<T*>(p);
+    p += bytes;
+    return r;
+}
+template <typename T>
+size_t carve_bytes(size_t count)
+{
+    return (count * sizeof(T) + 255) & ~size_t(255);
+}
+
+inline unsigned blocks_for(size_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+Builder::~Builder() { release(); }
+
+void Builder::release()
+{
+    if (mem_) cudaFree(mem_);
+    if (hostCounters_) cudaFreeHost(hostCounters_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    mem_ = nullptr;
+    hostCounters_ = nullptr;
+    ev0_ = ev1_ = nullptr;
+    cap_ = 0;
+}
+
+int Builder::reserve(uint32_t n, char* err, size_t errLen)
+{
+    if (n <= cap_ && mem_) return 0;
+    release();
+    size_t N = n ? n : 1;
+    size_t maxBig = N / kSmallMax + 2;
+    size_t maxChunks = N / kChunk + maxBig + 2;
+    size_t bytes = 0;
+    bytes += 2 * carve_bytes<float4>(N);           // primLo, primHi
+    bytes += 3 * carve_bytes<uint32_t>(N);         // refs x2, order
+    bytes += carve_bytes<BinNode>(2 * N);          // bnodes
+    bytes += 2 * carve_bytes<Task>(N);             // tasks x2
+    bytes += carve_bytes<Cand>(2 * N);             // cands
+    bytes += 4 * carve_bytes<uint32_t>(2 * N);     // candFlag, candPos, bigFlag, bigPos
+    bytes += 2 * carve_bytes<uint32_t>(2 * N);     // chunk counts (sparse) + offsets
+    bytes += carve_bytes<uint32_t>(maxBig);        // bigList
+    bytes += carve_bytes<uint32_t>(maxBig);        // chunkOff
+    bytes += 3 * carve_bytes<uint32_t>(maxChunks); // chunkTask, chunkLeft, chunkLeftOff
+    bytes += carve_bytes<uint32_t>(maxBig * kTaskBinWords);
+    bytes += carve_bytes<BigSplit>(maxBig);
+    bytes += 2 * carve_bytes<uint2>(N + 1);        // items x2
+    bytes += carve_bytes<int32_t>((N + 1) * kWidth);
+    bytes += 4 * carve_bytes<uint32_t>(N + 1);     // intCount, intOff, triCount, triOff
+    bytes += carve_bytes<uint32_t>(kCntWords);
+    bytes += carve_bytes<uint32_t>(scan_scratch_words(2 * N + 2));
+    bytes += carve_bytes<float>(1);
+    if (cudaMalloc(&mem_, bytes) != cudaSuccess) {
+        snprintf(err, errLen, "BVH build: cudaMalloc of %zu bytes failed", bytes);
+        mem_ = nullptr;
+        cudaGetLastError();
+        return -5;
+    }
+    memBytes_ = bytes;
+    char* p = static_cast<char*>(mem_);
+    primLo_ = carve<float4>(p, N);
+    primHi_ = carve<float4>(p, N);
+    refs_[0] = carve<uint32_t>(p, N);
+    refs_[1] = carve<uint32_t>(p, N);
+    order_ = carve<uint32_t>(p, N);
+    bnodes_ = carve<BinNode>(p, 2 * N);
+    tasks_[0] = carve<Task>(p, N);
+    tasks_[1] = carve<Task>(p, N);
+    cands_ = carve<Cand>(p, 2 * N);
+    candFlag_ = carve<uint32_t>(p, 2 * N);
+    candPos_ = carve<uint32_t>(p, 2 * N);
+    bigFlag_ = carve<uint32_t>(p, 2 * N);
+    bigPos_ = carve<uint32_t>(p, 2 * N);
+    bigChunks_ = carve<uint32_t>(p, 2 * N);
+    chunkOffSparse_ = carve<uint32_t>(p, 2 * N);
+    bigList_ = carve<uint32_t>(p, maxBig);
+    chunkOff_ = carve<uint32_t>(p, maxBig);
+    chunkTask_ = carve<uint32_t>(p, maxChunks);
+    chunkLeft_ = carve<uint32_t>(p, maxChunks);
+    chunkLeftOff_ = carve<uint32_t>(p, maxChunks);
+    bigBins_ = carve<uint32_t>(p, maxBig * kTaskBinWords);
+    bigSplit_ = carve<BigSplit>(p, maxBig);
+    items_[0] = reinterpret_cast<uint32_t*>(carve<uint2>(p, N + 1));
+    items_[1] = reinterpret_cast<uint32_t*>(carve<uint2>(p, N + 1));
+    slots_ = reinterpret_cast<uint32_t*>(carve<int32_t>(p, (N + 1) * kWidth));
+    intCount_ = carve<uint32_t>(p, N + 1);
+    intOff_ = carve<uint32_t>(p, N + 1);
+    triCount_ = carve<uint32_t>(p, N + 1);
+    triOff_ = carve<uint32_t>(p, N + 1);
+    counters_ = carve<uint32_t>(p, kCntWords);
+    scanScratch_ = carve<uint32_t>(p, scan_scratch_words(2 * N + 2));
+    sahAccum_ = carve<float>(p, 1);
+    if (cudaMallocHost(&hostCounters_, kCntWords * sizeof(uint32_t)) != cudaSuccess) {
+        snprintf(err, errLen, "BVH build: cudaMallocHost failed");
+        cudaGetLastError();
+        release();
+        return -5;
+    }
+    cudaEventCreate(&ev0_);
+    cudaEventCreate(&ev1_);
+    cap_ = n;
+    return 0;
+}
+
+int Builder::build(const float* verts, const uint32_t* idx, uint32_t n, WideNode* nodes, TriRecord* tris,
+                   uint32_t* deviceStatus, cudaStream_t st, BuildStats* stats, char* err, size_t errLen)
+{
+    BuildStats local;
+    if (n == 0) {
+        if (stats) *stats = local;
+        return 0;
+    }
+    if (int rc = reserve(n, err, errLen)) return rc;
+    const size_t N = n;
+    uint32_t* chunkOffSparse = chunkOffSparse_;
+    Task* tasks[2] = {static_cast<Task*>(tasks_[0]), static_cast<Task*>(tasks_[1])};
+    Cand* cands = static_cast<Cand*>(cands_);
+    BigSplit* splits = static_cast<BigSplit*>(bigSplit_);
+    uint32_t* bounds = counters_ + kCntBounds;
+
+    cudaEventRecord(ev0_, st);
+    k_init_bounds<<<1, 32, 0, st>>>(bounds);
+    k_prep_prims<<<blocks_for(N, 256), 256, 0, st>>>(verts, idx, n, primLo_, primHi_, refs_[0], bounds);
+    uint32_t numTasks = 1;
+    uint32_t numBig = n > kSmallMax ? 1u : 0u;
+    uint32_t totalChunks = numBig ? (n + kChunk - 1) / kChunk : 0u;
+    k_root<<<blocks_for(totalChunks + 1, 256), 256, 0, st>>>(n, bounds, tasks[0], bnodes_, bigList_, chunkOff_,
+                                                             chunkTask_, totalChunks);
+    uint32_t nodeCount = 1;
+    int cur = 0;
+    uint32_t level = 0;
+    while (numTasks > 0) {
+        if (++level > kMaxLevels) {
+            snprintf(err, errLen, "BVH build: more than %u levels", kMaxLevels);
+            return -4;
+        }
+        Task* tk = tasks[cur];
+        if (numBig > 0) {
+            k_bins_clear<<<numBig, 256, 0, st>>>(bigBins_, numBig);
+            k_bin_big<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
+                                                             chunkTask_, bigBins_);
+            k_split_big<<<numBig, 32, 0, st>>>(tk, bigList_, bigBins_, splits, cands, candFlag_);
+            k_part_count<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
+                                                                chunkTask_, splits, chunkLeft_);
+            exclusive_scan(chunkLeft_, chunkLeftOff_, totalChunks, nullptr, scanScratch_, st);
+            k_part_scatter<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], refs_[cur ^ 1], primLo_, primHi_,
+                                                                  bigList_, chunkOff_, chunkTask_, splits,
+                                                                  chunkLeftOff_, deviceStatus);
+        }
+        k_small<<<blocks_for(numTasks, kSmallWarps), 32 * kSmallWarps, 0, st>>>(
+            tk, numTasks, refs_[cur], refs_[cur ^ 1], primLo_, primHi_, bnodes_, cands, candFlag_, order_,
+            deviceStatus);
+        const uint32_t nc = 2 * numTasks;
+        k_cand_keys<<<blocks_for(nc, 256), 256, 0, st>>>(cands, candFlag_, nc, bigFlag_, bigChunks_);
+        exclusive_scan(candFlag_, candPos_, nc, counters_ + kCntTasks, scanScratch_, st);
+        exclusive_scan(bigFlag_, bigPos_, nc, counters_ + kCntBig, scanScratch_, st);
+        exclusive_scan(bigChunks_, chunkOffSparse, nc, counters_ + kCntChunks, scanScratch_, st);
+        k_compact<<<blocks_for(nc, 256), 256, 0, st>>>(tk, cands, candFlag_, candPos_, bigPos_, chunkOffSparse, nc,
+                                                       nodeCount, tasks[cur ^ 1], bnodes_, bigList_, chunkOff_,
+                                                       chunkTask_);
+        cudaMemcpyAsync(hostCounters_, counters_, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            snprintf(err, errLen, "BVH build: %s", cudaGetErrorString(cudaGetLastError()));
+            return -2;
+        }
+        numTasks = hostCounters_[kCntTasks];
+        numBig = hostCounters_[kCntBig];
+        totalChunks = hostCounters_[kCntChunks];
+        nodeCount += numTasks;
+        cur ^= 1;
+    }
+    local.binaryNodes = nodeCount;
+    local.binaryLevels = level;
+
+    // Wide collapse.
+    BinNode rb;
+    cudaMemcpyAsync(&rb, bnodes_, sizeof(BinNode), cudaMemcpyDeviceToHost, st);
+    uint2 rootItem = make_uint2(0, 0);
+    cudaMemcpyAsync(items_[0], &rootItem, sizeof(uint2), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(sahAccum_, 0, sizeof(float), st);
+    cudaStreamSynchronize(st);
+    float rootArea = (rb.hi.x - rb.lo.x) * (rb.hi.y - rb.lo.y) + (rb.hi.y - rb.lo.y) * (rb.hi.z - rb.lo.z) +
+                     (rb.hi.z - rb.lo.z) * (rb.hi.x - rb.lo.x);
+    float rootAreaInv = rootArea > 0.0f ? 1.0f / rootArea : 0.0f;
+    uint32_t numItems = 1, wideCount = 1, triCount = 0, depth = 0;
+    int ci = 0;
+    while (numItems > 0) {
+        if (++depth > 64) {
+            snprintf(err, errLen, "BVH collapse: more than 64 wide levels");
+            return -4;
+        }
+        const uint2* items = reinterpret_cast<const uint2*>(items_[ci]);
+        uint2* itemsNext = reinterpret_cast<uint2*>(items_[ci ^ 1]);
+        int32_t* slots = reinterpret_cast<int32_t*>(slots_);
+        k_collapse_decide<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intCount_,
+                                                                      triCount_);
+        exclusive_scan(intCount_, intOff_, numItems, counters_ + kCntInt, scanScratch_, st);
+        exclusive_scan(triCount_, triOff_, numItems, counters_ + kCntTri, scanScratch_, st);
+        k_collapse_emit<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intOff_, triOff_,
+                                                                    wideCount, triCount, order_, verts, idx, nodes,
+                                                                    tris, itemsNext, sahAccum_, rootAreaInv, n + 1, n,
+                                                                    deviceStatus);
+        cudaMemcpyAsync(hostCounters_ + kCntInt, counters_ + kCntInt, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            snprintf(err, errLen, "BVH collapse: %s", cudaGetErrorString(cudaGetLastError()));
+            return -2;
+        }
+        numItems = hostCounters_[kCntInt];
+        wideCount += numItems;
+        triCount += hostCounters_[kCntTri];
+        ci ^= 1;
+    }
+    cudaEventRecord(ev1_, st);
+    float sah = 0.0f;
+    cudaMemcpyAsync(&sah, sahAccum_, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        snprintf(err, errLen, "BVH build: %s", cudaGetErrorString(cudaGetLastError()));
+        return -2;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    local.wideNodes = wideCount;
+    local.wideDepth = depth;
+    local.triCount = triCount;
+    local.sahCost = sah;
+    local.buildMs = ms;
+    if (triCount != n) {
+        snprintf(err, errLen, "BVH build: %u triangles placed, expected %u", triCount, n);
+        return -3;
+    }
+    if (depth > (uint32_t)kTraversalStack) {
+        snprintf(err, errLen, "BVH build: wide depth %u exceeds the traversal stack (%d)", depth, kTraversalStack);
+        return -4;
+    }
+    if (stats) *stats = local;
+    return 0;
+}
+
+}  // namespace ag

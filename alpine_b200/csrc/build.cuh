@@ -1,0 +1,75 @@
+// GPU BVH builder: binned SAH (32 bins) binary build, then a greedy collapse to
+// the 8-wide quantised layout of bvh.cuh. Replaces the reference's CPU build
+// (src/accelerators/bvh_common.cpp:185-391 binned SAH with 9 bins and
+// src/accelerators/wide_bvh.cpp:200-243 collapse + 290-356 flatten).
+#pragma once
+
+#include "bvh.cuh"
+
+namespace ag {
+
+struct BuildStats {
+    uint32_t binaryNodes = 0;
+    uint32_t binaryLevels = 0;
+    uint32_t wideNodes = 0;
+    uint32_t wideDepth = 0;
+    uint32_t triCount = 0;
+    float sahCost = 0.0f;  // SAH cost of the wide tree (node + triangle tests per unit root area)
+    float buildMs = 0.0f;  // device time of the whole build
+};
+
+// Device buffers owned by a builder; grown on demand and reused across builds.
+class Builder {
+public:
+    Builder() = default;
+    ~Builder();
+    Builder(const Builder&) = delete;
+    Builder& operator=(const Builder&) = delete;
+
+    // verts: float[3 * nverts] (device), idx: uint32[3 * ntris] (device).
+    // Outputs: nodes (nodeCapacity >= ntris + 1), tris (ntris records).
+    // Returns 0 on success, a negative code on failure (message in err).
+    int build(const float* verts, const uint32_t* idx, uint32_t ntris, WideNode* nodes, TriRecord* tris,
+              uint32_t* deviceStatus, cudaStream_t stream, BuildStats* stats, char* err, size_t errLen);
+
+private:
+    int reserve(uint32_t ntris, char* err, size_t errLen);
+    void release();
+
+    uint32_t cap_ = 0;
+    void* mem_ = nullptr;  // one allocation carved into the arrays below
+    size_t memBytes_ = 0;
+    float4* primLo_ = nullptr;
+    float4* primHi_ = nullptr;
+    uint32_t* refs_[2] = {nullptr, nullptr};
+    uint32_t* order_ = nullptr;
+    BinNode* bnodes_ = nullptr;
+    void* tasks_[2] = {nullptr, nullptr};
+    void* cands_ = nullptr;
+    uint32_t* candFlag_ = nullptr;
+    uint32_t* candPos_ = nullptr;
+    uint32_t* bigFlag_ = nullptr;
+    uint32_t* bigPos_ = nullptr;
+    uint32_t* bigList_ = nullptr;
+    uint32_t* bigChunks_ = nullptr;
+    uint32_t* chunkOffSparse_ = nullptr;
+    uint32_t* chunkOff_ = nullptr;
+    uint32_t* chunkTask_ = nullptr;
+    uint32_t* chunkLeft_ = nullptr;
+    uint32_t* chunkLeftOff_ = nullptr;
+    uint32_t* bigBins_ = nullptr;
+    void* bigSplit_ = nullptr;
+    uint32_t* items_[2] = {nullptr, nullptr};
+    uint32_t* slots_ = nullptr;
+    uint32_t* intCount_ = nullptr;
+    uint32_t* intOff_ = nullptr;
+    uint32_t* triCount_ = nullptr;
+    uint32_t* triOff_ = nullptr;
+    uint32_t* counters_ = nullptr;  // small device scalars
+    uint32_t* hostCounters_ = nullptr;  // pinned mirror
+    uint32_t* scanScratch_ = nullptr;
+    float* sahAccum_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+};
+
+}  // namespace ag

@@ -1,0 +1,19 @@
+// Launchers for batched ray queries (rays: 32-byte alpine_gpu_ray records).
+#pragma once
+
+#include "bvh.cuh"
+
+namespace ag {
+
+constexpr int kTraceBlock = 128;
+
+// hits: 16-byte {prim, t, b1, b2} records.
+void launch_trace(const BvhView& bvh, const void* rays, uint64_t n, void* hits, uint32_t* status, cudaStream_t st);
+void launch_occluded(const BvhView& bvh, const void* rays, uint64_t n, uint8_t* occ, uint32_t* status,
+                     cudaStream_t st);
+
+// Instrumented traversal: counts[0] += wide nodes fetched, counts[1] += triangles tested.
+void launch_trace_count(const BvhView& bvh, const void* rays, uint64_t n, bool any, unsigned long long* counts,
+                        uint32_t* status, cudaStream_t st);
+
+}  // namespace ag

@@ -1,0 +1,202 @@
+// Wide-BVH traversal (closest hit and any hit) for one ray per thread.
+//
+// Semantics follow the reference's wide traversal
+// (src/accelerators/wide_bvh.cpp:487-619) and its triangle kernel
+// (src/ispc/triangle.ispc:46-87): a hit is accepted when |det| >= 1e-6,
+// t >= tmin (0 in the reference), b1 >= 0, b2 >= 0, b1 + b2 <= 1 and
+// t < current tmax (the reference's `t >= tNear -> reject`). The triangle
+// arithmetic is the reference's, with every product, sum and the reciprocal
+// rounded separately (__fmul_rn / __fadd_rn / __frcp_rn), so t, b1 and b2 are
+// bit-identical to the reference's FP32 values for the same triangle. Child
+// boxes are tested conservatively (quantised boxes are rounded outwards and
+// the exit distance is scaled by 1 + 4e-7 as bounding_box.ispc:29 does).
+//
+// Traversal order: a node group {childBase, hits | imask} holds the pending
+// internal children of one node in bits 24-31 (position = slot ^ octant of
+// the ray direction, so the lowest bit is the nearest octant), and the
+// triangle group {triBase, bits 0-23} the pending triangles. Groups with
+// pending children are pushed to a per-thread stack in shared memory.
+#pragma once
+
+#include "bvh.cuh"
+
+namespace ag {
+
+constexpr float kBoxExitScale = 1.0000004f;
+
+AG_D float dot_rn(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+
+AG_D bool opposite_nonzero(float a, float det)
+{
+    return ((__float_as_uint(a) ^ __float_as_uint(det)) & 0x80000000u) && a != 0.0f;
+}
+
+// Reference ray/triangle test with explicit rounding. Returns true for an
+// accepted hit in [tmin, tmax) and writes t, b1, b2.
+AG_D bool tri_test(float3 o, float3 d, float4 v0, float4 e0, float4 e1, float tmin, float tmax, float& t,
+                   float& b1, float& b2)
+{
+    float sx = __fsub_rn(o.x, v0.x), sy = __fsub_rn(o.y, v0.y), sz = __fsub_rn(o.z, v0.z);
+    float s1x = __fsub_rn(__fmul_rn(d.y, e1.z), __fmul_rn(d.z, e1.y));
+    float s1y = __fsub_rn(__fmul_rn(d.z, e1.x), __fmul_rn(d.x, e1.z));
+    float s1z = __fsub_rn(__fmul_rn(d.x, e1.y), __fmul_rn(d.y, e1.x));
+    float det = dot_rn(s1x, s1y, s1z, e0.x, e0.y, e0.z);
+    if (!(fabsf(det) >= 1e-6f)) return false;
+    float nb1 = dot_rn(s1x, s1y, s1z, sx, sy, sz);
+    // b1 = nb1 * (1/det) >= 0 needs nb1 == 0 or the sign of det (exact).
+    if (opposite_nonzero(nb1, det)) return false;
+    float s2x = __fsub_rn(__fmul_rn(sy, e0.z), __fmul_rn(sz, e0.y));
+    float s2y = __fsub_rn(__fmul_rn(sz, e0.x), __fmul_rn(sx, e0.z));
+    float s2z = __fsub_rn(__fmul_rn(sx, e0.y), __fmul_rn(sy, e0.x));
+    float nb2 = dot_rn(d.x, d.y, d.z, s2x, s2y, s2z);
+    if (opposite_nonzero(nb2, det)) return false;
+    float nt = dot_rn(s2x, s2y, s2z, e1.x, e1.y, e1.z);
+    if (tmin >= 0.0f && opposite_nonzero(nt, det)) return false;
+    float rcp = __frcp_rn(det);
+    float tt = __fmul_rn(nt, rcp);
+    float u = __fmul_rn(nb1, rcp);
+    float v = __fmul_rn(nb2, rcp);
+    if (!(tt >= tmin) || !(tt < tmax)) return false;
+    if (!(u >= 0.0f) || !(v >= 0.0f) || !(__fadd_rn(u, v) <= 1.0f)) return false;
+    t = tt;
+    b1 = u;
+    b2 = v;
+    return true;
+}
+
+struct TraceResult {
+    uint32_t prim;
+    float t, b1, b2;
+};
+
+AG_D float safe_rcp(float d)
+{
+    float a = fabsf(d) < 1e-20f ? copysignf(1e-20f, d) : d;
+    return __frcp_rn(a);
+}
+
+AG_D uint4 ldg4(const void* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
+
+// Intersects the 8 child boxes of a node; returns the hit mask (internal
+// children at bits 24 + (slot ^ oct), triangles at their offsets).
+AG_D uint32_t intersect_children(const uint4& w0, const uint4& w1, const uint4& w2, const uint4& w3, const uint4& w4,
+                                 float3 o, float3 id, uint32_t oct, float tmin, float tmax)
+{
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t e = w0.w;
+    const float sx = __fmul_rn(__uint_as_float((e & 0xffu) << 23), id.x);
+    const float sy = __fmul_rn(__uint_as_float(((e >> 8) & 0xffu) << 23), id.y);
+    const float sz = __fmul_rn(__uint_as_float(((e >> 16) & 0xffu) << 23), id.z);
+    const float ox = __fmul_rn(__fsub_rn(px, o.x), id.x);
+    const float oy = __fmul_rn(__fsub_rn(py, o.y), id.y);
+    const float oz = __fmul_rn(__fsub_rn(pz, o.z), id.z);
+    // near / far planes per axis chosen by the direction sign
+    const bool nx = oct & 1u, ny = oct & 2u, nz = oct & 4u;
+    const uint32_t nearX[2] = {nx ? w3.z : w2.x, nx ? w3.w : w2.y};
+    const uint32_t farX[2] = {nx ? w2.x : w3.z, nx ? w2.y : w3.w};
+    const uint32_t nearY[2] = {ny ? w4.x : w2.z, ny ? w4.y : w2.w};
+    const uint32_t farY[2] = {ny ? w2.z : w4.x, ny ? w2.w : w4.y};
+    const uint32_t nearZ[2] = {nz ? w4.z : w3.x, nz ? w4.w : w3.y};
+    const uint32_t farZ[2] = {nz ? w3.x : w4.z, nz ? w3.y : w4.w};
+    const uint32_t meta[2] = {w1.z, w1.w};
+    uint32_t hits = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int sh = 8 * k;
+            float tnx = fmaf(float((nearX[h] >> sh) & 0xffu), sx, ox);
+            float tny = fmaf(float((nearY[h] >> sh) & 0xffu), sy, oy);
+            float tnz = fmaf(float((nearZ[h] >> sh) & 0xffu), sz, oz);
+            float tfx = fmaf(float((farX[h] >> sh) & 0xffu), sx, ox);
+            float tfy = fmaf(float((farY[h] >> sh) & 0xffu), sy, oy);
+            float tfz = fmaf(float((farZ[h] >> sh) & 0xffu), sz, oz);
+            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            float tf = fminf(fminf(tfx, tfy), tfz) * kBoxExitScale;
+            if (tn <= tf && tn <= tmax) {
+                uint32_t m = (meta[h] >> sh) & 0xffu;
+                uint32_t low = m & 0x1fu;
+                uint32_t pos = low >= 24u ? (low ^ oct) : low;
+                hits |= (m >> 5) << pos;
+            }
+        }
+    }
+    return hits;
+}
+
+// Traces one ray. stack: this thread's first stack entry in shared memory,
+// entries `stride` elements apart. err accumulates DeviceError bits.
+// Returns true when something was hit (closest: result filled; any: first hit).
+// nodeVisits / triVisits count wide nodes fetched and triangles tested (the
+// reference's BvhStats counters, src/accelerators/bvh_common.h:19-61).
+template <bool kAny>
+AG_D bool trace(const BvhView& bvh, float3 o, float3 d, float tmin, float tmax, TraceResult& res, uint2* stack,
+                int stride, uint32_t& err, uint32_t& nodeVisits, uint32_t& triVisits)
+{
+    res.prim = 0xffffffffu;
+    res.t = 3.402823466e38f;
+    res.b1 = 0.0f;
+    res.b2 = 0.0f;
+    if (bvh.nodeCount == 0) return false;
+    const float3 id = mk3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    const uint32_t oct = (id.x < 0.0f ? 1u : 0u) | (id.y < 0.0f ? 2u : 0u) | (id.z < 0.0f ? 4u : 0u);
+    uint2 ngroup = make_uint2(0u, (1u << (24u + oct)) | 1u);  // the root as slot 0 of a virtual parent
+    uint2 tgroup = make_uint2(0u, 0u);
+    int sp = 0;
+    uint32_t visits = 0;
+    bool found = false;
+    for (;;) {
+        // triangles of the current node
+        while (tgroup.y != 0u) {
+            uint32_t k = __ffs(tgroup.y) - 1u;
+            tgroup.y &= tgroup.y - 1u;
+            uint32_t ti = tgroup.x + k;
+            if (ti >= bvh.triCount) { err |= kErrBadIndex; return false; }
+            ++triVisits;
+            const TriRecord* r = bvh.tris + ti;
+            float4 v0 = __ldg(&r->v0), e0 = __ldg(&r->e0), e1 = __ldg(&r->e1);
+            float t, b1, b2;
+            if (tri_test(o, d, v0, e0, e1, tmin, tmax, t, b1, b2)) {
+                if (kAny) {
+                    res.prim = __float_as_uint(v0.w);
+                    res.t = t;
+                    res.b1 = b1;
+                    res.b2 = b2;
+                    return true;
+                }
+                tmax = t;
+                res.prim = __float_as_uint(v0.w);
+                res.t = t;
+                res.b1 = b1;
+                res.b2 = b2;
+                found = true;
+            }
+        }
+        if ((ngroup.y & 0xff000000u) == 0u) {
+            if (sp == 0) break;
+            ngroup = stack[--sp * stride];
+        }
+        uint32_t p = __ffs(ngroup.y >> 24) - 1u;
+        ngroup.y &= ~(1u << (24u + p));
+        uint32_t slot = p ^ oct;
+        uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+        if (ngroup.y & 0xff000000u) {
+            if (sp >= kTraversalStack) { err |= kErrStackOverflow; return false; }
+            stack[sp++ * stride] = ngroup;
+        }
+        if (child >= bvh.nodeCount) { err |= kErrBadIndex; return false; }
+        if (++visits > kMaxVisits) { err |= kErrIterations; return false; }
+        ++nodeVisits;
+        const uint4* np = reinterpret_cast<const uint4*>(bvh.nodes + child);
+        uint4 w0 = ldg4(np), w1 = ldg4(np + 1), w2 = ldg4(np + 2), w3 = ldg4(np + 3), w4 = ldg4(np + 4);
+        uint32_t hits = intersect_children(w0, w1, w2, w3, w4, o, id, oct, tmin, tmax);
+        ngroup = make_uint2(w1.x, (hits & 0xff000000u) | (w0.w >> 24));
+        tgroup = make_uint2(w1.y, hits & 0x00ffffffu);
+    }
+    return found;
+}
+
+}  // namespace ag

@@ -1,0 +1,159 @@
+"""ctypes binding of the C ABI (include/alpine_gpu.h) and a thin Python wrapper.
+
+The CUDA library must have been built (``python -m alpine_b200.build``); there
+is no fallback: importing this module without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+OK = 0
+ERR_INVALID_ARGUMENT = -1
+ERR_CUDA = -2
+ERR_INVALID_STATE = -3
+ERR_LIMIT = -4
+ERR_OUT_OF_MEMORY = -5
+
+RAY_DTYPE = np.dtype([("org", np.float32, 3), ("tmin", np.float32), ("dir", np.float32, 3), ("tmax", np.float32)])
+HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32), ("b1", np.float32), ("b2", np.float32)])
+MISS = 0xFFFFFFFF
+
+
+class GpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"alpine_gpu error {code}: {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("width", C.c_uint32), ("height", C.c_uint32), ("max_depth", C.c_uint32)]
+
+
+class BvhStats(C.Structure):
+    _fields_ = [("triangles", C.c_uint32), ("binary_nodes", C.c_uint32), ("binary_levels", C.c_uint32),
+                ("wide_nodes", C.c_uint32), ("wide_depth", C.c_uint32), ("sah_cost", C.c_float),
+                ("build_ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Loads libalpine_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m alpine_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.alpine_gpu_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+        L.alpine_gpu_destroy.argtypes = [vp]
+        L.alpine_gpu_destroy.restype = None
+        L.alpine_gpu_last_error.argtypes = [vp]
+        L.alpine_gpu_last_error.restype = C.c_char_p
+        L.alpine_gpu_reset_scene.argtypes = [vp]
+        L.alpine_gpu_add_mesh.argtypes = [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.alpine_gpu_update_vertices.argtypes = [vp, C.c_uint32, vp]
+        L.alpine_gpu_build.argtypes = [vp, C.POINTER(BvhStats)]
+        L.alpine_gpu_trace.argtypes = [vp, vp, C.c_uint64, vp]
+        L.alpine_gpu_occluded.argtypes = [vp, vp, C.c_uint64, vp]
+        L.alpine_gpu_trace_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
+        L.alpine_gpu_occluded_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
+        L.alpine_gpu_synchronize.argtypes = [vp]
+        L.alpine_gpu_traversal_stats.argtypes = [vp, vp, C.c_uint64, C.c_int, C.POINTER(C.c_uint64),
+                                                 C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One alpine_gpu context (one device, one stream)."""
+
+    def __init__(self, device=0, width=0, height=0, max_depth=8):
+        self.L = lib()
+        self.h = C.c_void_p()
+        cfg = Config(device, width, height, max_depth)
+        rc = self.L.alpine_gpu_create(C.byref(cfg), C.byref(self.h))
+        if rc != OK:
+            raise GpuError(rc, "alpine_gpu_create failed")
+        self.stats = None
+
+    def _check(self, rc):
+        if rc != OK:
+            raise GpuError(rc, self.L.alpine_gpu_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self.L.alpine_gpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset_scene(self):
+        self._check(self.L.alpine_gpu_reset_scene(self.h))
+
+    def add_mesh(self, verts, idx) -> int:
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+        sid = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_mesh(self.h, _ptr(v), v.shape[0], _ptr(i), i.shape[0], C.byref(sid)))
+        return sid.value
+
+    def update_vertices(self, shape, verts):
+        v = np.ascontiguousarray(verts, np.float32)
+        self._check(self.L.alpine_gpu_update_vertices(self.h, shape, _ptr(v)))
+
+    def build(self) -> dict:
+        s = BvhStats()
+        self._check(self.L.alpine_gpu_build(self.h, C.byref(s)))
+        self.stats = s.as_dict()
+        return self.stats
+
+    def trace(self, rays: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hits = np.empty(r.shape[0], HIT_DTYPE) if out is None else out
+        self._check(self.L.alpine_gpu_trace(self.h, _ptr(r), r.shape[0], _ptr(hits)))
+        return hits
+
+    def occluded(self, rays: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        occ = np.empty(r.shape[0], np.uint8) if out is None else out
+        self._check(self.L.alpine_gpu_occluded(self.h, _ptr(r), r.shape[0], _ptr(occ)))
+        return occ
+
+    def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0):
+        self._check(self.L.alpine_gpu_trace_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),
+                                                   C.c_void_p(stream or None)))
+
+    def occluded_device(self, rays_ptr: int, n: int, occ_ptr: int, stream: int = 0):
+        self._check(self.L.alpine_gpu_occluded_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr),
+                                                      C.c_void_p(stream or None)))
+
+    def traversal_stats(self, rays_ptr: int, n: int, any_hit: bool):
+        """(wide nodes fetched, triangles tested) summed over n device rays."""
+        nv, tv = C.c_uint64(), C.c_uint64()
+        self._check(self.L.alpine_gpu_traversal_stats(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(nv),
+                                                      C.byref(tv)))
+        return nv.value, tv.value
+
+    def synchronize(self):
+        self._check(self.L.alpine_gpu_synchronize(self.h))

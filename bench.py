@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Traversal microbenchmark: closest-hit + any-hit rays/s on a 1M-triangle soup.
+
+Workload (one step): a 1,048,576-triangle soup in the unit cube (centroids
+uniform, edge lengths log-normal(ln 0.004, 0.5), uniform orientations), BVH
+built once on the GPU (binned SAH, 32 bins, 8-wide); 4,194,304 closest-hit
+rays (2,097,152 primary rays of a 2048x1024 pinhole camera at (0.5,0.5,-1),
+60 deg FOV + 2,097,152 incoherent rays: origins uniform in the cube,
+directions uniform on the sphere) and the same 4,194,304 rays as any-hit
+shadow rays with tmax uniform in (0, 1]. A step traces all 8,388,608 queries.
+
+`value` is device throughput with rays resident in HBM; `e2e` goes through
+the C ABI with pinned host buffers (host->device copy of the rays and
+device->host copy of the results inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: one process per GPU under torchrun; each rank is an independent
+replica of the workload (weak scaling), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "traversal Mrays/s (closest+any hit) vs CPU host"
+UNIT = "Mrays/s"
+WORKLOAD = "traversal microbenchmark: 1,048,576-tri soup, 4,194,304 closest + 4,194,304 any-hit rays"
+NODE_BYTES = 80
+TRI_BYTES = 48
+RAY_BYTES = 32
+HIT_BYTES = 16
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per closest-hit launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "trace_closest_soup1M.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_full_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML every 100 ms."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+        0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._nv = pynvml
+        except Exception:
+            self._h = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self._nv.nvmlDeviceGetClockInfo(self._h, self._nv.NVML_CLOCK_SM))
+                self.reasons |= self._nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        names = [n for b, n in self.REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+def cpu_baseline(verts, idx, closest, shadow, budget_s):
+    """The reference's own WideBvh (oracle/_ref: src/accelerators/wide_bvh.cpp
+    with the ISPC kernels restated in C++) on all host cores, on a bounded
+    sample of the same rays (interleaved closest / any-hit chunks)."""
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    ncores = os.cpu_count() or 1
+    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx)
+    rng = np.random.default_rng(7)
+    order = rng.permutation(closest.shape[0])
+    chunk = 16384
+    done, t_total, k = 0, 0.0, 0
+    while t_total < budget_s and (k + 1) * chunk <= order.size:
+        sel = np.sort(order[k * chunk:(k + 1) * chunk])
+        rc, rs = closest[sel], shadow[sel]
+        t0 = time.perf_counter()
+        acc.intersect(rc, nthreads=ncores)
+        acc.occluded(rs, nthreads=ncores)
+        t_total += time.perf_counter() - t0
+        done += 2 * chunk
+        k += 1
+    return {"value": done / t_total / 1e6, "unit": UNIT, "cores": ncores, "kind": "reference",
+            "sample": f"{done // 2} random rays of the workload (primary+incoherent mix), closest + any hit each; "
+                      f"reference WideBvh build {acc.build_ms:.0f} ms (not in the rate)",
+            "seconds": t_total}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU WideBvh on the host cores, same
+    metric; each step is a 131,072-query sample of the workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from alpine_b200 import scenes
+    import oracle
+
+    verts, idx, closest, shadow = scenes.traversal_workload()
+    ncores = os.cpu_count() or 1
+    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx)
+    rng = np.random.default_rng(11)
+    per = 65536
+    times = []
+    for s in range(args.warmup + args.steps):
+        sel = np.sort(rng.choice(closest.shape[0], per, replace=False))
+        rc, rs = closest[sel], shadow[sel]
+        t0 = time.perf_counter()
+        acc.intersect(rc, nthreads=ncores)
+        acc.occluded(rs, nthreads=ncores)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    ms = 1e3 * sum(times) / len(times)
+    value = 2 * per / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_per_step": f"{per} closest + {per} any-hit queries",
+                   "accelerator": "reference WideBvh (8-wide, ISPC kernels restated in C++), CPU"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "reference",
+                         "sample": f"{per} closest + {per} any-hit random rays of the workload per step",
+                         "build_ms": acc.build_ms},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    from alpine_b200 import gpu, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    verts, idx, closest, shadow = scenes.traversal_workload()
+    n = closest.shape[0]
+    ctx = gpu.Context(local)
+    ctx.add_mesh(verts, idx)
+    stats = ctx.build()
+    build_times = []
+    for _ in range(3):  # rebuild timings (device time of the whole build)
+        build_times.append(ctx.build()["build_ms"])
+
+    d_closest = torch.from_numpy(closest).cuda()
+    d_shadow = torch.from_numpy(shadow).cuda()
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    d_occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    nv_c, tv_c = ctx.traversal_stats(d_closest.data_ptr(), n, False)
+    nv_s, tv_s = ctx.traversal_stats(d_shadow.data_ptr(), n, True)
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        ctx.trace_device(d_closest.data_ptr(), n, d_hits.data_ptr(), sp)
+        if ev is not None:
+            ev[1].record(stream)
+        ctx.occluded_device(d_shadow.data_ptr(), n, d_occ.data_ptr(), sp)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        end.record(stream)
+        torch.cuda.synchronize()
+    ctx.synchronize()
+    barrier()
+    total_ms = start.elapsed_time(end)
+    ms_step = max_over_ranks(total_ms / args.steps)
+    closest_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    any_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    value = world * 2 * n / (ms_step / 1e3) / 1e6
+
+    # end to end through the C ABI with pinned host buffers
+    h_closest = torch.from_numpy(closest).pin_memory().numpy()
+    h_shadow = torch.from_numpy(shadow).pin_memory().numpy()
+    h_hits = torch.empty(n * 16, dtype=torch.uint8).pin_memory().numpy().view(gpu.HIT_DTYPE)
+    h_occ = torch.empty(n, dtype=torch.uint8).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        ctx.trace(h_closest, h_hits)
+        ctx.occluded(h_shadow, h_occ)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.trace(h_closest, h_hits)
+        ctx.occluded(h_shadow, h_occ)
+    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - t0) / args.steps)
+    barrier()
+    e2e_value = world * 2 * n / (e2e_ms / 1e3) / 1e6
+
+    peak, peak_kind = peaks()
+    bytes_closest = n * (RAY_BYTES + HIT_BYTES) + nv_c * NODE_BYTES + tv_c * TRI_BYTES
+    bytes_any = n * (RAY_BYTES + 1) + nv_s * NODE_BYTES + tv_s * TRI_BYTES
+    achieved = bytes_closest / (closest_ms / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm", "kernel": "k_trace<closest>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_from_profile(),
+        "algorithmic_bytes_per_launch": bytes_closest,
+        "per_ray": {"node_visits": nv_c / n, "tri_tests": tv_c / n, "bytes": bytes_closest / n},
+        "any_hit": {"ms": any_ms, "achieved_gbs": bytes_any / (any_ms / 1e3) / 1e9,
+                    "node_visits": nv_s / n, "tri_tests": tv_s / n},
+        "closest_ms": closest_ms,
+    }
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": WORKLOAD, "triangles": int(idx.shape[0]), "rays_per_step": 2 * n,
+                "bvh": "GPU binned SAH (32 bins) -> 8-wide quantised BVH",
+                "build_ms": stats["build_ms"], "rebuild_ms": build_times, "wide_nodes": stats["wide_nodes"],
+                "wide_depth": stats["wide_depth"], "sah_cost": stats["sah_cost"],
+                "l2": "inputs larger than L2 (rays 2 x 128 MiB + hits 64 MiB per step); BVH resident",
+                "parallelism": f"replicas x{world}",
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * RAY_BYTES,
+                    "d2h_bytes_per_step": n * (HIT_BYTES + 1), "ms_per_step": e2e_ms},
+            "roofline": roofline,
+            "cpu_baseline": base,
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

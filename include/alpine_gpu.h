@@ -1,0 +1,143 @@
+/*
+ * alpine_gpu.h -- C ABI of the B200 (sm_100a) backend of alpine.
+ *
+ * Plain C types only: pointers, sizes and int status codes; no exceptions or
+ * C++/torch types cross this boundary. One context owns one CUDA stream and
+ * all device memory it allocates; calls on one context are not re-entrant
+ * (use one context per host thread). Host arrays are caller-owned and copied.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the
+ * alpine source tree).
+ */
+#ifndef ALPINE_GPU_H
+#define ALPINE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALPINE_GPU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define ALPINE_GPU_API __attribute__((visibility("default")))
+#else
+#define ALPINE_GPU_API
+#endif
+
+/* Status codes. Every entry point returns one of these (0 on success); the
+ * message of the last failure is available from alpine_gpu_last_error(). */
+typedef enum alpine_gpu_status {
+    ALPINE_GPU_OK = 0,
+    ALPINE_GPU_ERR_INVALID_ARGUMENT = -1,
+    ALPINE_GPU_ERR_CUDA = -2,
+    ALPINE_GPU_ERR_INVALID_STATE = -3,
+    ALPINE_GPU_ERR_LIMIT = -4,         /* a device-side limit was exceeded (stack, visits, queue) */
+    ALPINE_GPU_ERR_OUT_OF_MEMORY = -5
+} alpine_gpu_status;
+
+typedef struct alpine_gpu_ctx alpine_gpu_ctx;
+
+typedef struct alpine_gpu_config {
+    int device;          /* CUDA device ordinal */
+    uint32_t width;      /* framebuffer size for rendering; 0 for a trace-only context */
+    uint32_t height;
+    uint32_t max_depth;  /* path length limit, as alpine::initialize's maxDepth */
+} alpine_gpu_config;
+
+/* One ray: 32 bytes. The reference's Ray (src/ray.h:6-10) plus the parametric
+ * range: hits are accepted for t in [tmin, tmax). Reference semantics are
+ * tmin = 0 and tmax = FLT_MAX (closest hit) or tmax = tFar (any hit). */
+typedef struct alpine_gpu_ray {
+    float org[3];
+    float tmin;
+    float dir[3];
+    float tmax;
+} alpine_gpu_ray;
+
+/* Closest hit: 16 bytes. prim is the global triangle index (triangles are
+ * numbered across meshes in the order they were added); 0xffffffff and
+ * t = FLT_MAX on a miss. b1, b2 are the barycentrics of the second and third
+ * vertex (the reference's Intersection::barycentric, src/intersection.h:8-16). */
+typedef struct alpine_gpu_hit {
+    uint32_t prim;
+    float t;
+    float b1;
+    float b2;
+} alpine_gpu_hit;
+
+typedef struct alpine_gpu_bvh_stats {
+    uint32_t triangles;
+    uint32_t binary_nodes;
+    uint32_t binary_levels;
+    uint32_t wide_nodes;
+    uint32_t wide_depth;
+    float sah_cost;      /* SAH cost of the wide tree, relative to the root area */
+    float build_ms;      /* device time of the last build */
+} alpine_gpu_bvh_stats;
+
+/* Creates a context on cfg->device (replaces alpine::initialize,
+ * include/alpine/alpine.h:10-14, for the GPU backend). */
+ALPINE_GPU_API int alpine_gpu_create(const alpine_gpu_config* cfg, alpine_gpu_ctx** out);
+
+/* Releases every resource of the context (alpine::shutdown, alpine.h:16). */
+ALPINE_GPU_API void alpine_gpu_destroy(alpine_gpu_ctx* ctx);
+
+/* Message of the last failed call on this context ("" if none). */
+ALPINE_GPU_API const char* alpine_gpu_last_error(const alpine_gpu_ctx* ctx);
+
+/* Removes all meshes, lights and the acceleration structure
+ * (alpine::resetScene, alpine.h:23; Scene::reset, src/scenes/scene.h:21-26). */
+ALPINE_GPU_API int alpine_gpu_reset_scene(alpine_gpu_ctx* ctx);
+
+/* Appends one triangle mesh (Accelerator::appendMesh,
+ * src/accelerators/accelerator.h:19-22): vertices float[3 * vertex_count],
+ * indices uint32[3 * triangle_count] (local to this mesh). Writes the shape id
+ * (0, 1, ... in call order). */
+ALPINE_GPU_API int alpine_gpu_add_mesh(alpine_gpu_ctx* ctx, const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+                        uint32_t triangle_count, uint32_t* shape_id);
+
+/* Replaces the vertex positions of one mesh (Accelerator::getVertexBuffer +
+ * updateShape, accelerator.h:27-29). Takes effect at the next build. */
+ALPINE_GPU_API int alpine_gpu_update_vertices(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* vertices);
+
+/* Full (re)build of the BVH on the GPU: binned SAH with 32 bins, collapsed to
+ * an 8-wide quantised BVH (Accelerator::updateScene, accelerator.h:31;
+ * src/accelerators/wide_bvh.cpp:175-197). stats may be NULL. */
+ALPINE_GPU_API int alpine_gpu_build(alpine_gpu_ctx* ctx, alpine_gpu_bvh_stats* stats);
+
+/* Closest hit for `count` rays in HOST memory (Accelerator::intersect,
+ * accelerator.h:33, batched). Pinned buffers are copied in chunks overlapped
+ * with the traversal; pageable buffers are staged. Blocks until done. */
+ALPINE_GPU_API int alpine_gpu_trace(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, alpine_gpu_hit* hits);
+
+/* Any hit in [tmin, tmax) for rays in HOST memory (Accelerator::intersectAny,
+ * accelerator.h:35, batched): occluded[i] = 1 when something is hit. */
+ALPINE_GPU_API int alpine_gpu_occluded(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, uint8_t* occluded);
+
+/* The same two queries on DEVICE buffers, enqueued on `stream` (a
+ * cudaStream_t; NULL = the context's stream). Asynchronous: errors raised by
+ * the kernels are reported by the next alpine_gpu_synchronize(). */
+ALPINE_GPU_API int alpine_gpu_trace_device(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, alpine_gpu_hit* hits,
+                            void* stream);
+ALPINE_GPU_API int alpine_gpu_occluded_device(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, uint8_t* occluded,
+                               void* stream);
+
+/* Traversal statistics for `count` rays in DEVICE memory: runs the same
+ * traversal as alpine_gpu_trace_device / alpine_gpu_occluded_device (any_hit
+ * selects which) with counters, and writes the wide nodes fetched and the
+ * triangles tested, summed over all rays. The reference's BvhStats
+ * (src/accelerators/bvh_common.h:19-61, enabled by ENABLE_BVH_STATS).
+ * Synchronous. */
+ALPINE_GPU_API int alpine_gpu_traversal_stats(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count,
+                                              int any_hit, uint64_t* node_visits, uint64_t* triangle_visits);
+
+/* Waits for all work of the context and reports device-side errors. */
+ALPINE_GPU_API int alpine_gpu_synchronize(alpine_gpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,405 @@
+// Test infrastructure (oracle): a C-ABI harness around the UNMODIFIED reference
+// sources, compiled from the reference tree by oracle/Makefile into
+// oracle/_ref/libalpine_ref.so. It is used only by the tests, by smoke() as the
+// checker, and by bench.py's CPU-baseline / `--impl reference` arms.
+//
+// Two parts:
+//  * ref_accel_*  : drive alpine::Bvh / alpine::WideBvh directly through the
+//                   reference's Accelerator interface
+//                   (src/accelerators/accelerator.h:13-39) with a thread pool
+//                   calling intersect / intersectAny, as a microbenchmark
+//                   would.
+//  * ref_render_* : drive the reference integrator (class Alpine in
+//                   src/alpine.cpp) through its own methods. alpine.cpp is
+//                   included into this translation unit with `private`
+//                   redefined so that the HDR accumulator (mAccumBuffer,
+//                   mTotalSamples; src/alpine.cpp:109-112) can be read back.
+//                   No reference file is modified.
+//
+// The reference's loaders need tinyobjloader / tinygltf / stb, which are not
+// vendored; this harness therefore defines loadObj/loadGltf/loadHdr
+// (src/loaders/file_loader.h:10-12): loadObj is a minimal reader for the
+// `v / vn / f / usemtl / mtllib Kd` subset, building Mesh::Data the way
+// src/loaders/obj_loader.cpp:45-119 does; GLB and HDR loading report failure.
+
+// Standard headers first, so that the `private` redefinition below only
+// reaches the reference's own headers.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cassert>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <future>
+#include <limits>
+#include <map>
+#include <memory>
+#include <memory_resource>
+#include <mutex>
+#include <numbers>
+#include <optional>
+#include <span>
+#include <sstream>
+#include <string>
+#include <string_view>
+#include <thread>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#define private public
+#include "alpine.cpp"
+#undef private
+
+#include <accelerators/bvh.h>
+#include <accelerators/wide_bvh.h>
+#include <materials/conductor.h>
+#include <materials/dielectric.h>
+#include <shapes/mesh.h>
+#include <intersection.h>
+#include <ray.h>
+
+namespace alpine {
+// ---------------------------------------------------------------------------
+// Loaders (see file header).
+bool
+loadObj(Scene* scene, std::string_view filename)
+{
+    std::ifstream in{std::string(filename)};
+    if (!in)
+    {
+        printf("ERROR: cannot open %s\n", std::string(filename).c_str());
+        return false;
+    }
+    std::string dir(filename);
+    auto slash = dir.find_last_of('/');
+    dir = slash == std::string::npos ? std::string() : dir.substr(0, slash + 1);
+
+    std::map<std::string, float3> kd;
+    std::vector<std::string> names;
+    Mesh::Data data;
+    std::vector<std::shared_ptr<Material>> mats;
+    std::map<std::string, uint32_t> matIndex;
+    int32_t current = -1;
+
+    auto loadMtl = [&](const std::string& file) {
+        std::ifstream m(dir + file);
+        std::string line, cur;
+        while (std::getline(m, line))
+        {
+            std::istringstream ls(line);
+            std::string tok;
+            ls >> tok;
+            if (tok == "newmtl") { ls >> cur; kd[cur] = float3(0.0f); }
+            else if (tok == "Kd") { float r, g, b; ls >> r >> g >> b; kd[cur] = float3(r, g, b); }
+        }
+    };
+
+    std::string line;
+    while (std::getline(in, line))
+    {
+        std::istringstream ls(line);
+        std::string tok;
+        ls >> tok;
+        if (tok == "v") { float x, y, z; ls >> x >> y >> z; data.vertices.push_back(float3(x, y, z)); }
+        else if (tok == "vn") { float x, y, z; ls >> x >> y >> z; data.normals.push_back(float3(x, y, z)); }
+        else if (tok == "mtllib") { std::string f; ls >> f; loadMtl(f); }
+        else if (tok == "usemtl")
+        {
+            std::string n; ls >> n;
+            auto it = matIndex.find(n);
+            if (it == matIndex.end())
+            {
+                // obj_loader.cpp:73-75: every OBJ material is Dielectric(alpha = 1).
+                mats.push_back(std::make_shared<Dielectric>(float2(1.0f), kd[n], nullptr, nullptr));
+                it = matIndex.emplace(n, static_cast<uint32_t>(mats.size() - 1)).first;
+            }
+            current = static_cast<int32_t>(it->second);
+        }
+        else if (tok == "f")
+        {
+            uint32_t v[3], n[3];
+            bool hasN = true;
+            for (int k = 0; k < 3; ++k)
+            {
+                std::string f; ls >> f;
+                v[k] = static_cast<uint32_t>(std::stoul(f)) - 1;
+                auto p = f.find("//");
+                if (p != std::string::npos) { n[k] = static_cast<uint32_t>(std::stoul(f.substr(p + 2))) - 1; }
+                else
+                {
+                    auto p1 = f.find('/');
+                    auto p2 = p1 == std::string::npos ? p1 : f.find('/', p1 + 1);
+                    if (p2 != std::string::npos) { n[k] = static_cast<uint32_t>(std::stoul(f.substr(p2 + 1))) - 1; }
+                    else { hasN = false; n[k] = 0; }
+                }
+            }
+            if (current < 0)
+            {
+                printf("ERROR: face without material in %s\n", std::string(filename).c_str());
+                return false;
+            }
+            data.prims.push_back(uint3(v[0], v[1], v[2]));
+            if (hasN) { data.normalPrims.push_back(uint3(n[0], n[1], n[2])); }
+            data.materials.push_back(mats[current]);
+        }
+    }
+    if (data.normalPrims.size() != data.prims.size()) { data.normalPrims.clear(); data.normals.clear(); }
+    scene->shapes.push_back(std::make_shared<Mesh>(std::move(data), 0));
+    return true;
+}
+
+bool
+loadGltf(Scene*, std::string_view)
+{
+    printf("ERROR: GLB loading needs tinygltf, which is not vendored.\n");
+    return false;
+}
+
+bool
+loadHdr(std::unique_ptr<EnvironmentMap>&, std::string_view)
+{
+    printf("ERROR: HDR loading needs stb_image, which is not vendored.\n");
+    return false;
+}
+}
+
+using namespace alpine;
+
+namespace {
+struct RefAccel
+{
+    std::vector<std::byte> arena;
+    std::unique_ptr<Accelerator> acc;
+    int dummyShape = 0;
+};
+
+template <typename F>
+void parallelFor(uint64_t n, int nthreads, F&& body)
+{
+    if (nthreads <= 0)
+    {
+        nthreads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    }
+    constexpr uint64_t kChunk = 256;
+    std::atomic<uint64_t> next{0};
+    auto worker = [&]() {
+        for (;;)
+        {
+            uint64_t b = next.fetch_add(kChunk);
+            if (b >= n) { break; }
+            uint64_t e = std::min(n, b + kChunk);
+            for (uint64_t i = b; i < e; ++i) { body(i); }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) { pool.emplace_back(worker); }
+    worker();
+    for (auto& th : pool) { th.join(); }
+}
+
+inline Ray makeRay(const float* r)
+{
+    Ray ray;
+    ray.org = float3(r[0], r[1], r[2]);
+    ray.dir = float3(r[4], r[5], r[6]);
+    return ray;
+}
+}
+
+extern "C" {
+// kind: 0 = Bvh (binary), 1 = WideBvh (8-wide, ISPC kernels restated).
+void*
+ref_accel_create(int kind, uint64_t arenaBytes)
+{
+    auto* h = new RefAccel;
+    h->arena.resize(arenaBytes);
+    if (kind == 1)
+    {
+        h->acc = std::make_unique<WideBvh>(std::span<std::byte>(h->arena));
+    }
+    else
+    {
+        h->acc = std::make_unique<Bvh>(std::span<std::byte>(h->arena));
+    }
+    return h;
+}
+
+uint32_t
+ref_accel_add_mesh(void* hp, const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    std::vector<float3> v(nverts);
+    for (uint32_t i = 0; i < nverts; ++i) { v[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    std::vector<uint3> p(ntris);
+    for (uint32_t i = 0; i < ntris; ++i) { p[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]); }
+    return h->acc->appendMesh(v, p, &h->dummyShape);
+}
+
+// Returns the wall time of Accelerator::updateScene (full build) in ms.
+double
+ref_accel_build(void* hp)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    auto t0 = std::chrono::steady_clock::now();
+    h->acc->updateScene();
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// rays: 8 floats per ray {ox, oy, oz, tmin, dx, dy, dz, tmax}. The reference's
+// intersect() has no tmin/tmax (t >= 0, tFar = FLT_MAX); both are ignored here.
+// Misses write prim = 0xffffffff, t = FLT_MAX, b1 = b2 = 0.
+void
+ref_accel_intersect(void* hp, const float* rays, uint64_t n, int nthreads,
+    uint32_t* prim, float* t, float* b1, float* b2)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    parallelFor(n, nthreads, [&](uint64_t i) {
+        auto isect = h->acc->intersect(makeRay(rays + 8 * i));
+        if (isect.has_value())
+        {
+            prim[i] = isect->primId;
+            t[i] = isect->t;
+            b1[i] = isect->barycentric.x;
+            b2[i] = isect->barycentric.y;
+        }
+        else
+        {
+            prim[i] = 0xffffffffu;
+            t[i] = FLT_MAX;
+            b1[i] = 0.0f;
+            b2[i] = 0.0f;
+        }
+    });
+}
+
+// intersectAny(ray, tFar = tmax) for each ray; writes 1 when occluded.
+void
+ref_accel_occluded(void* hp, const float* rays, uint64_t n, int nthreads, uint8_t* occluded)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    parallelFor(n, nthreads, [&](uint64_t i) {
+        occluded[i] = h->acc->intersectAny(makeRay(rays + 8 * i), rays[8 * i + 7]) ? 1 : 0;
+    });
+}
+
+void
+ref_accel_destroy(void* hp)
+{
+    delete static_cast<RefAccel*>(hp);
+}
+
+// ---------------------------------------------------------------------------
+// Integrator harness: the public alpine:: API plus direct mesh/material input.
+int
+ref_render_init(uint32_t width, uint32_t height, uint32_t maxDepth, uint64_t arenaBytes)
+{
+    if (sAlpine) { shutdown(); }
+    return initialize(static_cast<uint32_t>(arenaBytes), width, height, maxDepth) ? 1 : 0;
+}
+
+void ref_render_reset_scene(int acc) { resetScene(static_cast<AcceleratorType>(acc)); }
+
+// Adds one mesh. materials: `nmat` records of 5 floats {kind, r, g, b, roughness}
+// with kind 0 = Dielectric, 1 = Conductor (the two material classes the loaders
+// create, gltf_loader.cpp:404-414). normals: per-vertex, may be null.
+int
+ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
+    const float* normals, const uint32_t* triMaterial, const float* materials, uint32_t nmat)
+{
+    Mesh::Data d;
+    d.vertices.resize(nverts);
+    for (uint32_t i = 0; i < nverts; ++i) { d.vertices[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    if (normals)
+    {
+        d.normals.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i) { d.normals[i] = float3(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]); }
+    }
+    std::vector<std::shared_ptr<Material>> mats(nmat);
+    for (uint32_t m = 0; m < nmat; ++m)
+    {
+        const float* r = materials + 5 * m;
+        float3 bc(r[1], r[2], r[3]);
+        if (r[0] == 1.0f) { mats[m] = std::make_shared<Conductor>(float2(r[4]), bc, nullptr, nullptr); }
+        else { mats[m] = std::make_shared<Dielectric>(float2(r[4]), bc, nullptr, nullptr); }
+    }
+    d.prims.resize(ntris);
+    d.materials.resize(ntris);
+    for (uint32_t i = 0; i < ntris; ++i)
+    {
+        d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]);
+        uint32_t m = triMaterial[i];
+        if (m >= nmat) { return 0; }
+        d.materials[i] = mats[m];
+    }
+    auto mesh = std::make_shared<Mesh>(std::move(d), 0);
+    auto& a = alpine::alpine();
+    a.mScene.shapes.push_back(mesh);
+    mesh->appendTo(a.mAccelerator.get());
+    return 1;
+}
+
+int ref_render_load_obj(const char* path) { return loadScene(path, FileType::Obj) ? 1 : 0; }
+
+void
+ref_render_add_disk_light(float power, const float* color, const float* pos, const float* target, float radius)
+{
+    addDiskLight(power, color, pos, target, radius);
+}
+
+void ref_render_add_point_light(float power, const float* color, const float* pos) { addPointLight(power, color, pos); }
+void ref_render_update_scene(float time) { updateScene(time); }
+void ref_render_build_light_sampler(int type) { buildLightSampler(static_cast<LightSamplerType>(type)); }
+void ref_render_set_background(float r, float g, float b) { setBackgroundColor(r, g, b); }
+
+void
+ref_render_set_camera(const float* eye, const float* target, const float* up, float fovy, float aspect)
+{
+    getCamera()->setLookAt(eye, target, up, fovy, aspect);
+}
+
+void ref_render_reset_accumulation() { resetAccumulation(); }
+
+double
+ref_render(uint32_t spp)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    render(spp);
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// Copies the per-pixel radiance SUMS (color, albedo, normal; 9 floats per pixel,
+// denoiser::RenderTarget layout) and returns the accumulated sample count.
+uint32_t
+ref_render_read_accum(float* out)
+{
+    auto& a = alpine::alpine();
+    for (size_t i = 0; i < a.mAccumBuffer.size(); ++i)
+    {
+        const auto& p = a.mAccumBuffer[i];
+        float* o = out + 9 * i;
+        o[0] = p.color.x; o[1] = p.color.y; o[2] = p.color.z;
+        o[3] = p.albedo.x; o[4] = p.albedo.y; o[5] = p.albedo.z;
+        o[6] = p.normal.x; o[7] = p.normal.y; o[8] = p.normal.z;
+    }
+    return a.mTotalSamples;
+}
+
+void
+ref_render_post_process(int tonemap, uint8_t* rgb)
+{
+    postProcess(false, tonemap != 0);
+    auto& a = alpine::alpine();
+    std::memcpy(rgb, getFrameBuffer(), a.mFrameBuffer.size() * 3);
+}
+
+void ref_render_shutdown() { shutdown(); }
+}
