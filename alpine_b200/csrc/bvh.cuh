@@ -63,7 +63,7 @@ constexpr int kWidth = 8;
 constexpr int kMaxLeafTris = 3;          // unary count field holds 1..3
 constexpr int kSahBins = 32;             // binned SAH resolution
 constexpr int kTraversalStack = 32;      // node-group stack entries per ray
-constexpr uint32_t kMaxVisits = 1u << 20;  // per-ray node+triangle visit cap
+constexpr uint32_t kMaxVisits = 1u << 16;  // per-ray wide-node visit cap
 
 struct BvhView {
     const WideNode* nodes;

@@ -49,6 +49,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", action="store_true",
+                   help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     return p.parse_args()
 
 
@@ -236,18 +238,27 @@ def run_ours(args):
     ctx.add_mesh(verts, idx)
     stats = ctx.build()
     build_times = []
-    for _ in range(3):  # rebuild timings (device time of the whole build)
-        build_times.append(ctx.build()["build_ms"])
+    if args.profile:
+        args.warmup, args.steps, args.no_cpu_baseline = 1, 1, True
+    else:
+        for _ in range(3):  # rebuild timings (device time of the whole build)
+            build_times.append(ctx.build()["build_ms"])
 
     d_closest = torch.from_numpy(closest).cuda()
     d_shadow = torch.from_numpy(shadow).cuda()
     d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
     d_occ = torch.empty(n, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the kernels and the CUDA events must share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    assert sp != 0
 
-    nv_c, tv_c = ctx.traversal_stats(d_closest.data_ptr(), n, False)
-    nv_s, tv_s = ctx.traversal_stats(d_shadow.data_ptr(), n, True)
+    if args.profile:
+        nv_c = tv_c = nv_s = tv_s = 0
+    else:
+        nv_c, tv_c = ctx.traversal_stats(d_closest.data_ptr(), n, False)
+        nv_s, tv_s = ctx.traversal_stats(d_shadow.data_ptr(), n, True)
 
     def step(ev=None):
         if ev is not None:
@@ -279,6 +290,11 @@ def run_ours(args):
     any_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
     value = world * 2 * n / (ms_step / 1e3) / 1e6
 
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "closest_ms": closest_ms, "any_ms": any_ms}), flush=True)
+        ctx.close()
+        return
     # end to end through the C ABI with pinned host buffers
     h_closest = torch.from_numpy(closest).pin_memory().numpy()
     h_shadow = torch.from_numpy(shadow).pin_memory().numpy()
