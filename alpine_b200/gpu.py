@@ -24,6 +24,7 @@ ERR_OUT_OF_MEMORY = -5
 RAY_DTYPE = np.dtype([("org", np.float32, 3), ("tmin", np.float32), ("dir", np.float32, 3), ("tmax", np.float32)])
 HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32), ("b1", np.float32), ("b2", np.float32)])
 MISS = 0xFFFFFFFF
+NOALLOC_MAX_RAYS = 65536
 
 
 class GpuError(RuntimeError):
@@ -70,6 +71,7 @@ def lib():
         L.alpine_gpu_trace_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
         L.alpine_gpu_occluded_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
         L.alpine_gpu_synchronize.argtypes = [vp]
+        L.alpine_gpu_trace_noalloc.argtypes = [vp, vp, C.c_uint64, vp]
         L.alpine_gpu_traversal_stats.argtypes = [vp, vp, C.c_uint64, C.c_int, C.POINTER(C.c_uint64),
                                                  C.POINTER(C.c_uint64)]
         _lib = L
@@ -132,6 +134,14 @@ class Context:
         r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         hits = np.empty(r.shape[0], HIT_DTYPE) if out is None else out
         self._check(self.L.alpine_gpu_trace(self.h, _ptr(r), r.shape[0], _ptr(hits)))
+        return hits
+
+    def trace_noalloc(self, rays: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """Closest hit through the entry point that allocates no memory
+        (at most NOALLOC_MAX_RAYS rays per call)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hits = np.empty(r.shape[0], HIT_DTYPE) if out is None else out
+        self._check(self.L.alpine_gpu_trace_noalloc(self.h, _ptr(r), r.shape[0], _ptr(hits)))
         return hits
 
     def occluded(self, rays: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:

@@ -125,6 +125,23 @@ ALPINE_GPU_API int alpine_gpu_trace_device(alpine_gpu_ctx* ctx, const alpine_gpu
 ALPINE_GPU_API int alpine_gpu_occluded_device(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, uint8_t* occluded,
                                void* stream);
 
+/* Closest hit for at most ALPINE_GPU_NOALLOC_MAX_RAYS rays in HOST memory,
+ * allocating no memory. This entry point has no counterpart in the reference.
+ * It is for callers that cannot call cudaMalloc at query time: a host
+ * application that owns the device-memory budget through its own pools, or a
+ * per-frame path that cannot accept an allocation's implicit synchronisation
+ * or a late out-of-memory failure. alpine_gpu_trace grows device staging
+ * buffers as needed; this variant stages through one fixed 3 MiB array in
+ * device memory that every GPU loading the library holds until exit. Larger
+ * batches are rejected with ALPINE_GPU_ERR_INVALID_ARGUMENT. The first call
+ * on a device looks up the array's device address; make it before any stream
+ * capture. All calls share the array, so calls are serialised inside the
+ * library; calls that overlapped on one device would race. Blocks until done.
+ * Results are identical to alpine_gpu_trace. */
+#define ALPINE_GPU_NOALLOC_MAX_RAYS 65536
+ALPINE_GPU_API int alpine_gpu_trace_noalloc(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count,
+                                            alpine_gpu_hit* hits);
+
 /* Traversal statistics for `count` rays in DEVICE memory: runs the same
  * traversal as alpine_gpu_trace_device / alpine_gpu_occluded_device (any_hit
  * selects which) with counters, and writes the wide nodes fetched and the
