@@ -62,7 +62,10 @@ static_assert(sizeof(BinNode) == 48, "binary node is 48 bytes");
 constexpr int kWidth = 8;
 constexpr int kMaxLeafTris = 3;          // unary count field holds 1..3
 constexpr int kSahBins = 32;             // binned SAH resolution
-constexpr int kTraversalStack = 32;      // node-group stack entries per ray
+#ifndef AG_TRAVERSAL_STACK
+#define AG_TRAVERSAL_STACK 24
+#endif
+constexpr int kTraversalStack = AG_TRAVERSAL_STACK;  // node-group stack entries per ray
 constexpr uint32_t kMaxVisits = 1u << 16;  // per-ray wide-node visit cap
 
 struct BvhView {

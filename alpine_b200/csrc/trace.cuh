@@ -5,9 +5,13 @@
 
 namespace ag {
 
-constexpr int kTraceBlock = 128;
+#ifndef AG_TRACE_BLOCK
+#define AG_TRACE_BLOCK 128
+#endif
+constexpr int kTraceBlock = AG_TRACE_BLOCK;
 
-// hits: 16-byte {prim, t, b1, b2} records.
+// hits: 16-byte {prim, t, b1, b2} records. status: device word receiving
+// DeviceError bits (ORed).
 void launch_trace(const BvhView& bvh, const void* rays, uint64_t n, void* hits, uint32_t* status, cudaStream_t st);
 void launch_occluded(const BvhView& bvh, const void* rays, uint64_t n, uint8_t* occ, uint32_t* status,
                      cudaStream_t st);

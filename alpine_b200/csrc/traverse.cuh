@@ -80,6 +80,34 @@ AG_D float safe_rcp(float d)
 
 AG_D uint4 ldg4(const void* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
 
+// Exact float value of byte k of w: either by the conversion unit (I2F,
+// measured faster on B200) or by placing the byte under the exponent of 2^23
+// (PRMT) and subtracting 2^23 (FADD).
+#ifndef AG_BYTE_CVT_I2F
+#define AG_BYTE_CVT_I2F 1
+#endif
+AG_D float byte_to_float(uint32_t w, uint32_t k)
+{
+#if AG_BYTE_CVT_I2F
+    return float((w >> (8 * k)) & 0xffu);
+#else
+    return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7440u | k)) - 8388608.0f;
+#endif
+}
+
+AG_D float max3f(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+AG_D float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Intersects the 8 child boxes of a node; returns the hit mask (internal
 // children at bits 24 + (slot ^ oct), triangles at their offsets).
 AG_D uint32_t intersect_children(const uint4& w0, const uint4& w1, const uint4& w2, const uint4& w3, const uint4& w4,
@@ -106,18 +134,17 @@ AG_D uint32_t intersect_children(const uint4& w0, const uint4& w1, const uint4& 
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int sh = 8 * k;
-            float tnx = fmaf(float((nearX[h] >> sh) & 0xffu), sx, ox);
-            float tny = fmaf(float((nearY[h] >> sh) & 0xffu), sy, oy);
-            float tnz = fmaf(float((nearZ[h] >> sh) & 0xffu), sz, oz);
-            float tfx = fmaf(float((farX[h] >> sh) & 0xffu), sx, ox);
-            float tfy = fmaf(float((farY[h] >> sh) & 0xffu), sy, oy);
-            float tfz = fmaf(float((farZ[h] >> sh) & 0xffu), sz, oz);
-            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-            float tf = fminf(fminf(tfx, tfy), tfz) * kBoxExitScale;
+        for (uint32_t k = 0; k < 4; ++k) {
+            float tnx = fmaf(byte_to_float(nearX[h], k), sx, ox);
+            float tny = fmaf(byte_to_float(nearY[h], k), sy, oy);
+            float tnz = fmaf(byte_to_float(nearZ[h], k), sz, oz);
+            float tfx = fmaf(byte_to_float(farX[h], k), sx, ox);
+            float tfy = fmaf(byte_to_float(farY[h], k), sy, oy);
+            float tfz = fmaf(byte_to_float(farZ[h], k), sz, oz);
+            float tn = max3f(tnx, tny, fmaxf(tnz, tmin));
+            float tf = min3f(tfx, tfy, tfz) * kBoxExitScale;
             if (tn <= tf && tn <= tmax) {
-                uint32_t m = (meta[h] >> sh) & 0xffu;
+                uint32_t m = (meta[h] >> (8 * k)) & 0xffu;
                 uint32_t low = m & 0x1fu;
                 uint32_t pos = low >= 24u ? (low ^ oct) : low;
                 hits |= (m >> 5) << pos;
@@ -127,76 +154,109 @@ AG_D uint32_t intersect_children(const uint4& w0, const uint4& w1, const uint4& 
     return hits;
 }
 
-// Traces one ray. stack: this thread's first stack entry in shared memory,
-// entries `stride` elements apart. err accumulates DeviceError bits.
-// Returns true when something was hit (closest: result filled; any: first hit).
+// Traversal state of one ray (kept in registers; the stack is in shared memory).
+struct RayState {
+    float3 o, d, id;
+    float tmin, tmax;
+    uint32_t oct;
+    uint2 ngroup, tgroup;
+    int sp;
+    uint32_t visits;
+    TraceResult res;
+    bool found;
+};
+
+AG_D void ray_init(RayState& s, float3 o, float3 d, float tmin, float tmax)
+{
+    s.o = o;
+    s.d = d;
+    s.id = mk3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    s.tmin = tmin;
+    s.tmax = tmax;
+    s.oct = (s.id.x < 0.0f ? 1u : 0u) | (s.id.y < 0.0f ? 2u : 0u) | (s.id.z < 0.0f ? 4u : 0u);
+    s.ngroup = make_uint2(0u, (1u << (24u + s.oct)) | 1u);  // the root as slot 0 of a virtual parent
+    s.tgroup = make_uint2(0u, 0u);
+    s.sp = 0;
+    s.visits = 0;
+    s.res.prim = 0xffffffffu;
+    s.res.t = 3.402823466e38f;
+    s.res.b1 = 0.0f;
+    s.res.b2 = 0.0f;
+    s.found = false;
+}
+
+// One traversal step: tests the pending triangles, then fetches and
+// intersects the next node. Returns true when the ray is finished (s.found
+// tells whether it hit; on a device-side error the ray ends as a miss).
+// stack: this thread's first entry in shared memory, entries `stride` apart.
 // nodeVisits / triVisits count wide nodes fetched and triangles tested (the
 // reference's BvhStats counters, src/accelerators/bvh_common.h:19-61).
+template <bool kAny>
+AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, uint32_t& err, uint32_t& nodeVisits,
+                   uint32_t& triVisits)
+{
+    while (s.tgroup.y != 0u) {
+        uint32_t k = __ffs(s.tgroup.y) - 1u;
+        s.tgroup.y &= s.tgroup.y - 1u;
+        uint32_t ti = s.tgroup.x + k;
+        if (ti >= bvh.triCount) { err |= kErrBadIndex; s.found = false; return true; }
+        ++triVisits;
+        const TriRecord* r = bvh.tris + ti;
+        float4 v0 = __ldg(&r->v0), e0 = __ldg(&r->e0), e1 = __ldg(&r->e1);
+        float t, b1, b2;
+        if (tri_test(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2)) {
+            s.res.prim = __float_as_uint(v0.w);
+            s.res.t = t;
+            s.res.b1 = b1;
+            s.res.b2 = b2;
+            s.found = true;
+            if (kAny) return true;
+            s.tmax = t;
+        }
+    }
+    if ((s.ngroup.y & 0xff000000u) == 0u) {
+        if (s.sp == 0) return true;
+        s.ngroup = stack[--s.sp * stride];
+    }
+    uint32_t p = __ffs(s.ngroup.y >> 24) - 1u;
+    s.ngroup.y &= ~(1u << (24u + p));
+    uint32_t slot = p ^ s.oct;
+    uint32_t child = s.ngroup.x + __popc(s.ngroup.y & 0xffu & ((1u << slot) - 1u));
+    if (s.ngroup.y & 0xff000000u) {
+        if (s.sp >= kTraversalStack) { err |= kErrStackOverflow; s.found = false; return true; }
+        stack[s.sp++ * stride] = s.ngroup;
+    }
+    if (child >= bvh.nodeCount) { err |= kErrBadIndex; s.found = false; return true; }
+    if (++s.visits > kMaxVisits) { err |= kErrIterations; s.found = false; return true; }
+    ++nodeVisits;
+    const uint4* np = reinterpret_cast<const uint4*>(bvh.nodes + child);
+    uint4 w0 = ldg4(np), w1 = ldg4(np + 1), w2 = ldg4(np + 2), w3 = ldg4(np + 3), w4 = ldg4(np + 4);
+    uint32_t hits = intersect_children(w0, w1, w2, w3, w4, s.o, s.id, s.oct, s.tmin, s.tmax);
+    s.ngroup = make_uint2(w1.x, (hits & 0xff000000u) | (w0.w >> 24));
+    s.tgroup = make_uint2(w1.y, hits & 0x00ffffffu);
+    return false;
+}
+
+// Traces one ray to completion. Returns true when something was hit
+// (closest: res filled; any: the first hit found).
 template <bool kAny>
 AG_D bool trace(const BvhView& bvh, float3 o, float3 d, float tmin, float tmax, TraceResult& res, uint2* stack,
                 int stride, uint32_t& err, uint32_t& nodeVisits, uint32_t& triVisits)
 {
-    res.prim = 0xffffffffu;
-    res.t = 3.402823466e38f;
-    res.b1 = 0.0f;
-    res.b2 = 0.0f;
-    if (bvh.nodeCount == 0) return false;
-    const float3 id = mk3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
-    const uint32_t oct = (id.x < 0.0f ? 1u : 0u) | (id.y < 0.0f ? 2u : 0u) | (id.z < 0.0f ? 4u : 0u);
-    uint2 ngroup = make_uint2(0u, (1u << (24u + oct)) | 1u);  // the root as slot 0 of a virtual parent
-    uint2 tgroup = make_uint2(0u, 0u);
-    int sp = 0;
-    uint32_t visits = 0;
-    bool found = false;
-    for (;;) {
-        // triangles of the current node
-        while (tgroup.y != 0u) {
-            uint32_t k = __ffs(tgroup.y) - 1u;
-            tgroup.y &= tgroup.y - 1u;
-            uint32_t ti = tgroup.x + k;
-            if (ti >= bvh.triCount) { err |= kErrBadIndex; return false; }
-            ++triVisits;
-            const TriRecord* r = bvh.tris + ti;
-            float4 v0 = __ldg(&r->v0), e0 = __ldg(&r->e0), e1 = __ldg(&r->e1);
-            float t, b1, b2;
-            if (tri_test(o, d, v0, e0, e1, tmin, tmax, t, b1, b2)) {
-                if (kAny) {
-                    res.prim = __float_as_uint(v0.w);
-                    res.t = t;
-                    res.b1 = b1;
-                    res.b2 = b2;
-                    return true;
-                }
-                tmax = t;
-                res.prim = __float_as_uint(v0.w);
-                res.t = t;
-                res.b1 = b1;
-                res.b2 = b2;
-                found = true;
-            }
+    RayState s;
+    ray_init(s, o, d, tmin, tmax);
+    if (bvh.nodeCount != 0) {
+        while (!ray_step<kAny>(bvh, s, stack, stride, err, nodeVisits, triVisits)) {
         }
-        if ((ngroup.y & 0xff000000u) == 0u) {
-            if (sp == 0) break;
-            ngroup = stack[--sp * stride];
-        }
-        uint32_t p = __ffs(ngroup.y >> 24) - 1u;
-        ngroup.y &= ~(1u << (24u + p));
-        uint32_t slot = p ^ oct;
-        uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
-        if (ngroup.y & 0xff000000u) {
-            if (sp >= kTraversalStack) { err |= kErrStackOverflow; return false; }
-            stack[sp++ * stride] = ngroup;
-        }
-        if (child >= bvh.nodeCount) { err |= kErrBadIndex; return false; }
-        if (++visits > kMaxVisits) { err |= kErrIterations; return false; }
-        ++nodeVisits;
-        const uint4* np = reinterpret_cast<const uint4*>(bvh.nodes + child);
-        uint4 w0 = ldg4(np), w1 = ldg4(np + 1), w2 = ldg4(np + 2), w3 = ldg4(np + 3), w4 = ldg4(np + 4);
-        uint32_t hits = intersect_children(w0, w1, w2, w3, w4, o, id, oct, tmin, tmax);
-        ngroup = make_uint2(w1.x, (hits & 0xff000000u) | (w0.w >> 24));
-        tgroup = make_uint2(w1.y, hits & 0x00ffffffu);
     }
-    return found;
+    if (!s.found) {
+        s.res.prim = 0xffffffffu;
+        s.res.t = 3.402823466e38f;
+        s.res.b1 = 0.0f;
+        s.res.b2 = 0.0f;
+    }
+    res = s.res;
+    return s.found;
 }
 
 }  // namespace ag

@@ -12,7 +12,8 @@ import numpy as np
 
 from . import build as _build
 
-LIB_PATH = _build.LIB
+# ALPINE_GPU_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("ALPINE_GPU_LIB", _build.LIB)
 
 OK = 0
 ERR_INVALID_ARGUMENT = -1
