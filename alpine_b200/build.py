@@ -54,7 +54,9 @@ def needs_build() -> bool:
 
 def _compile(src: str, verbose: bool, extra=()):
     obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-c", src, "-o", obj]
+    # *_exact.cu: no multiply-add contraction (bit-compatible FP32 arithmetic)
+    per_file = ["-fmad=false"] if src.endswith("_exact.cu") else []
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *per_file, *extra, "-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -2,6 +2,7 @@
 #include "context.cuh"
 #include "trace.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -208,6 +209,14 @@ int alpine_gpu_reset_scene(alpine_gpu_ctx* c)
     c->bvhDirty = true;
     c->nodeCount = 0;
     c->triCount = 0;
+    // Scene::reset also drops the lights (src/scenes/scene.h:21-26)
+    c->triInfo.clear();
+    c->normals.clear();
+    c->attribsDirty = true;
+    c->lights.clear();
+    c->lightsDirty = true;
+    c->samplerKind = ag::kSamplerNone;
+    c->samplerLightCount = 0;
     return ALPINE_GPU_OK;
 }
 

@@ -3,6 +3,7 @@
 
 #include "../../include/alpine_gpu.h"
 #include "build.cuh"
+#include "shading.cuh"
 
 #include <string>
 #include <vector>
@@ -69,6 +70,49 @@ struct alpine_gpu_ctx {
 
     // staging for host-memory queries
     ag::DeviceBuffer dRays, dOut;
+
+    // rendering: per-triangle material/normal flags and per-vertex normals
+    std::vector<uint32_t> triInfo;  // material id | 0x80000000 when the mesh has vertex normals
+    std::vector<float> normals;     // 3 per vertex (zero for meshes without normals)
+    bool attribsDirty = true;
+    ag::DeviceBuffer dTriInfo, dNormals;
+    std::vector<ag::Material> materials;
+    bool materialsDirty = true;
+    ag::DeviceBuffer dMaterials;
+    uint32_t materialCount = 0;
+    // lights and the light sampler
+    std::vector<ag::Light> lights;
+    bool lightsDirty = true;
+    ag::DeviceBuffer dLights, dAlias, dLightNodes;
+    uint32_t samplerKind = ag::kSamplerNone;
+    uint32_t samplerLightCount = 0;
+    uint32_t lightNodeCount = 0;
+    // camera, background, options, accumulation
+    float3 background = make_float3(0.0f, 0.0f, 0.0f);
+    ag::Camera camera{};
+    bool cameraSet = false;
+    alpine_gpu_render_options options{ALPINE_GPU_SAMPLER_COUNTER, 0u, 0u, 0u, 0u};
+    bool accumValid = false;
+    ag::DeviceBuffer dAccum, dPixelRng;
+    size_t accumBytes = 0;
+    uint32_t totalSamples = 0;
+    ag::DeviceBuffer dWave;
+    uint32_t waveCapacity = 0;
+
+    // Reads and clears the device status word (stream must be idle).
+    int check_device_status()
+    {
+        cudaError_t e = cudaMemcpyAsync(hStatus, dStatus, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return fail(ALPINE_GPU_ERR_CUDA, std::string("status readback: ") + cudaGetErrorString(e));
+        if (*hStatus) {
+            uint32_t bits = *hStatus;
+            cudaMemsetAsync(dStatus, 0, sizeof(uint32_t), stream);
+            cudaStreamSynchronize(stream);
+            return fail(ALPINE_GPU_ERR_LIMIT, "device-side limit reached, status bits " + std::to_string(bits));
+        }
+        return ALPINE_GPU_OK;
+    }
 
     int fail(int code, const std::string& msg)
     {

@@ -1,0 +1,394 @@
+// Wavefront path-tracing kernels.
+//
+// The reference integrator (src/alpine.cpp:290-432) runs one path at a time
+// per host thread. Here a wave of paths (S samples of every pixel) advances
+// bounce by bounce through queue kernels:
+//   generate -> [extend (closest hit) -> shade -> shadow (any hit) -> resolve]
+//   x maxDepth -> accumulate.
+// shade does, per path vertex, exactly the reference's steps: miss ->
+// background; AOVs at depth 0; next-event estimation (light selection, light
+// sample + MIS, BSDF sample + MIS; estimateDirectIllumination,
+// alpine.cpp:370-432) whose shadow rays are traced in a batch; continuation
+// sample, the geometric-normal reflection test and the ray offsets
+// (alpine.cpp:342-361). resolve adds the unoccluded direct light in the
+// reference's summation order. Queues are compacted with warp-aggregated
+// atomics; every path's arithmetic is independent of its queue position, so
+// results do not depend on scheduling.
+//
+// The header is compiled twice: integrator_fast.cu (default flags, counter
+// RNG) and integrator_exact.cu (no FMA contraction; also serves the reference
+// RNG stream), inside different namespaces.
+#pragma once
+
+#include "../../include/alpine_gpu.h"
+#include "bvh.cuh"
+#include "shading.cuh"
+
+namespace ag {
+
+struct SceneView {
+    const float* verts;
+    const uint32_t* idx;
+    const float* normals;      // per vertex, may be null
+    const uint32_t* triInfo;   // per triangle: material id (bits 0-30), bit 31 = has vertex normals
+    const Material* materials;
+    uint32_t materialCount;
+    LightSamplerView lights;
+    float3 background;
+    Camera cam;
+    uint32_t width, height, maxDepth;
+};
+
+struct WaveView {
+    uint32_t numPaths;     // S * numPixels
+    uint32_t numPixels;
+    uint32_t sampleBase;   // sample index of slice 0 (counter RNG)
+    uint32_t samplesInWave;
+    uint32_t seed;
+    uint32_t rrStart;      // Russian roulette from this depth; 0 = off (reference behaviour)
+    uint32_t depth;        // bounce being shaded
+    uint32_t pixelBase;    // first pixel of this wave's pixel range
+    // per path
+    float4* thr;
+    float4* rad;
+    float4* albedo;
+    float4* nrm;
+    uint4* rng;
+    float4* pendL;         // light-sample term of the pending direct light
+    float4* pendB;         // BSDF-sample term; w = light-selection pdf
+    float4* pendThr;       // throughput at the vertex
+    int2* pendShadow;      // shadow-queue slots of the two terms (-1 = none)
+    // queues
+    alpine_gpu_ray* rays;
+    uint32_t* queuePath;
+    uint4* hits;
+    uint32_t* queueCount;
+    alpine_gpu_ray* raysNext;
+    uint32_t* queuePathNext;
+    uint32_t* queueCountNext;
+    alpine_gpu_ray* shadowRays;
+    uint8_t* shadowOcc;
+    uint32_t* shadowCount;
+    // persistent per-pixel reference RNG state (stream mode)
+    uint4* pixelRng;
+};
+
+struct IntegratorKernels {
+    void (*generate)(const SceneView&, const WaveView&, bool streamRng, cudaStream_t);
+    void (*shade)(const SceneView&, const WaveView&, bool streamRng, uint32_t maxQueue, cudaStream_t);
+    void (*resolve)(const WaveView&, uint32_t maxQueue, cudaStream_t);
+    void (*accumulate)(const WaveView&, float* accum, double* accum64, bool streamRng, cudaStream_t);
+};
+
+const IntegratorKernels& integrator_fast();
+const IntegratorKernels& integrator_exact();
+
+}  // namespace ag
+
+#ifdef AG_INTEGRATOR_NS
+namespace ag {
+namespace AG_INTEGRATOR_NS {
+
+constexpr int kThreads = 128;
+
+// Random numbers of one path: the reference's per-pixel xorshift stream, or
+// the counter hash.
+struct PathRng {
+    bool stream;
+    XorShift128 xs;
+    CounterRng cr;
+    AG_D void load(uint4 s)
+    {
+        if (stream) {
+            xs.s[0] = s.x; xs.s[1] = s.y; xs.s[2] = s.z; xs.s[3] = s.w;
+        } else {
+            cr.key = ((uint64_t)s.y << 32) | s.x;
+            cr.dim = s.z;
+        }
+    }
+    AG_D uint4 save() const
+    {
+        if (stream) return make_uint4(xs.s[0], xs.s[1], xs.s[2], xs.s[3]);
+        return make_uint4((uint32_t)cr.key, (uint32_t)(cr.key >> 32), cr.dim, 0u);
+    }
+    AG_D float next() { return stream ? xorshift_1d(xs) : counter_1d(cr); }
+};
+
+// Appends one entry per calling lane with pred set: one atomic per warp.
+AG_D uint32_t warp_append(uint32_t* counter, bool pred)
+{
+    const uint32_t am = __activemask();
+    const uint32_t m = __ballot_sync(am, pred);
+    uint32_t base = 0;
+    const int leader = m ? __ffs(m) - 1 : __ffs(am) - 1;
+    if (m && (int)(threadIdx.x & 31) == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(am, base, leader);
+    return base + __popc(m & lanemask_lt());
+}
+
+AG_D float4 f4(float3 v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
+AG_D float3 f3(float4 v) { return mk3(v.x, v.y, v.z); }
+
+__global__ void __launch_bounds__(kThreads) k_generate(SceneView sc, WaveView w, bool streamRng)
+{
+    uint32_t p = blockIdx.x * kThreads + threadIdx.x;
+    if (p >= w.numPaths) return;
+    uint32_t slice = p / w.numPixels;
+    uint32_t pixel = w.pixelBase + p % w.numPixels;
+    PathRng r;
+    r.stream = streamRng;
+    if (streamRng) r.load(w.pixelRng[pixel]);
+    else counter_init(r.cr, w.seed, pixel, w.sampleBase + slice);
+    uint32_t x = pixel % sc.width, y = pixel / sc.width;
+    // Sampler::get2D draws x then y (src/sampler.cpp:24-27)
+    float jx = r.next();
+    float jy = r.next();
+    float3 org, dir;
+    camera_ray(sc.cam, ((float)x + jx) / (float)sc.width, ((float)y + jy) / (float)sc.height, org, dir);
+    w.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    w.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    w.albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    w.nrm[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    w.pendShadow[p] = make_int2(-1, -1);
+    w.rng[p] = r.save();
+    alpine_gpu_ray ray;
+    ray.org[0] = org.x; ray.org[1] = org.y; ray.org[2] = org.z;
+    ray.tmin = 0.0f;
+    ray.dir[0] = dir.x; ray.dir[1] = dir.y; ray.dir[2] = dir.z;
+    ray.tmax = 3.402823466e38f;
+    w.rays[p] = ray;
+    w.queuePath[p] = p;
+    if (p == 0) *w.queueCount = w.numPaths;
+}
+
+AG_D alpine_gpu_ray make_ray(float3 o, float3 d, float tmax)
+{
+    alpine_gpu_ray r;
+    r.org[0] = o.x; r.org[1] = o.y; r.org[2] = o.z;
+    r.tmin = 0.0f;
+    r.dir[0] = d.x; r.dir[1] = d.y; r.dir[2] = d.z;
+    r.tmax = tmax;
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bool streamRng)
+{
+    const uint32_t n = *w.queueCount;
+    uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+    if (q >= n) return;
+    const uint32_t p = w.queuePath[q];
+    const uint4 h = w.hits[q];
+    const alpine_gpu_ray ray = w.rays[q];
+    const float3 ro = mk3(ray.org[0], ray.org[1], ray.org[2]);
+    const float3 rd = mk3(ray.dir[0], ray.dir[1], ray.dir[2]);
+    float3 thr = f3(w.thr[p]);
+    PathRng rng;
+    rng.stream = streamRng;
+    rng.load(w.rng[p]);
+    int2 shadow = make_int2(-1, -1);
+    bool cont = false;
+
+    if (h.x == 0xffffffffu) {
+        // miss: background (alpine.cpp:318-324; no environment map in this backend)
+        float3 rad = f3(w.rad[p]);
+        rad += thr * sc.background;
+        w.rad[p] = f4(rad);
+    } else {
+        const uint32_t prim = h.x;
+        const float t = __uint_as_float(h.y);
+        const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
+        const uint32_t* ti = sc.idx + 3ull * prim;
+        const uint32_t i0 = ti[0], i1 = ti[1], i2 = ti[2];
+        const float3 v0 = mk3(sc.verts[3ull * i0], sc.verts[3ull * i0 + 1], sc.verts[3ull * i0 + 2]);
+        const float3 v1 = mk3(sc.verts[3ull * i1], sc.verts[3ull * i1 + 1], sc.verts[3ull * i1 + 2]);
+        const float3 v2 = mk3(sc.verts[3ull * i2], sc.verts[3ull * i2 + 1], sc.verts[3ull * i2 + 2]);
+        // Primitive::ng = normalize(cross(e0, e1)) (bvh_common.cpp:114-117)
+        const float3 ng = normalize3(cross(v1 - v0, v2 - v0));
+        const uint32_t info = sc.triInfo[prim];
+        uint32_t mid = info & 0x7fffffffu;
+        if (mid >= sc.materialCount) mid = 0;
+        const Material mat = sc.materials[mid];
+        // Mesh::getIntersectionAttributes (mesh.cpp:57-154): interpolated
+        // vertex normal (b0 = 1 - b1 - b2), not re-normalised; else ng
+        float3 ns;
+        if (info & 0x80000000u) {
+            const float b0 = 1.0f - b1 - b2;
+            const float3 n0 = mk3(sc.normals[3ull * i0], sc.normals[3ull * i0 + 1], sc.normals[3ull * i0 + 2]);
+            const float3 n1 = mk3(sc.normals[3ull * i1], sc.normals[3ull * i1 + 1], sc.normals[3ull * i1 + 2]);
+            const float3 n2 = mk3(sc.normals[3ull * i2], sc.normals[3ull * i2 + 1], sc.normals[3ull * i2 + 2]);
+            ns = n0 * b0 + n1 * b1 + n2 * b2;
+        } else {
+            ns = ng;
+        }
+        float3 ss, ts;
+        get_basis(ns, ss, ts);
+        const float3 hit = ro + rd * t;
+        if (w.depth == 0) {
+            w.albedo[p] = f4(mat_color(mat));
+            w.nrm[p] = f4(ns);
+        }
+        const float3 wo = to_local(-rd, ss, ts, ns);
+
+        // estimateDirectIllumination (alpine.cpp:370-432)
+        // the selection number is drawn whenever a sampler exists, even with
+        // no lights (LightSampler::sample(sampler.get1D(), ...))
+        if (sc.lights.kind != kSamplerNone) {
+            float lssPdf = 0.0f;
+            int li = sample_light(sc.lights, rng.next(), hit, ns, lssPdf);
+            if (li >= 0) {
+                const Light light = sc.lights.lights[li];
+                float3 termL = mk3(0.0f, 0.0f, 0.0f), termB = mk3(0.0f, 0.0f, 0.0f);
+                const float3 so = hit + ns * kRayOffset;  // shadow rays leave along ns (alpine.cpp:389-395)
+                // light sampling
+                LightSample ls;
+                float lu0 = rng.next();
+                float lu1 = rng.next();
+                if (light_sample(light, lu0, lu1, hit, ls)) {
+                    float3 wi = to_local(ls.wi, ss, ts, ns);
+                    float bsdfPdf = mat_pdf(mat, wo, wi);
+                    if (bsdfPdf > 0.0f) {
+                        float3 bsdf = mat_bsdf(mat, wo, wi);
+                        float cosTerm = fmaxf(0.0f, dot(ls.wi, ns));
+                        float mis = !light_is_delta(light) ? power_heuristic(ls.pdf, bsdfPdf) : 1.0f;
+                        termL = ls.L * mis * bsdf * cosTerm / ls.pdf;
+                        uint32_t slot = warp_append(w.shadowCount, true);
+                        w.shadowRays[slot] = make_ray(so, ls.wi, ls.distance);
+                        shadow.x = (int)slot;
+                    }
+                }
+                // BSDF sampling (non-delta lights only)
+                if (!light_is_delta(light)) {
+                    BsdfSample ms;
+                    float bu0 = rng.next();
+                    float bu1 = rng.next();
+                    if (mat_sample(mat, wo, bu0, bu1, ms)) {
+                        float3 lightDir = to_world(ms.wi, ss, ts, ns);
+                        float lightDist;
+                        float lightPdf = light_pdf(light, hit, lightDir, lightDist);
+                        if (lightPdf > 0.0f) {
+                            float3 em = light_emitted(light);
+                            float mis = power_heuristic(ms.pdf, lightPdf);
+                            termB = em * mis * ms.estimator;
+                            uint32_t slot = warp_append(w.shadowCount, true);
+                            w.shadowRays[slot] = make_ray(so, lightDir, lightDist);
+                            shadow.y = (int)slot;
+                        }
+                    }
+                }
+                if (shadow.x >= 0 || shadow.y >= 0) {
+                    w.pendL[p] = f4(termL);
+                    w.pendB[p] = f4(termB, lssPdf);
+                    w.pendThr[p] = f4(thr);
+                }
+            }
+        }
+
+        // continuation (alpine.cpp:342-361)
+        BsdfSample ms;
+        float cu0 = rng.next();
+        float cu1 = rng.next();
+        if (mat_sample(mat, wo, cu0, cu1, ms)) {
+            float3 wiW = to_world(ms.wi, ss, ts, ns);
+            if (dot(wiW, ng) > 0.0f) {
+                thr = thr * ms.estimator;
+                cont = w.depth + 1 < sc.maxDepth;
+                // Russian roulette (not in the reference; off unless rrStart > 0)
+                if (cont && w.rrStart > 0 && w.depth + 1 >= w.rrStart) {
+                    float qs = fminf(0.95f, maxc(thr));
+                    if (rng.next() >= qs) cont = false;
+                    else thr = thr / qs;
+                }
+                if (cont) {
+                    uint32_t slot = warp_append(w.queueCountNext, true);
+                    w.raysNext[slot] = make_ray(hit + ng * kRayOffset, wiW, 3.402823466e38f);
+                    w.queuePathNext[slot] = p;
+                }
+                w.thr[p] = f4(thr);
+            }
+        }
+    }
+    w.pendShadow[p] = shadow;
+    w.rng[p] = rng.save();
+}
+
+__global__ void __launch_bounds__(kThreads) k_resolve(WaveView w)
+{
+    const uint32_t n = *w.queueCount;
+    uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+    if (q >= n) return;
+    const uint32_t p = w.queuePath[q];
+    const int2 s = w.pendShadow[p];
+    if (s.x < 0 && s.y < 0) return;
+    const bool visL = s.x >= 0 && !w.shadowOcc[s.x];
+    const bool visB = s.y >= 0 && !w.shadowOcc[s.y];
+    if (visL || visB) {
+        // radiance(local) = 0; += light term; += BSDF term; / selection pdf
+        const float4 pb = w.pendB[p];
+        float3 direct = mk3(0.0f, 0.0f, 0.0f);
+        if (visL) direct += f3(w.pendL[p]);
+        if (visB) direct += f3(pb);
+        direct = direct / pb.w;
+        float3 rad = f3(w.rad[p]);
+        rad += f3(w.pendThr[p]) * direct;
+        w.rad[p] = f4(rad);
+    }
+    w.pendShadow[p] = make_int2(-1, -1);
+}
+
+// Adds the wave's per-sample results to the per-pixel sums in sample order
+// (the reference adds sample after sample, alpine.cpp:364).
+__global__ void __launch_bounds__(kThreads) k_accumulate(WaveView w, float* accum, double* accum64, bool streamRng)
+{
+    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= w.numPixels) return;
+    const uint32_t pixel = w.pixelBase + i;
+    if (accum64) {
+        double* a = accum64 + 9ull * pixel;
+        double s[9];
+        for (int k = 0; k < 9; ++k) s[k] = a[k];
+        for (uint32_t sl = 0; sl < w.samplesInWave; ++sl) {
+            uint32_t p = sl * w.numPixels + i;
+            float4 c = w.rad[p], al = w.albedo[p], nm = w.nrm[p];
+            s[0] += c.x; s[1] += c.y; s[2] += c.z;
+            s[3] += al.x; s[4] += al.y; s[5] += al.z;
+            s[6] += nm.x; s[7] += nm.y; s[8] += nm.z;
+        }
+        for (int k = 0; k < 9; ++k) a[k] = s[k];
+    } else {
+        float* a = accum + 9ull * pixel;
+        float s[9];
+        for (int k = 0; k < 9; ++k) s[k] = a[k];
+        for (uint32_t sl = 0; sl < w.samplesInWave; ++sl) {
+            uint32_t p = sl * w.numPixels + i;
+            float4 c = w.rad[p], al = w.albedo[p], nm = w.nrm[p];
+            s[0] += c.x; s[1] += c.y; s[2] += c.z;
+            s[3] += al.x; s[4] += al.y; s[5] += al.z;
+            s[6] += nm.x; s[7] += nm.y; s[8] += nm.z;
+        }
+        for (int k = 0; k < 9; ++k) a[k] = s[k];
+    }
+    if (streamRng) w.pixelRng[pixel] = w.rng[i];  // one sample per pixel per wave in stream mode
+}
+
+inline unsigned grid(uint32_t n) { return (n + kThreads - 1) / kThreads; }
+
+void generate(const SceneView& sc, const WaveView& w, bool streamRng, cudaStream_t st)
+{
+    if (w.numPaths) k_generate<<<grid(w.numPaths), kThreads, 0, st>>>(sc, w, streamRng);
+}
+void shade(const SceneView& sc, const WaveView& w, bool streamRng, uint32_t maxQueue, cudaStream_t st)
+{
+    if (maxQueue) k_shade<<<grid(maxQueue), kThreads, 0, st>>>(sc, w, streamRng);
+}
+void resolve(const WaveView& w, uint32_t maxQueue, cudaStream_t st)
+{
+    if (maxQueue) k_resolve<<<grid(maxQueue), kThreads, 0, st>>>(w);
+}
+void accumulate(const WaveView& w, float* accum, double* accum64, bool streamRng, cudaStream_t st)
+{
+    if (w.numPixels) k_accumulate<<<grid(w.numPixels), kThreads, 0, st>>>(w, accum, accum64, streamRng);
+}
+
+}  // namespace AG_INTEGRATOR_NS
+}  // namespace ag
+#endif

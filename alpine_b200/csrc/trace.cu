@@ -56,6 +56,27 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const 
     if (err) atomicOr(status, err);
 }
 
+// Variant whose ray count is read from device memory (wavefront queues).
+template <bool kAny>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_dyn(BvhView bvh, const float4* __restrict__ rays,
+                                                           const uint32_t* __restrict__ count, void* __restrict__ out,
+                                                           uint32_t* __restrict__ status)
+{
+    __shared__ uint2 stack[kTraversalStack * kTraceBlock];
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+        float4 a = rays[2ull * i];
+        float4 b = rays[2ull * i + 1];
+        TraceResult r;
+        uint32_t err = 0, nv = 0, tv = 0;
+        bool hit = trace<kAny>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
+                               kTraceBlock, err, nv, tv);
+        if (kAny) static_cast<uint8_t*>(out)[i] = hit ? 1 : 0;
+        else static_cast<uint4*>(out)[i] = make_uint4(r.prim, __float_as_uint(r.t), __float_as_uint(r.b1), __float_as_uint(r.b2));
+        if (err) atomicOr(status, err);
+    }
+}
+
 template <bool kAny>
 void launch(const BvhView& bvh, const void* rays, uint64_t n, void* out, uint32_t* status, cudaStream_t st)
 {
@@ -70,6 +91,16 @@ void launch(const BvhView& bvh, const void* rays, uint64_t n, void* out, uint32_
     }
 }
 }  // namespace
+
+void launch_trace_dyn(const BvhView& bvh, const void* rays, const uint32_t* count, uint32_t maxCount, bool any,
+                      void* out, uint32_t* status, cudaStream_t st)
+{
+    if (maxCount == 0) return;
+    unsigned blocks = (maxCount + kTraceBlock - 1) / kTraceBlock;
+    const float4* r = static_cast<const float4*>(rays);
+    if (any) k_trace_dyn<true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, count, out, status);
+    else k_trace_dyn<false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, count, out, status);
+}
 
 void launch_trace_count(const BvhView& bvh, const void* rays, uint64_t n, bool any, unsigned long long* counts,
                         uint32_t* status, cudaStream_t st)

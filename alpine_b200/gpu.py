@@ -47,7 +47,22 @@ class BvhStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class RenderOptions(C.Structure):
+    _fields_ = [("sampler", C.c_uint32), ("max_paths_per_wave", C.c_uint32), ("russian_roulette_depth", C.c_uint32),
+                ("seed", C.c_uint32), ("accumulate_fp64", C.c_uint32)]
+
+
+MATERIAL_DTYPE = np.dtype([("kind", np.uint32), ("base_color", np.float32, 3), ("roughness", np.float32)])
+DIELECTRIC = 0
+CONDUCTOR = 1
+SAMPLER_UNIFORM, SAMPLER_POWER, SAMPLER_BVH = 0, 1, 2
+RNG_REFERENCE_STREAM, RNG_COUNTER = 0, 1
+
 _lib = None
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
 
 
 def lib():
@@ -73,6 +88,24 @@ def lib():
         L.alpine_gpu_occluded_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
         L.alpine_gpu_synchronize.argtypes = [vp]
         L.alpine_gpu_trace_noalloc.argtypes = [vp, vp, C.c_uint64, vp]
+        f3 = C.POINTER(C.c_float)
+        u32p = C.POINTER(C.c_uint32)
+        L.alpine_gpu_set_materials.argtypes = [vp, vp, C.c_uint32]
+        L.alpine_gpu_set_triangle_attributes.argtypes = [vp, C.c_uint32, vp, vp]
+        L.alpine_gpu_add_point_light.argtypes = [vp, C.c_float, f3, f3, u32p]
+        L.alpine_gpu_add_disk_light.argtypes = [vp, C.c_float, f3, f3, f3, C.c_float, u32p]
+        L.alpine_gpu_add_quad_light.argtypes = [vp, f3, f3, f3, f3, u32p]
+        L.alpine_gpu_set_light_scale.argtypes = [vp, C.c_uint32, C.c_float]
+        L.alpine_gpu_build_light_sampler.argtypes = [vp, C.c_int]
+        L.alpine_gpu_set_background.argtypes = [vp, C.c_float, C.c_float, C.c_float]
+        L.alpine_gpu_set_camera.argtypes = [vp, f3, f3, f3, C.c_float, C.c_float]
+        L.alpine_gpu_set_render_options.argtypes = [vp, C.POINTER(RenderOptions)]
+        L.alpine_gpu_reset_accumulation.argtypes = [vp]
+        L.alpine_gpu_render.argtypes = [vp, C.c_uint32]
+        L.alpine_gpu_read_accumulation.argtypes = [vp, vp, u32p]
+        L.alpine_gpu_read_accumulation_f64.argtypes = [vp, vp, u32p]
+        L.alpine_gpu_post_process.argtypes = [vp, C.c_int, vp, vp]
+        L.alpine_gpu_read_sampler_state.argtypes = [vp, vp]
         L.alpine_gpu_traversal_stats.argtypes = [vp, vp, C.c_uint64, C.c_int, C.POINTER(C.c_uint64),
                                                  C.POINTER(C.c_uint64)]
         _lib = L
@@ -165,6 +198,79 @@ class Context:
         self._check(self.L.alpine_gpu_traversal_stats(self.h, C.c_void_p(rays_ptr), n, int(any_hit), C.byref(nv),
                                                       C.byref(tv)))
         return nv.value, tv.value
+
+    # ---- rendering -------------------------------------------------------
+    def set_materials(self, materials):
+        """materials: sequence of (kind, (r, g, b), roughness)."""
+        m = np.zeros(len(materials), MATERIAL_DTYPE)
+        for i, (k, col, r) in enumerate(materials):
+            m[i] = (k, col, r)
+        self._check(self.L.alpine_gpu_set_materials(self.h, _ptr(m) if len(m) else None, len(m)))
+
+    def set_triangle_attributes(self, shape, normals=None, tri_material=None):
+        n = None if normals is None else np.ascontiguousarray(normals, np.float32)
+        t = None if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
+        self._check(self.L.alpine_gpu_set_triangle_attributes(self.h, shape, None if n is None else _ptr(n),
+                                                              None if t is None else _ptr(t)))
+
+    def add_point_light(self, power, color, position):
+        i = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_point_light(self.h, power, _f3(color), _f3(position), C.byref(i)))
+        return i.value
+
+    def add_disk_light(self, power, color, position, target, radius):
+        i = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_disk_light(self.h, power, _f3(color), _f3(position), _f3(target), radius,
+                                                     C.byref(i)))
+        return i.value
+
+    def add_quad_light(self, radiance, corner, edge_u, edge_v):
+        i = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_quad_light(self.h, _f3(radiance), _f3(corner), _f3(edge_u), _f3(edge_v),
+                                                     C.byref(i)))
+        return i.value
+
+    def set_light_scale(self, light, scale):
+        self._check(self.L.alpine_gpu_set_light_scale(self.h, light, scale))
+
+    def build_light_sampler(self, kind):
+        self._check(self.L.alpine_gpu_build_light_sampler(self.h, kind))
+
+    def set_background(self, r, g, b):
+        self._check(self.L.alpine_gpu_set_background(self.h, r, g, b))
+
+    def set_camera(self, eye, target, up, fovy, aspect):
+        self._check(self.L.alpine_gpu_set_camera(self.h, _f3(eye), _f3(target), _f3(up), fovy, aspect))
+
+    def set_render_options(self, sampler=RNG_COUNTER, max_paths_per_wave=0, russian_roulette_depth=0, seed=0,
+                           accumulate_fp64=False):
+        o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64))
+        self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
+
+    def reset_accumulation(self):
+        self._check(self.L.alpine_gpu_reset_accumulation(self.h))
+
+    def render(self, spp):
+        self._check(self.L.alpine_gpu_render(self.h, spp))
+
+    def read_accumulation(self, width, height, fp64=False):
+        """(sums float[H, W, 9] = colour, albedo, normal sums; total samples)."""
+        out = np.empty((height, width, 9), np.float64 if fp64 else np.float32)
+        n = C.c_uint32()
+        f = self.L.alpine_gpu_read_accumulation_f64 if fp64 else self.L.alpine_gpu_read_accumulation
+        self._check(f(self.h, _ptr(out), C.byref(n)))
+        return out, n.value
+
+    def read_sampler_state(self, width, height):
+        out = np.empty((height, width, 4), np.uint32)
+        self._check(self.L.alpine_gpu_read_sampler_state(self.h, _ptr(out)))
+        return out
+
+    def post_process(self, width, height, tonemap=True):
+        mean = np.empty((height, width, 3), np.float32)
+        ldr = np.empty((height, width, 3), np.uint8)
+        self._check(self.L.alpine_gpu_post_process(self.h, int(tonemap), _ptr(mean), _ptr(ldr)))
+        return mean, ldr
 
     def synchronize(self):
         self._check(self.L.alpine_gpu_synchronize(self.h))

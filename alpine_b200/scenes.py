@@ -122,3 +122,149 @@ def traversal_workload(n_tris=1 << 20, n_primary=(2048, 1024), n_incoherent=1 <<
     shadow = closest.copy()
     shadow[:, 7] = shadow_tmax(closest.shape[0], seed=seed + 2)
     return verts, idx, closest, shadow
+
+
+# ---------------------------------------------------------------------------
+# Rendering scenes. A scene is a dict:
+#   meshes:    list of {verts, idx, normals (or None), tri_material}
+#   materials: list of (kind, (r, g, b), roughness), kind 0 = dielectric, 1 = conductor
+#   lights:    list of ("disk", power, color, position, target, radius) |
+#                      ("point", power, color, position) |
+#                      ("quad", radiance, corner, edge_u, edge_v)
+#   camera:    (eye, target, up, fovy_radians)
+#   background (r, g, b)
+
+def box_mesh(lo, hi, inward=False):
+    """12-triangle axis-aligned box; normals (cross(e0, e1)) point outwards,
+    or inwards when inward=True."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float32)
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 4, 7, 3), (1, 2, 6, 5), (0, 1, 5, 4), (3, 7, 6, 2)]  # outward CCW
+    tris = []
+    for a, b, c, d in quads:
+        t1, t2 = (a, b, c), (a, c, d)
+        if inward:
+            t1, t2 = (a, c, b), (a, d, c)
+        tris += [t1, t2]
+    return v, np.array(tris, np.uint32)
+
+
+def rotate_y(v, angle, center):
+    c, s = math.cos(angle), math.sin(angle)
+    R = np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]], np.float64)
+    return ((v - center) @ R.T + center).astype(np.float32)
+
+
+def uv_sphere(center, radius, segments=64, bands=32):
+    """UV sphere with smooth per-vertex normals; pole bands are triangle fans."""
+    verts, norms = [], []
+    for j in range(bands + 1):
+        th = math.pi * j / bands
+        for i in range(segments):
+            ph = 2 * math.pi * i / segments
+            n = (math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph))
+            norms.append(n)
+            verts.append([center[k] + radius * n[k] for k in range(3)])
+    tris = []
+    idx = lambda j, i: j * segments + (i % segments)
+    for j in range(bands):
+        for i in range(segments):
+            a, b, c, d = idx(j, i), idx(j, i + 1), idx(j + 1, i + 1), idx(j + 1, i)
+            if j != 0:
+                tris.append((a, b, c))
+            if j != bands - 1:
+                tris.append((a, c, d))
+    return (np.array(verts, np.float32), np.array(tris, np.uint32), np.array(norms, np.float32))
+
+
+def room_scene(seed=1, light="disk", sphere_segments=64, sphere_bands=32):
+    """The small procedural room: a closed 2x2x2 box (inward normals), two
+    boxes rotated by a seeded angle in [0, pi/2), a UV sphere with smooth
+    normals, a 0.5 x 0.5 ceiling light of radiance 15. Walls and boxes are
+    Lambertian with albedo uniform in [0.2, 0.8]^3 (one box is a GGX
+    dielectric with roughness 0.3); the sphere is a GGX conductor with
+    roughness 0.3. light='disk' uses a disk light of equal area and power (the
+    reference has no quad light), light='quad' the quad itself."""
+    rng = np.random.default_rng(seed)
+    meshes, materials = [], []
+
+    def albedo():
+        return tuple(float(x) for x in rng.uniform(0.2, 0.8, 3))
+
+    rv, ri = box_mesh((-1, -1, -1), (1, 1, 1), inward=True)
+    wall_mats = []
+    for _ in range(6):
+        materials.append((0, albedo(), 1.0))
+        wall_mats.append(len(materials) - 1)
+    meshes.append({"verts": rv, "idx": ri, "normals": None,
+                   "tri_material": np.repeat(np.array(wall_mats, np.uint32), 2)})
+    for k, (lo, hi, rough) in enumerate([((-0.7, -1.0, -0.2), (-0.2, -0.2, 0.3), 1.0),
+                                         ((0.15, -1.0, 0.2), (0.65, -0.55, 0.7), 0.3)]):
+        bv, bi = box_mesh(lo, hi)
+        ang = float(rng.uniform(0, math.pi / 2))
+        ctr = (np.array(lo) + np.array(hi)) / 2
+        bv = rotate_y(bv, ang, ctr)
+        materials.append((0, albedo(), rough))
+        meshes.append({"verts": bv, "idx": bi, "normals": None,
+                       "tri_material": np.full(bi.shape[0], len(materials) - 1, np.uint32)})
+    sv, si, sn = uv_sphere((0.35, -0.25, -0.35), 0.3, sphere_segments, sphere_bands)
+    materials.append((1, (0.95, 0.75, 0.45), 0.3))
+    meshes.append({"verts": sv, "idx": si, "normals": sn,
+                   "tri_material": np.full(si.shape[0], len(materials) - 1, np.uint32)})
+    L, side = 15.0, 0.5
+    y = 0.999
+    if light == "quad":
+        # edges (side, 0, 0) x (0, 0, side): cross points down (-y), into the room
+        lights = [("quad", (L, L, L), (-0.25, y, -0.25), (side, 0.0, 0.0), (0.0, 0.0, side))]
+    else:
+        area = side * side
+        lights = [("disk", L * area * math.pi, (1.0, 1.0, 1.0), (0.0, y, 0.0), (0.0, 0.0, 0.0),
+                   math.sqrt(area / math.pi))]
+    camera = ((0.0, 0.0, -0.95), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), math.radians(70.0))
+    return {"meshes": meshes, "materials": materials, "lights": lights, "camera": camera,
+            "background": (0.0, 0.0, 0.0)}
+
+
+def add_random_lights(scene, n, seed=5, kinds=("disk", "point")):
+    """Adds n seeded disk / point lights spread over the room's ceiling half
+    (many-light sampler tests)."""
+    rng = np.random.default_rng(seed)
+    for i in range(n):
+        kind = kinds[i % len(kinds)]
+        pos = (float(rng.uniform(-0.9, 0.9)), float(rng.uniform(0.2, 0.95)), float(rng.uniform(-0.9, 0.9)))
+        color = tuple(float(x) for x in rng.uniform(0.3, 1.0, 3))
+        power = float(np.exp(rng.normal(0.0, 1.5)))
+        if kind == "disk":
+            tgt = (pos[0] + float(rng.normal(0, 0.3)), -1.0, pos[2] + float(rng.normal(0, 0.3)))
+            scene["lights"].append(("disk", power, color, pos, tgt, float(rng.uniform(0.02, 0.1))))
+        else:
+            scene["lights"].append(("point", power * 0.2, color, pos))
+    return scene
+
+
+def load_scene(target, scene, width, height):
+    """Loads a scene description into an alpine_b200 gpu.Context or an
+    oracle RefRenderer (same method names)."""
+    is_gpu = hasattr(target, "set_triangle_attributes")
+    if is_gpu:
+        target.reset_scene()
+        target.set_materials(scene["materials"])
+    for m in scene["meshes"]:
+        if is_gpu:
+            sid = target.add_mesh(m["verts"], m["idx"])
+            target.set_triangle_attributes(sid, m["normals"], m["tri_material"])
+        else:
+            target.add_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"])
+    for l in scene["lights"]:
+        if l[0] == "disk":
+            target.add_disk_light(*l[1:])
+        elif l[0] == "point":
+            target.add_point_light(*l[1:])
+        else:
+            target.add_quad_light(*l[1:])
+    eye, tgt, up, fovy = scene["camera"]
+    target.set_camera(eye, tgt, up, fovy, width / height)
+    target.set_background(*scene["background"])
+    target.build()

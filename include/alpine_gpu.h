@@ -151,6 +151,116 @@ ALPINE_GPU_API int alpine_gpu_trace_noalloc(alpine_gpu_ctx* ctx, const alpine_gp
 ALPINE_GPU_API int alpine_gpu_traversal_stats(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count,
                                               int any_hit, uint64_t* node_visits, uint64_t* triangle_visits);
 
+/* ---------------------------------------------------------------------------
+ * Rendering: the wavefront path tracer (alpine::render and its state,
+ * src/alpine.cpp:259-483). The framebuffer size and path length come from
+ * alpine_gpu_config (width, height, max_depth). */
+
+/* Materials (src/materials/): DIELECTRIC is a uniform mixture of Lambertian
+ * and GGX microfacet (F0 = 0.04), the latter only when 2 roughness^2 < 1
+ * (dielectric.cpp:15-20); CONDUCTOR is GGX microfacet with F0 = base colour
+ * (conductor.cpp:9-16). alpha = roughness, clamped to >= 0.001. The loaders
+ * create exactly these two (gltf_loader.cpp:404-414; OBJ files yield
+ * DIELECTRIC with roughness 1, obj_loader.cpp:73-75). */
+#define ALPINE_GPU_MATERIAL_DIELECTRIC 0u
+#define ALPINE_GPU_MATERIAL_CONDUCTOR 1u
+typedef struct alpine_gpu_material {
+    uint32_t kind;
+    float base_color[3];
+    float roughness;
+} alpine_gpu_material;
+
+/* Replaces the material table (the loaders' per-primitive Material objects,
+ * src/shapes/mesh.h:16-36). Material 0 is used by triangles without one. */
+ALPINE_GPU_API int alpine_gpu_set_materials(alpine_gpu_ctx* ctx, const alpine_gpu_material* materials,
+                                            uint32_t count);
+
+/* Per-vertex shading normals (float[3 * vertex_count], may be NULL: the
+ * geometric normal is used) and per-triangle material ids (may be NULL:
+ * material 0) of one mesh (Mesh::Data normals / materials,
+ * src/shapes/mesh.h:16-36; Mesh::getIntersectionAttributes, mesh.cpp:57-154). */
+ALPINE_GPU_API int alpine_gpu_set_triangle_attributes(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* normals,
+                                                      const uint32_t* triangle_material);
+
+/* Lights (alpine::addPointLight / addDiskLight, include/alpine/alpine.h:35-42;
+ * src/lights/). A quad light is a one-sided emitting parallelogram
+ * corner + [0,1] edge_u + [0,1] edge_v with constant radiance, emitting on the
+ * side of cross(edge_u, edge_v); it has no counterpart in the reference and
+ * follows DiskLight's sampling contract (src/lights/light.h:30-41). Lights are
+ * not visible to camera rays, as in the reference. */
+ALPINE_GPU_API int alpine_gpu_add_point_light(alpine_gpu_ctx* ctx, float power, const float color[3],
+                                              const float position[3], uint32_t* light_id);
+ALPINE_GPU_API int alpine_gpu_add_disk_light(alpine_gpu_ctx* ctx, float power, const float color[3],
+                                             const float position[3], const float target[3], float radius,
+                                             uint32_t* light_id);
+ALPINE_GPU_API int alpine_gpu_add_quad_light(alpine_gpu_ctx* ctx, const float radiance[3], const float corner[3],
+                                             const float edge_u[3], const float edge_v[3], uint32_t* light_id);
+/* LightHandle::setScale (include/alpine/light.h:6-7). Rebuild the light
+ * sampler afterwards for power- and BVH-based sampling. */
+ALPINE_GPU_API int alpine_gpu_set_light_scale(alpine_gpu_ctx* ctx, uint32_t light_id, float scale);
+
+/* alpine::buildLightSampler (alpine.h:44-51): call after all lights are added.
+ * Same numbering as LightSamplerType. */
+#define ALPINE_GPU_LIGHT_SAMPLER_UNIFORM 0
+#define ALPINE_GPU_LIGHT_SAMPLER_POWER 1
+#define ALPINE_GPU_LIGHT_SAMPLER_BVH 2
+ALPINE_GPU_API int alpine_gpu_build_light_sampler(alpine_gpu_ctx* ctx, int type);
+
+/* alpine::setBackgroundColor (alpine.h:53): radiance of rays that escape. */
+ALPINE_GPU_API int alpine_gpu_set_background(alpine_gpu_ctx* ctx, float r, float g, float b);
+
+/* CameraHandle::setLookAt (include/alpine/camera.h:6-12): pinhole camera,
+ * fovy in radians, film at distance 1. */
+ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3], const float target[3],
+                                         const float up[3], float fovy, float aspect);
+
+/* Render options (no counterpart in the reference's API).
+ * sampler: REFERENCE_STREAM reproduces the reference's per-pixel xorshift128
+ *   stream (src/sampler.cpp), drawn in the reference's order, one sample per
+ *   pixel at a time, with FP32 arithmetic rounded like the reference;
+ *   COUNTER (default) hashes (seed, pixel, sample, dimension), so all samples
+ *   of a pixel run in parallel and every run is deterministic.
+ * max_paths_per_wave: 0 = 2^21.
+ * russian_roulette_depth: 0 = off (the reference has none); d > 0 applies
+ *   roulette to continuations from depth d on (COUNTER sampler only).
+ * accumulate_fp64: per-pixel sums in FP64 (long convergence runs). */
+#define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
+#define ALPINE_GPU_SAMPLER_COUNTER 1u
+typedef struct alpine_gpu_render_options {
+    uint32_t sampler;
+    uint32_t max_paths_per_wave;
+    uint32_t russian_roulette_depth;
+    uint32_t seed;
+    uint32_t accumulate_fp64;
+} alpine_gpu_render_options;
+ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
+
+/* alpine::resetAccumulation (alpine.h:60): zero the sums, restart the
+ * per-pixel reference streams (Sampler::reset(pixel index)). */
+ALPINE_GPU_API int alpine_gpu_reset_accumulation(alpine_gpu_ctx* ctx);
+
+/* alpine::render(spp) (alpine.h:61, alpine.cpp:271-288): adds spp samples
+ * per pixel to the accumulation. Synchronous. */
+ALPINE_GPU_API int alpine_gpu_render(alpine_gpu_ctx* ctx, uint32_t spp);
+
+/* Per-pixel sums of colour, albedo and normal (9 floats per pixel, the
+ * reference's RenderTarget layout, src/denoisers/denoiser.h:7-12) and the
+ * number of samples accumulated. Either pointer may be NULL. */
+ALPINE_GPU_API int alpine_gpu_read_accumulation(alpine_gpu_ctx* ctx, float* sums, uint32_t* total_samples);
+ALPINE_GPU_API int alpine_gpu_read_accumulation_f64(alpine_gpu_ctx* ctx, double* sums, uint32_t* total_samples);
+
+/* alpine::postProcess + getFrameBuffer (alpine.h:63-65, alpine.cpp:446-483)
+ * without the denoiser: mean colour (3 floats per pixel, may be NULL) and the
+ * tone-mapped (ACES when tonemap != 0), clamped, sRGB-encoded 8-bit image
+ * (3 bytes per pixel, may be NULL). */
+ALPINE_GPU_API int alpine_gpu_post_process(alpine_gpu_ctx* ctx, int tonemap, float* mean_rgb, uint8_t* rgb8);
+
+/* Per-pixel state of the reference random stream (4 words per pixel, the
+ * reference's Sampler state, src/sampler.h; src/alpine.cpp:108), as left by
+ * the last render in REFERENCE_STREAM mode. For parity checks of the draw
+ * order. */
+ALPINE_GPU_API int alpine_gpu_read_sampler_state(alpine_gpu_ctx* ctx, uint32_t* state);
+
 /* Waits for all work of the context and reports device-side errors. */
 ALPINE_GPU_API int alpine_gpu_synchronize(alpine_gpu_ctx* ctx);
 

@@ -96,6 +96,7 @@ def ref():
         L.ref_render_load_obj.restype = C.c_int
         L.ref_render_add_disk_light.argtypes = [C.c_float, _f32p, _f32p, _f32p, C.c_float]
         L.ref_render_add_point_light.argtypes = [C.c_float, _f32p, _f32p]
+        L.ref_render_add_quad_light.argtypes = [_f32p, _f32p, _f32p, _f32p]
         L.ref_render_update_scene.argtypes = [C.c_float]
         L.ref_render_build_light_sampler.argtypes = [C.c_int]
         L.ref_render_set_background.argtypes = [C.c_float, C.c_float, C.c_float]
@@ -105,6 +106,7 @@ def ref():
         L.ref_render_read_accum.argtypes = [_f32p]
         L.ref_render_read_accum.restype = C.c_uint32
         L.ref_render_post_process.argtypes = [C.c_int, _u8p]
+        L.ref_render_read_sampler_state.argtypes = [_u32p]
         _ref = L
     return _ref
 
@@ -197,6 +199,82 @@ class OracleBvh:
         if getattr(self, "h", None):
             lib().orc_bvh_destroy(self.h)
             self.h = None
+
+
+class RefRenderer:
+    """The reference integrator (class Alpine, src/alpine.cpp) through the
+    harness: one process-wide instance, as the reference is a singleton."""
+
+    ACC_BVH, ACC_WIDE_BVH = 0, 1
+
+    def __init__(self, width, height, max_depth, accelerator=ACC_BVH, arena_bytes=1 << 30):
+        self.L = ref()
+        self.w, self.h = width, height
+        if not self.L.ref_render_init(width, height, max_depth, arena_bytes):
+            raise RuntimeError("ref_render_init failed")
+        self.L.ref_render_reset_scene(accelerator)
+
+    def add_mesh(self, verts, idx, normals=None, tri_material=None, materials=((0, (0.5, 0.5, 0.5), 1.0),)):
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        i = np.ascontiguousarray(idx, np.uint32).reshape(-1)
+        nt = i.size // 3
+        tm = np.zeros(nt, np.uint32) if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
+        mats = np.array([[k, *c, r] for k, c, r in materials], np.float32).reshape(-1)
+        nptr = None
+        if normals is not None:
+            self._normals = np.ascontiguousarray(normals, np.float32).reshape(-1)
+            nptr = self._normals.ctypes.data
+        if not self.L.ref_render_add_mesh(v, v.size // 3, i, nt, nptr, tm, mats, len(materials)):
+            raise RuntimeError("ref_render_add_mesh failed")
+
+    def add_disk_light(self, power, color, position, target, radius):
+        self.L.ref_render_add_disk_light(power, np.asarray(color, np.float32), np.asarray(position, np.float32),
+                                         np.asarray(target, np.float32), radius)
+
+    def add_point_light(self, power, color, position):
+        self.L.ref_render_add_point_light(power, np.asarray(color, np.float32), np.asarray(position, np.float32))
+
+    def add_quad_light(self, radiance, corner, edge_u, edge_v):
+        """The oracle's project-written QuadLight (not in the reference)."""
+        self.L.ref_render_add_quad_light(np.asarray(radiance, np.float32), np.asarray(corner, np.float32),
+                                         np.asarray(edge_u, np.float32), np.asarray(edge_v, np.float32))
+
+    def build(self):
+        self.L.ref_render_update_scene(0.0)
+
+    def build_light_sampler(self, kind):
+        self.L.ref_render_build_light_sampler(kind)
+
+    def set_background(self, r, g, b):
+        self.L.ref_render_set_background(r, g, b)
+
+    def set_camera(self, eye, target, up, fovy, aspect):
+        self.L.ref_render_set_camera(np.asarray(eye, np.float32), np.asarray(target, np.float32),
+                                     np.asarray(up, np.float32), fovy, aspect)
+
+    def reset_accumulation(self):
+        self.L.ref_render_reset_accumulation()
+
+    def render(self, spp):
+        return self.L.ref_render(spp)
+
+    def read_accumulation(self):
+        out = np.empty((self.h, self.w, 9), np.float32)
+        n = self.L.ref_render_read_accum(out.reshape(-1))
+        return out, n
+
+    def post_process(self, tonemap=True):
+        out = np.empty((self.h, self.w, 3), np.uint8)
+        self.L.ref_render_post_process(int(tonemap), out.reshape(-1))
+        return out
+
+    def read_sampler_state(self):
+        out = np.empty((self.h, self.w, 4), np.uint32)
+        self.L.ref_render_read_sampler_state(out.reshape(-1))
+        return out
+
+    def close(self):
+        self.L.ref_render_shutdown()
 
 
 class RefAccel:

@@ -173,6 +173,62 @@ loadHdr(std::unique_ptr<EnvironmentMap>&, std::string_view)
 using namespace alpine;
 
 namespace {
+// Project-written oracle light (the reference has point and disk lights only):
+// a one-sided parallelogram corner + u * edgeU + v * edgeV of constant
+// radiance, emitting on the side of cross(edgeU, edgeV), following the
+// DiskLight contract (src/lights/disk_light.cpp:30-81): area sampling with
+// pdf = d^2 / (A cos), computePdf by ray/plane intersection.
+class QuadLight final : public Light
+{
+public:
+    QuadLight(const float3& radiance, const float3& corner, const float3& eu, const float3& ev)
+        : mRadiance(radiance), mEu(eu), mEv(ev)
+    {
+        mPosition = corner;
+        float3 n = cross(eu, ev);
+        mArea = length(n);
+        mNormal = n / mArea;
+        float3 c[4] = {corner, corner + eu, corner + ev, corner + eu + ev};
+        for (const auto& p : c) { mBbox = merge(mBbox, BoundingBox{p, p}); }
+    }
+
+    std::optional<Sample> sample(const float2& u, const float3& hit) const override
+    {
+        float3 p = mPosition + mEu * u.x + mEv * u.y;
+        float3 wi = p - hit;
+        float d = length(wi);
+        if (d == 0.0f) { return {}; }
+        wi /= d;
+        float c = std::max(0.0f, dot(-wi, mNormal));
+        if (c == 0.0f) { return {}; }
+        return Sample{mRadiance * mScale, wi, d, (d * d) / (mArea * c)};
+    }
+
+    std::pair<float, float> computePdf(const float3& hit, const float3& wi) const override
+    {
+        float c = std::max(0.0f, dot(-wi, mNormal));
+        if (c == 0.0f) { return {0.0f, 0.0f}; }
+        float dist = dot(hit - mPosition, mNormal) / c;
+        if (dist < 0.0f) { return {0.0f, 0.0f}; }
+        float3 q = hit + wi * dist - mPosition;
+        float su = dot(q, mEu) / dot(mEu, mEu);
+        float sv = dot(q, mEv) / dot(mEv, mEv);
+        bool inside = su >= 0.0f && su <= 1.0f && sv >= 0.0f && sv <= 1.0f;
+        if (inside && c > 0.0f) { return {(dist * dist) / (mArea * c), dist}; }
+        return {0.0f, 0.0f};
+    }
+
+    float3 getEmittedRadiance() const override { return mRadiance * mScale; }
+    float3 getPower() const override { return mRadiance * (mArea * std::numbers::pi_v<float>) * mScale; }
+    bool isDelta() const override { return false; }
+    BoundingBox getBoundingBox() const override { return mBbox; }
+
+private:
+    float3 mRadiance, mEu, mEv, mNormal;
+    float mArea = 0.0f;
+    BoundingBox mBbox;
+};
+
 struct RefAccel
 {
     std::vector<std::byte> arena;
@@ -355,6 +411,13 @@ ref_render_add_disk_light(float power, const float* color, const float* pos, con
 }
 
 void ref_render_add_point_light(float power, const float* color, const float* pos) { addPointLight(power, color, pos); }
+
+void
+ref_render_add_quad_light(const float* radiance, const float* corner, const float* eu, const float* ev)
+{
+    alpine::alpine().mScene.lights.push_back(std::make_shared<QuadLight>(
+        float3(radiance), float3(corner), float3(eu), float3(ev)));
+}
 void ref_render_update_scene(float time) { updateScene(time); }
 void ref_render_build_light_sampler(int type) { buildLightSampler(static_cast<LightSamplerType>(type)); }
 void ref_render_set_background(float r, float g, float b) { setBackgroundColor(r, g, b); }
@@ -399,6 +462,15 @@ ref_render_post_process(int tonemap, uint8_t* rgb)
     postProcess(false, tonemap != 0);
     auto& a = alpine::alpine();
     std::memcpy(rgb, getFrameBuffer(), a.mFrameBuffer.size() * 3);
+}
+
+// Per-pixel sampler state (Sampler::mSeed, src/sampler.h), 4 words per pixel.
+void
+ref_render_read_sampler_state(uint32_t* out)
+{
+    auto& a = alpine::alpine();
+    for (size_t i = 0; i < a.mSamplers.size(); ++i)
+        for (int k = 0; k < 4; ++k) out[4 * i + k] = a.mSamplers[i].mSeed[k];
 }
 
 void ref_render_shutdown() { shutdown(); }
