@@ -3,6 +3,7 @@
 
 #include "../../include/alpine_gpu.h"
 #include "build.cuh"
+#include "guide_host.cuh"
 #include "shading.cuh"
 
 #include <string>
@@ -98,6 +99,11 @@ struct alpine_gpu_ctx {
     uint32_t totalSamples = 0;
     ag::DeviceBuffer dWave;
     uint32_t waveCapacity = 0;
+
+    // learned path guiding
+    ag::guide::Guide guide;
+    uint32_t guideSeed = 1;
+    bool guideBoxSet = false;
 
     // Reads and clears the device status word (stream must be idle).
     int check_device_status()

@@ -1,0 +1,83 @@
+// Host-side interface of the learned guide (parameters, inference, training).
+#pragma once
+
+#include "guide.cuh"
+
+namespace ag {
+namespace guide {
+
+// One inference query: the shading position, roughness, outgoing direction
+// (world space, towards the previous vertex) and shading normal. 48 bytes.
+struct Query {
+    float pos[3];
+    float rough;
+    float wo[3];
+    float pad0;
+    float n[3];
+    float pad1;
+};
+static_assert(sizeof(Query) == 48, "Query layout");
+
+// One training sample: query, sampled incident direction and the weight of
+// the KL gradient (incident radiance luminance / sampling pdf). 64 bytes.
+struct Sample {
+    Query q;
+    float dir[3];
+    float weight;
+};
+static_assert(sizeof(Sample) == 64, "Sample layout");
+
+class Guide {
+public:
+    Guide() = default;
+    ~Guide();
+    Guide(const Guide&) = delete;
+    Guide& operator=(const Guide&) = delete;
+
+    // (Re)initialises all parameters deterministically from `seed`.
+    int reset(uint32_t seed, cudaStream_t st);
+    bool ready() const { return ready_; }
+    void set_scene_box(float3 lo, float3 hi);
+    Params params() const;
+    // raw: n x 40 fp32 mixture parameters.
+    void infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const;
+    // Adds the gradient of the batch (mean loss, scaled by invBatch) to the
+    // gradient buffers, without an update.
+    void accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st);
+    void apply_adam(float lr, cudaStream_t st);
+    // gradients + Adam; returns the batch loss (synchronises).
+    float train_step(const Sample* s, uint32_t n, float lr, cudaStream_t st);
+    // Recomputes the BF16 / FP16 compute copies from the FP32 masters.
+    void publish(cudaStream_t st);
+
+    float* weight_master() const { return wP_; }
+    float* weight_grad() const { return wG_; }
+    float* grid_master() const { return gridP_; }
+    float* grid_grad() const { return gridG_; }
+    uint32_t steps() const { return step_; }
+
+private:
+    bool allocate();
+    void release();
+
+    void* mem_ = nullptr;
+    bool ready_ = false;
+    uint32_t step_ = 0;
+    float* gridP_ = nullptr;
+    float* gridM_ = nullptr;
+    float* gridV_ = nullptr;
+    float* gridG_ = nullptr;
+    __half* gridH_ = nullptr;
+    float* wP_ = nullptr;
+    float* wM_ = nullptr;
+    float* wV_ = nullptr;
+    float* wG_ = nullptr;
+    __nv_bfloat16* wB_ = nullptr;
+    __nv_bfloat16* wT_ = nullptr;
+    float* loss_ = nullptr;
+    float3 bmin_ = make_float3(0.0f, 0.0f, 0.0f);
+    float3 invExtent_ = make_float3(1.0f, 1.0f, 1.0f);
+};
+
+}  // namespace guide
+}  // namespace ag

@@ -106,6 +106,15 @@ def lib():
         L.alpine_gpu_read_accumulation_f64.argtypes = [vp, vp, u32p]
         L.alpine_gpu_post_process.argtypes = [vp, C.c_int, vp, vp]
         L.alpine_gpu_read_sampler_state.argtypes = [vp, vp]
+        L.alpine_gpu_guide_dims.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32p]
+        L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
+        L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
+        L.alpine_gpu_guide_gradients.argtypes = [vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp]
+        L.alpine_gpu_guide_train.argtypes = [vp, vp, C.c_uint32, C.c_float, f3]
+        L.alpine_gpu_guide_get_weights.argtypes = [vp, vp]
+        L.alpine_gpu_guide_set_weights.argtypes = [vp, vp]
+        L.alpine_gpu_guide_grid.argtypes = [vp, vp, C.c_uint32, vp, vp]
+        L.alpine_gpu_guide_sample_mixture.argtypes = [vp, vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_traversal_stats.argtypes = [vp, vp, C.c_uint64, C.c_int, C.POINTER(C.c_uint64),
                                                  C.POINTER(C.c_uint64)]
         _lib = L
@@ -271,6 +280,64 @@ class Context:
         ldr = np.empty((height, width, 3), np.uint8)
         self._check(self.L.alpine_gpu_post_process(self.h, int(tonemap), _ptr(mean), _ptr(ldr)))
         return mean, ldr
+
+    # ---- learned guide ----------------------------------------------------
+    def guide_dims(self):
+        wc, gp, ts = C.c_uint32(), C.c_uint64(), C.c_uint32()
+        res = (C.c_uint32 * 16)()
+        self._check(self.L.alpine_gpu_guide_dims(C.byref(wc), C.byref(gp), C.byref(ts), res))
+        return {"weights": wc.value, "grid_params": gp.value, "table_size": ts.value, "res": list(res)}
+
+    def guide_reset(self, seed, lo, hi):
+        self._check(self.L.alpine_gpu_guide_reset(self.h, seed, _f3(lo), _f3(hi)))
+
+    def guide_infer(self, queries):
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 12)
+        raw = np.empty((q.shape[0], 40), np.float32)
+        self._check(self.L.alpine_gpu_guide_infer(self.h, _ptr(q), q.shape[0], _ptr(raw)))
+        return raw
+
+    def guide_gradients(self, samples, grid_index=None):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        dW = np.empty(self.guide_dims()["weights"], np.float32)
+        gi = None if grid_index is None else np.ascontiguousarray(grid_index, np.uint64)
+        gg = None if gi is None else np.empty(gi.size, np.float32)
+        self._check(self.L.alpine_gpu_guide_gradients(self.h, _ptr(s), s.shape[0], _ptr(dW),
+                                                      None if gi is None else _ptr(gi), 0 if gi is None else gi.size,
+                                                      None if gg is None else _ptr(gg), None))
+        return dW, gg
+
+    def guide_train(self, samples, lr=1e-2):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        loss = (C.c_float * 3)()
+        self._check(self.L.alpine_gpu_guide_train(self.h, _ptr(s), s.shape[0], lr, loss))
+        return loss[0]
+
+    def guide_get_weights(self):
+        w = np.empty(self.guide_dims()["weights"], np.float32)
+        self._check(self.L.alpine_gpu_guide_get_weights(self.h, _ptr(w)))
+        return w
+
+    def guide_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self.L.alpine_gpu_guide_set_weights(self.h, _ptr(w)))
+
+    def guide_grid(self, index, write=None):
+        idx = np.ascontiguousarray(index, np.uint64)
+        out = np.empty(idx.size, np.float32)
+        wv = None if write is None else np.ascontiguousarray(write, np.float32)
+        self._check(self.L.alpine_gpu_guide_grid(self.h, _ptr(idx), idx.size, _ptr(out),
+                                                 None if wv is None else _ptr(wv)))
+        return out
+
+    def guide_sample_mixture(self, raw, u):
+        r = np.ascontiguousarray(raw, np.float32).reshape(40)
+        uu = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+        dirs = np.empty((uu.shape[0], 3), np.float32)
+        pdfs = np.empty(uu.shape[0], np.float32)
+        self._check(self.L.alpine_gpu_guide_sample_mixture(self.h, _ptr(r), _ptr(uu), uu.shape[0], _ptr(dirs),
+                                                           _ptr(pdfs)))
+        return dirs, pdfs
 
     def synchronize(self):
         self._check(self.L.alpine_gpu_synchronize(self.h))

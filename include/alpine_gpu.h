@@ -255,6 +255,31 @@ ALPINE_GPU_API int alpine_gpu_read_accumulation_f64(alpine_gpu_ctx* ctx, double*
  * (3 bytes per pixel, may be NULL). */
 ALPINE_GPU_API int alpine_gpu_post_process(alpine_gpu_ctx* ctx, int tonemap, float* mean_rgb, uint8_t* rgb8);
 
+/* ---------------------------------------------------------------------------
+ * Learned path guiding (no counterpart in the reference): a hash-grid encoded
+ * MLP predicting an 8-lobe von Mises-Fisher mixture over incident directions,
+ * trained online. These entry points expose the model for tests and tools;
+ * the integrator uses it through alpine_gpu_set_guiding.
+ * Query record: 12 floats {pos[3], roughness, wo[3], 0, normal[3], 0}.
+ * Sample record: 16 floats {query[12], dir[3], weight}.
+ * Raw output: 40 floats = 8 lobes x {direction[3], log kappa, logit}. */
+ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_params, uint32_t* table_size,
+                                         uint32_t* resolutions);
+ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],
+                                          const float scene_hi[3]);
+ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw);
+ALPINE_GPU_API int alpine_gpu_guide_gradients(alpine_gpu_ctx* ctx, const float* samples, uint32_t count, float* dW,
+                                              const uint64_t* grid_index, uint32_t grid_count, float* grid_grad,
+                                              float* loss);
+ALPINE_GPU_API int alpine_gpu_guide_train(alpine_gpu_ctx* ctx, const float* samples, uint32_t count, float lr,
+                                          float* loss);
+ALPINE_GPU_API int alpine_gpu_guide_get_weights(alpine_gpu_ctx* ctx, float* weights);
+ALPINE_GPU_API int alpine_gpu_guide_set_weights(alpine_gpu_ctx* ctx, const float* weights);
+ALPINE_GPU_API int alpine_gpu_guide_grid(alpine_gpu_ctx* ctx, const uint64_t* index, uint32_t count, float* read,
+                                         const float* write);
+ALPINE_GPU_API int alpine_gpu_guide_sample_mixture(alpine_gpu_ctx* ctx, const float* raw, const float* u,
+                                                   uint32_t count, float* dirs, float* pdfs);
+
 /* Per-pixel state of the reference random stream (4 words per pixel, the
  * reference's Sampler state, src/sampler.h; src/alpine.cpp:108), as left by
  * the last render in REFERENCE_STREAM mode. For parity checks of the draw

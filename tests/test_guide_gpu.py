@@ -1,0 +1,147 @@
+"""GPU tests of the learned guide: BF16 tensor-core inference and training
+kernels against the FP64 oracle (oracle/guide_ref.py)."""
+import math
+
+import numpy as np
+import pytest
+
+from alpine_b200 import gpu
+from oracle import guide_ref as G
+
+pytestmark = pytest.mark.gpu
+
+LO, HI = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+
+
+def _queries(n, seed):
+    rng = np.random.default_rng(seed)
+    q = np.zeros((n, 12), np.float32)
+    q[:, 0:3] = rng.uniform(-1, 1, (n, 3))
+    q[:, 3] = rng.uniform(0.02, 1.0, n)
+    wo = rng.normal(size=(n, 3))
+    q[:, 4:7] = wo / np.linalg.norm(wo, axis=1, keepdims=True)
+    nn = rng.normal(size=(n, 3))
+    q[:, 8:11] = nn / np.linalg.norm(nn, axis=1, keepdims=True)
+    return q
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = gpu.Context(0)
+    c.guide_reset(7, LO, HI)
+    yield c
+    c.close()
+
+
+def _randomise(ctx, q, seed):
+    """Random weights and random grid values at the entries the queries touch."""
+    rng = np.random.default_rng(seed)
+    w = np.concatenate([rng.uniform(-1, 1, G.layer_out(l) * G.layer_in(l)) * math.sqrt(6.0 / G.layer_in(l))
+                        for l in range(G.LAYERS)]).astype(np.float32)
+    ctx.guide_set_weights(w)
+    res = G.resolutions()
+    idx = G.grid_flat_indices(q, LO, HI, res)
+    vals = rng.uniform(-1, 1, idx.size).astype(np.float32)
+    ctx.guide_grid(idx, write=vals)
+    table = dict(zip(idx.tolist(), vals.tolist()))
+    return w, res, (lambda flat: np.array([table[int(i)] for i in flat]))
+
+
+def test_dims_match_oracle(ctx):
+    d = ctx.guide_dims()
+    assert d["weights"] == G.WEIGHT_COUNT
+    assert d["table_size"] == G.T
+    assert d["res"] == G.resolutions()
+
+
+def test_inference_matches_oracle(ctx):
+    q = _queries(1000, 1)
+    w, res, lookup = _randomise(ctx, q, 2)
+    raw = ctx.guide_infer(q)
+    X = G.encode(q, LO, HI, res, lookup, half=True)
+    ref, _ = G.forward(X, G.unpack(w), emulate_bf16=True)
+    err = np.linalg.norm(raw - ref[:, :40]) / np.linalg.norm(ref[:, :40])
+    print(f"inference relative L2 error vs BF16-emulated FP64 oracle: {err:.2e}")
+    assert err < 2e-2
+
+
+def test_gradients_match_oracle(ctx):
+    q = _queries(2048, 3)
+    w, res, lookup = _randomise(ctx, q, 4)
+    rng = np.random.default_rng(5)
+    d = rng.normal(size=(q.shape[0], 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    weight = rng.uniform(0.2, 3.0, q.shape[0])
+    samples = np.concatenate([q, d, weight[:, None]], axis=1).astype(np.float32)
+    gidx = G.grid_flat_indices(q[:64], LO, HI, res)
+    dW, gg = ctx.guide_gradients(samples, gidx)
+    Ws = G.unpack(w)
+    X = G.encode(q, LO, HI, res, lookup, half=True)
+    raw, acts = G.forward(X, Ws, emulate_bf16=True)
+    dWs, dX = G.backward(acts, [G.bf16(W) for W in Ws], G.output_grad(raw, d, weight / q.shape[0]))
+    ref = np.concatenate([x.reshape(-1) for x in dWs])
+    err = np.linalg.norm(dW - ref) / np.linalg.norm(ref)
+    cos = float(dW @ ref / (np.linalg.norm(dW) * np.linalg.norm(ref)))
+    print(f"weight gradient: relative L2 error {err:.2e}, cosine {cos:.6f}")
+    assert err < 5e-2 and cos > 0.998
+    # grid gradient at the entries of the first 64 queries: scatter the oracle's
+    # input gradient with the trilinear weights
+    p = G.normalise(q[:, 0:3], LO, HI)
+    gref = {}
+    for l in range(G.LEVELS):
+        idx, cw = G.corners(p, res[l])
+        base = (np.uint64(l) * np.uint64(G.T) + idx) * np.uint64(2)
+        for f in range(2):
+            contrib = cw * dX[:, 2 * l + f][:, None]
+            for i, c in zip((base + np.uint64(f)).reshape(-1).tolist(), contrib.reshape(-1).tolist()):
+                gref[i] = gref.get(i, 0.0) + c
+    gr = np.array([gref.get(int(i), 0.0) for i in gidx])
+    gerr = np.linalg.norm(gg - gr) / np.linalg.norm(gr)
+    print(f"grid gradient: relative L2 error {gerr:.2e} over {gidx.size} parameters")
+    assert gerr < 5e-2
+
+
+def test_mixture_sampling(ctx):
+    rng = np.random.default_rng(6)
+    raw = rng.normal(size=40).astype(np.float32)
+    raw[3::5] = rng.uniform(0.0, 4.0, 8)
+    u = rng.random((1 << 18, 3)).astype(np.float32)
+    dirs, pdfs = ctx.guide_sample_mixture(raw, u)
+    assert np.allclose(np.linalg.norm(dirs, axis=1), 1.0, atol=1e-4)
+    ref = G.mixture_pdf(np.repeat(raw[None, :], dirs.shape[0], 0), dirs)
+    assert np.allclose(pdfs, ref, rtol=2e-3, atol=1e-6)
+    # E[1/q] over q-distributed directions is the area of the sphere
+    est = np.mean(1.0 / pdfs.astype(np.float64))
+    se = np.std(1.0 / pdfs.astype(np.float64)) / math.sqrt(pdfs.size)
+    assert abs(est - 4 * math.pi) < 5 * se + 1e-3
+
+
+def test_training_learns_a_target_distribution(ctx):
+    """Directions drawn around mu(x) = normalize(x - c): the trained mixture
+    concentrates its density there (online Adam, lr 1e-2, batches of 4096)."""
+    ctx.guide_reset(11, LO, HI)
+    rng = np.random.default_rng(7)
+    c = np.array([0.3, -0.2, 0.1])
+
+    def batch(n):
+        q = _queries(n, int(rng.integers(1 << 30)))
+        mu = q[:, 0:3] - c
+        mu /= np.linalg.norm(mu, axis=1, keepdims=True)
+        d = mu + 0.15 * rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        return np.concatenate([q, d, np.ones((n, 1))], axis=1).astype(np.float32), mu
+
+    first = None
+    for it in range(300):
+        s, _ = batch(4096)
+        loss = ctx.guide_train(s, 1e-2)
+        first = loss if first is None else first
+    s, mu = batch(2048)
+    raw = ctx.guide_infer(s[:, :12])
+    p_mode = G.mixture_pdf(raw, mu)
+    p_anti = G.mixture_pdf(raw, -mu)
+    print(f"training: loss {first:.3f} -> {loss:.3f}; median pdf at target mode {np.median(p_mode):.2f}, "
+          f"opposite {np.median(p_anti):.4f}, uniform {1 / (4 * math.pi):.4f}")
+    assert loss < first - 1.0
+    assert np.median(p_mode) > 10 / (4 * math.pi)
+    assert np.median(p_anti) < 1 / (4 * math.pi)
