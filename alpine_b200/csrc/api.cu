@@ -170,7 +170,7 @@ int alpine_gpu_create(const alpine_gpu_config* cfg, alpine_gpu_ctx** out)
     for (int i = 0; i < ag::kCopyStreams && e == cudaSuccess; ++i)
         e = cudaStreamCreateWithFlags(&c->copyStreams[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->dStatus, sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMallocHost(&c->hStatus, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->hStatus, 16 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(c->dStatus, 0, sizeof(uint32_t));
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -42,6 +42,25 @@ struct DeviceBuffer {
 
 constexpr int kCopyStreams = 4;
 
+// A material record of the C ABI as the device Material: Dielectric or
+// Conductor with alpha = roughness (gltf_loader.cpp:404-414), alpha clamped
+// to 0.001 (microfacet.h:9-12); a Dielectric adds the microfacet lobe when
+// dot(alpha, alpha) < 1 (dielectric.cpp:15-27). False for an unknown kind.
+inline bool make_material(const alpine_gpu_material& in, Material& x)
+{
+    if (in.kind != ALPINE_GPU_MATERIAL_DIELECTRIC && in.kind != ALPINE_GPU_MATERIAL_CONDUCTOR) return false;
+    x = Material{};
+    x.kind = in.kind == ALPINE_GPU_MATERIAL_CONDUCTOR ? kMatConductor : kMatDielectric;
+    x.r = in.base_color[0];
+    x.g = in.base_color[1];
+    x.b = in.base_color[2];
+    const float a = in.roughness;
+    x.ax = a > 0.001f ? a : 0.001f;
+    x.ay = x.ax;
+    x.lobes = (a * a + a * a < 1.0f) ? 2u : 1u;
+    return true;
+}
+
 }  // namespace ag
 
 struct alpine_gpu_ctx {
@@ -66,6 +85,7 @@ struct alpine_gpu_ctx {
     alpine_gpu_bvh_stats stats{};
 
     // device status word (DeviceError bits) and its pinned host mirror
+    // (16 words: [0] status, [1..] small read-backs)
     uint32_t* dStatus = nullptr;
     uint32_t* hStatus = nullptr;
 
@@ -104,6 +124,10 @@ struct alpine_gpu_ctx {
     ag::guide::Guide guide;
     uint32_t guideSeed = 1;
     bool guideBoxSet = false;
+    ag::DeviceBuffer dGuideWave;     // queries, mixture parameters, training records
+    uint32_t guideWavePaths = 0, guideTrainCap = 0;
+    uint32_t guideWaveIndex = 0;     // waves rendered with guiding (record selection hash)
+    float guideLastLoss = 0.0f;
 
     // Reads and clears the device status word (stream must be idle).
     int check_device_status()

@@ -68,9 +68,11 @@ AG_D void forward32(const __nv_bfloat16* W, __nv_bfloat16* X, __nv_bfloat16* tmp
     __syncwarp();
 }
 
+// n queries, or *nDev when nDev is not null (a queue length written on the device).
 __global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Query* __restrict__ q, uint32_t n,
-                                                          float* __restrict__ raw)
+                                                          const uint32_t* __restrict__ nDev, float* __restrict__ raw)
 {
+    if (nDev) n = min(n, *nDev);
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -99,7 +101,9 @@ __global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Quer
 // Training: forward with saved activations, mixture gradient, backward with
 // tensor cores; dW accumulated per block in shared memory then merged into
 // the global gradient with atomics; grid gradients scattered with atomics.
+// Sample i of the batch is s[offset + i * stride].
 __global__ void __launch_bounds__(32 * kTrainWarps) k_train(Params g, const Sample* __restrict__ s, uint32_t n,
+                                                          uint32_t offset, uint32_t stride,
                                                           float invBatch, float* __restrict__ dW,
                                                           float* __restrict__ dGrid, float* __restrict__ loss)
 {
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) k_train(Params g, const Samp
         const uint32_t i = ch * 32 + lane;
         const bool valid = i < n;
         Sample smp;
-        if (valid) smp = s[i];
+        if (valid) smp = s[offset + (uint64_t)i * stride];
         __nv_bfloat16* X0 = saved;  // the encoded input is layer 0's saved input
         if (valid) encode_row(g, smp.q, X0 + lane * kHidden);
         else
@@ -412,32 +416,29 @@ Params Guide::params() const
     return p;
 }
 
-void Guide::infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const
+void Guide::infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const { infer_queue(q, nullptr, n, raw, st); }
+
+void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st) const
 {
-    if (n == 0) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
-        attr = true;
-    }
-    uint32_t chunks = (n + 31) / 32;
+    if (maxN == 0) return;
+    // per call: the attribute belongs to the current device
+    cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
+    uint32_t chunks = (maxN + 31) / 32;
     uint32_t blocks = (chunks + kInferWarps - 1) / kInferWarps;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    k_infer<<<blocks, 32 * kInferWarps, infer_smem(), st>>>(params(), q, n, raw);
+    k_infer<<<blocks, 32 * kInferWarps, infer_smem(), st>>>(params(), q, maxN, count, raw);
 }
 
-void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st)
+void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset,
+                                 uint32_t stride)
 {
     if (n == 0) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
-        attr = true;
-    }
+    cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
     uint32_t chunks = (n + 31) / 32;
     uint32_t blocks = (chunks + kTrainWarps - 1) / kTrainWarps;
     if (blocks > 148 * 4) blocks = 148 * 4;
-    k_train<<<blocks, 32 * kTrainWarps, train_smem(), st>>>(params(), s, n, invBatch, wG_, gridG_, loss_);
+    k_train<<<blocks, 32 * kTrainWarps, train_smem(), st>>>(params(), s, n, offset, stride, invBatch, wG_, gridG_,
+                                                            loss_);
 }
 
 void Guide::apply_adam(float lr, cudaStream_t st)

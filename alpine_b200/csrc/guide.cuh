@@ -59,6 +59,27 @@ struct Params {
     uint32_t res[kLevels];         // grid resolution per level
 };
 
+// One inference query: the shading position, roughness, outgoing direction
+// (world space, towards the previous vertex) and shading normal. 48 bytes.
+struct Query {
+    float pos[3];
+    float rough;
+    float wo[3];
+    float pad0;
+    float n[3];
+    float pad1;
+};
+static_assert(sizeof(Query) == 48, "Query layout");
+
+// One training sample: query, sampled incident direction and the weight of
+// the KL gradient (incident radiance luminance / sampling pdf). 64 bytes.
+struct Sample {
+    Query q;
+    float dir[3];
+    float weight;
+};
+static_assert(sizeof(Sample) == 64, "Sample layout");
+
 // ---------------------------------------------------------------------------
 // Hash-grid encoding.
 AG_HD uint32_t grid_index(uint32_t res, uint32_t x, uint32_t y, uint32_t z)

@@ -74,6 +74,14 @@ int alpine_gpu_guide_reset(alpine_gpu_ctx* c, uint32_t seed, const float lo[3], 
     return ALPINE_GPU_OK;
 }
 
+int alpine_gpu_guide_steps(alpine_gpu_ctx* c, uint32_t* adam_steps, uint32_t* guided_waves)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (adam_steps) *adam_steps = c->guide.steps();
+    if (guided_waves) *guided_waves = c->guideWaveIndex;
+    return ALPINE_GPU_OK;
+}
+
 int alpine_gpu_guide_infer(alpine_gpu_ctx* c, const float* queries, uint32_t n, float* raw)
 {
     if (!c || (n && (!queries || !raw))) return ALPINE_GPU_ERR_INVALID_ARGUMENT;

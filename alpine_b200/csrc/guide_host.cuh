@@ -6,27 +6,6 @@
 namespace ag {
 namespace guide {
 
-// One inference query: the shading position, roughness, outgoing direction
-// (world space, towards the previous vertex) and shading normal. 48 bytes.
-struct Query {
-    float pos[3];
-    float rough;
-    float wo[3];
-    float pad0;
-    float n[3];
-    float pad1;
-};
-static_assert(sizeof(Query) == 48, "Query layout");
-
-// One training sample: query, sampled incident direction and the weight of
-// the KL gradient (incident radiance luminance / sampling pdf). 64 bytes.
-struct Sample {
-    Query q;
-    float dir[3];
-    float weight;
-};
-static_assert(sizeof(Sample) == 64, "Sample layout");
-
 class Guide {
 public:
     Guide() = default;
@@ -41,9 +20,12 @@ public:
     Params params() const;
     // raw: n x 40 fp32 mixture parameters.
     void infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const;
-    // Adds the gradient of the batch (mean loss, scaled by invBatch) to the
-    // gradient buffers, without an update.
-    void accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st);
+    // The same for a queue whose length (at most maxN) is in device memory.
+    void infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st) const;
+    // Adds the gradient of the batch s[offset + i * stride], i < n (mean
+    // loss, scaled by invBatch) to the gradient buffers, without an update.
+    void accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset = 0,
+                              uint32_t stride = 1);
     void apply_adam(float lr, cudaStream_t st);
     // gradients + Adam; returns the batch loss (synchronises).
     float train_step(const Sample* s, uint32_t n, float lr, cudaStream_t st);

@@ -22,6 +22,7 @@
 
 #include "../../include/alpine_gpu.h"
 #include "bvh.cuh"
+#include "guide.cuh"
 #include "shading.cuh"
 
 namespace ag {
@@ -71,6 +72,17 @@ struct WaveView {
     uint32_t* shadowCount;
     // persistent per-pixel reference RNG state (stream mode)
     uint4* pixelRng;
+    // learned guiding (counter RNG only)
+    guide::Query* guideQuery;  // per queue entry; null = guiding off
+    const float* guideRaw;     // per queue entry: 40 mixture parameters; null = material sampling only
+    float guideFraction;       // probability of sampling the guide at an eligible vertex
+    guide::Sample* trainRec;   // recorded vertices: query, direction (weight filled by finalize)
+    float4* trainAux;          // 2 per record: (radiance after the vertex, path bits), (throughput at it, 0)
+    int* trainSlot;            // per path: record waiting for its radiance-after value, -1 = none
+    uint32_t* trainCount;
+    uint32_t trainCap;
+    uint32_t trainStride;      // record the vertices of paths whose hash % stride == 0; 0 = none
+    uint32_t waveIndex;
 };
 
 struct IntegratorKernels {
@@ -78,6 +90,9 @@ struct IntegratorKernels {
     void (*shade)(const SceneView&, const WaveView&, bool streamRng, uint32_t maxQueue, cudaStream_t);
     void (*resolve)(const WaveView&, uint32_t maxQueue, cudaStream_t);
     void (*accumulate)(const WaveView&, float* accum, double* accum64, bool streamRng, cudaStream_t);
+    // guiding: queries of the current queue; recorded vertices -> training samples
+    void (*guide_query)(const SceneView&, const WaveView&, uint32_t maxQueue, cudaStream_t);
+    void (*train_finalize)(const WaveView&, guide::Sample* out, uint32_t* outCount, cudaStream_t);
 };
 
 const IntegratorKernels& integrator_fast();
@@ -150,6 +165,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(SceneView sc, WaveView w,
     w.albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     w.nrm[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     w.pendShadow[p] = make_int2(-1, -1);
+    if (w.trainSlot) w.trainSlot[p] = -1;
     w.rng[p] = r.save();
     alpine_gpu_ray ray;
     ray.org[0] = org.x; ray.org[1] = org.y; ray.org[2] = org.z;
@@ -159,6 +175,38 @@ __global__ void __launch_bounds__(kThreads) k_generate(SceneView sc, WaveView w,
     w.rays[p] = ray;
     w.queuePath[p] = p;
     if (p == 0) *w.queueCount = w.numPaths;
+}
+
+// Surface attributes at a hit (Mesh::getIntersectionAttributes, mesh.cpp:57-154).
+struct Surface {
+    float3 ng;      // Primitive::ng = normalize(cross(e0, e1)) (bvh_common.cpp:114-117)
+    float3 ns;      // interpolated vertex normal (b0 = 1 - b1 - b2), not re-normalised; else ng
+    Material mat;
+};
+
+AG_D void surface_at(const SceneView& sc, const uint4 h, Surface& s)
+{
+    const uint32_t prim = h.x;
+    const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
+    const uint32_t* ti = sc.idx + 3ull * prim;
+    const uint32_t i0 = ti[0], i1 = ti[1], i2 = ti[2];
+    const float3 v0 = mk3(sc.verts[3ull * i0], sc.verts[3ull * i0 + 1], sc.verts[3ull * i0 + 2]);
+    const float3 v1 = mk3(sc.verts[3ull * i1], sc.verts[3ull * i1 + 1], sc.verts[3ull * i1 + 2]);
+    const float3 v2 = mk3(sc.verts[3ull * i2], sc.verts[3ull * i2 + 1], sc.verts[3ull * i2 + 2]);
+    s.ng = normalize3(cross(v1 - v0, v2 - v0));
+    const uint32_t info = sc.triInfo[prim];
+    uint32_t mid = info & 0x7fffffffu;
+    if (mid >= sc.materialCount) mid = 0;
+    s.mat = sc.materials[mid];
+    if (info & 0x80000000u) {
+        const float b0 = 1.0f - b1 - b2;
+        const float3 n0 = mk3(sc.normals[3ull * i0], sc.normals[3ull * i0 + 1], sc.normals[3ull * i0 + 2]);
+        const float3 n1 = mk3(sc.normals[3ull * i1], sc.normals[3ull * i1 + 1], sc.normals[3ull * i1 + 2]);
+        const float3 n2 = mk3(sc.normals[3ull * i2], sc.normals[3ull * i2 + 1], sc.normals[3ull * i2 + 2]);
+        s.ns = n0 * b0 + n1 * b1 + n2 * b2;
+    } else {
+        s.ns = s.ng;
+    }
 }
 
 AG_D alpine_gpu_ray make_ray(float3 o, float3 d, float tmax)
@@ -171,6 +219,78 @@ AG_D alpine_gpu_ray make_ray(float3 o, float3 d, float tmax)
     return r;
 }
 
+// One-sample MIS continuation: the direction comes from the guide's mixture
+// (moved into the local shading frame) with probability alpha, else from the
+// material's procedure; either way the weight is f / (alpha p_guide +
+// (1 - alpha) p_mat) with f and p_mat the material procedure's effective
+// integrand and true density (plain_eval), an unbiased estimate of what the
+// material's own sampling estimates.
+AG_D bool guided_continuation(const Material& mat, float3 wo, const float* raw, float alpha, float3 ss, float3 ts,
+                              float3 ns, PathRng& rng, float3& wi, float3& est)
+{
+    float r[40];
+#pragma unroll
+    for (int k = 0; k < 40; k += 4) {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(raw + k));
+        r[k] = v.x; r[k + 1] = v.y; r[k + 2] = v.z; r[k + 3] = v.w;
+    }
+    guide::Mixture m;
+    guide::decode_mixture(r, m);
+#pragma unroll
+    for (int k = 0; k < guide::kLobes; ++k) {
+        const float3 mu = to_local(m.mu[k], ss, ts, ns);
+        const float l = len3(mu);
+        m.mu[k] = l > 0.0f ? mu / l : mk3(0.0f, 0.0f, 1.0f);
+    }
+    const float us = rng.next();
+    const float u0 = rng.next();
+    const float u1 = rng.next();
+    const float u2 = rng.next();
+    if (us < alpha) {
+        wi = guide::mixture_sample(m, u0, u1, u2);
+    } else {
+        BsdfSample ms;
+        if (!mat_sample(mat, wo, u0, u1, ms)) return false;
+        wi = ms.wi;
+    }
+    float pm;
+    float3 fcos;
+    if (!plain_eval(mat, wo, wi, pm, fcos)) return false;  // outside the procedure's support: f = 0
+    float pg = guide::mixture_pdf(m, wi);
+    if (!(pg >= 0.0f && pg < 3.0e38f)) pg = 0.0f;
+    const float qm = alpha * pg + (1.0f - alpha) * pm;
+    if (!(qm > 0.0f)) return false;
+    est = fcos / qm;
+    return true;
+}
+
+// Guide queries of the current queue: shading position, roughness, direction
+// towards the previous vertex and shading normal (zeros for misses).
+__global__ void __launch_bounds__(kThreads) k_guide_query(SceneView sc, WaveView w)
+{
+    const uint32_t n = *w.queueCount;
+    uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+    if (q >= n) return;
+    const uint4 h = w.hits[q];
+    guide::Query gq = {};
+    if (h.x != 0xffffffffu) {
+        const alpine_gpu_ray ray = w.rays[q];
+        Surface sf;
+        surface_at(sc, h, sf);
+        const float t = __uint_as_float(h.y);
+        const float3 ro = mk3(ray.org[0], ray.org[1], ray.org[2]);
+        const float3 rd = mk3(ray.dir[0], ray.dir[1], ray.dir[2]);
+        const float3 hit = ro + rd * t;
+        const float3 wo = normalize3(-rd);
+        gq.pos[0] = hit.x; gq.pos[1] = hit.y; gq.pos[2] = hit.z;
+        gq.rough = sf.mat.ax;
+        gq.wo[0] = wo.x; gq.wo[1] = wo.y; gq.wo[2] = wo.z;
+        gq.n[0] = sf.ns.x; gq.n[1] = sf.ns.y; gq.n[2] = sf.ns.z;
+    }
+    w.guideQuery[q] = gq;
+}
+
+template <bool kGuided>
 __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bool streamRng)
 {
     const uint32_t n = *w.queueCount;
@@ -194,32 +314,11 @@ __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bo
         rad += thr * sc.background;
         w.rad[p] = f4(rad);
     } else {
-        const uint32_t prim = h.x;
         const float t = __uint_as_float(h.y);
-        const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
-        const uint32_t* ti = sc.idx + 3ull * prim;
-        const uint32_t i0 = ti[0], i1 = ti[1], i2 = ti[2];
-        const float3 v0 = mk3(sc.verts[3ull * i0], sc.verts[3ull * i0 + 1], sc.verts[3ull * i0 + 2]);
-        const float3 v1 = mk3(sc.verts[3ull * i1], sc.verts[3ull * i1 + 1], sc.verts[3ull * i1 + 2]);
-        const float3 v2 = mk3(sc.verts[3ull * i2], sc.verts[3ull * i2 + 1], sc.verts[3ull * i2 + 2]);
-        // Primitive::ng = normalize(cross(e0, e1)) (bvh_common.cpp:114-117)
-        const float3 ng = normalize3(cross(v1 - v0, v2 - v0));
-        const uint32_t info = sc.triInfo[prim];
-        uint32_t mid = info & 0x7fffffffu;
-        if (mid >= sc.materialCount) mid = 0;
-        const Material mat = sc.materials[mid];
-        // Mesh::getIntersectionAttributes (mesh.cpp:57-154): interpolated
-        // vertex normal (b0 = 1 - b1 - b2), not re-normalised; else ng
-        float3 ns;
-        if (info & 0x80000000u) {
-            const float b0 = 1.0f - b1 - b2;
-            const float3 n0 = mk3(sc.normals[3ull * i0], sc.normals[3ull * i0 + 1], sc.normals[3ull * i0 + 2]);
-            const float3 n1 = mk3(sc.normals[3ull * i1], sc.normals[3ull * i1 + 1], sc.normals[3ull * i1 + 2]);
-            const float3 n2 = mk3(sc.normals[3ull * i2], sc.normals[3ull * i2 + 1], sc.normals[3ull * i2 + 2]);
-            ns = n0 * b0 + n1 * b1 + n2 * b2;
-        } else {
-            ns = ng;
-        }
+        Surface sf;
+        surface_at(sc, h, sf);
+        const float3 ng = sf.ng, ns = sf.ns;
+        const Material mat = sf.mat;
         float3 ss, ts;
         get_basis(ns, ss, ts);
         const float3 hit = ro + rd * t;
@@ -283,14 +382,25 @@ __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bo
             }
         }
 
-        // continuation (alpine.cpp:342-361)
-        BsdfSample ms;
-        float cu0 = rng.next();
-        float cu1 = rng.next();
-        if (mat_sample(mat, wo, cu0, cu1, ms)) {
-            float3 wiW = to_world(ms.wi, ss, ts, ns);
+        // continuation (alpine.cpp:342-361); with a guide, one-sample MIS
+        // between the guide and the material's procedure
+        bool ok;
+        float3 wiL, est;
+        if (kGuided && w.guideRaw && wo.z > 0.0f) {
+            ok = guided_continuation(mat, wo, w.guideRaw + 40ull * q, w.guideFraction, ss, ts, ns, rng, wiL, est);
+        } else {
+            BsdfSample ms;
+            float cu0 = rng.next();
+            float cu1 = rng.next();
+            ok = mat_sample(mat, wo, cu0, cu1, ms);
+            wiL = ms.wi;
+            est = ms.estimator;
+        }
+        if (ok) {
+            float3 wiW = to_world(wiL, ss, ts, ns);
             if (dot(wiW, ng) > 0.0f) {
-                thr = thr * ms.estimator;
+                const float3 thrV = thr;
+                thr = thr * est;
                 cont = w.depth + 1 < sc.maxDepth;
                 // Russian roulette (not in the reference; off unless rrStart > 0)
                 if (cont && w.rrStart > 0 && w.depth + 1 >= w.rrStart) {
@@ -302,6 +412,24 @@ __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bo
                     uint32_t slot = warp_append(w.queueCountNext, true);
                     w.raysNext[slot] = make_ray(hit + ng * kRayOffset, wiW, 3.402823466e38f);
                     w.queuePathNext[slot] = p;
+                }
+                // training record: the radiance this direction brings is
+                // (R_final - R_after) / throughput at the vertex
+                const bool rec = cont && w.trainStride &&
+                                 (uint32_t)(splitmix64(((uint64_t)w.waveIndex << 32) | p) % w.trainStride) == 0u;
+                if (kGuided && w.trainStride) {
+                    const uint32_t r = warp_append(w.trainCount, rec);
+                    if (rec && r < w.trainCap) {
+                        guide::Sample smp;
+                        smp.q = w.guideQuery[q];
+                        const float3 d = normalize3(wiW);
+                        smp.dir[0] = d.x; smp.dir[1] = d.y; smp.dir[2] = d.z;
+                        smp.weight = 0.0f;
+                        w.trainRec[r] = smp;
+                        w.trainAux[2ull * r] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(p));
+                        w.trainAux[2ull * r + 1] = f4(thrV);
+                        w.trainSlot[p] = (int)r;
+                    }
                 }
                 w.thr[p] = f4(thr);
             }
@@ -318,21 +446,59 @@ __global__ void __launch_bounds__(kThreads) k_resolve(WaveView w)
     if (q >= n) return;
     const uint32_t p = w.queuePath[q];
     const int2 s = w.pendShadow[p];
-    if (s.x < 0 && s.y < 0) return;
-    const bool visL = s.x >= 0 && !w.shadowOcc[s.x];
-    const bool visB = s.y >= 0 && !w.shadowOcc[s.y];
-    if (visL || visB) {
-        // radiance(local) = 0; += light term; += BSDF term; / selection pdf
-        const float4 pb = w.pendB[p];
-        float3 direct = mk3(0.0f, 0.0f, 0.0f);
-        if (visL) direct += f3(w.pendL[p]);
-        if (visB) direct += f3(pb);
-        direct = direct / pb.w;
-        float3 rad = f3(w.rad[p]);
-        rad += f3(w.pendThr[p]) * direct;
-        w.rad[p] = f4(rad);
+    if (s.x >= 0 || s.y >= 0) {
+        const bool visL = s.x >= 0 && !w.shadowOcc[s.x];
+        const bool visB = s.y >= 0 && !w.shadowOcc[s.y];
+        if (visL || visB) {
+            // radiance(local) = 0; += light term; += BSDF term; / selection pdf
+            const float4 pb = w.pendB[p];
+            float3 direct = mk3(0.0f, 0.0f, 0.0f);
+            if (visL) direct += f3(w.pendL[p]);
+            if (visB) direct += f3(pb);
+            direct = direct / pb.w;
+            float3 rad = f3(w.rad[p]);
+            rad += f3(w.pendThr[p]) * direct;
+            w.rad[p] = f4(rad);
+        }
+        w.pendShadow[p] = make_int2(-1, -1);
     }
-    w.pendShadow[p] = make_int2(-1, -1);
+    if (w.trainSlot) {
+        const int r = w.trainSlot[p];
+        if (r >= 0) {
+            const float4 rad = w.rad[p];
+            w.trainAux[2ull * r] = make_float4(rad.x, rad.y, rad.z, __uint_as_float(p));
+            w.trainSlot[p] = -1;
+        }
+    }
+}
+
+// Training samples of the wave's recorded vertices: weight = luminance of
+// (R_final - R_after) / throughput, i.e. f cos Li / q of the sampled
+// direction; vertices that received no radiance are dropped.
+__global__ void __launch_bounds__(kThreads) k_train_finalize(WaveView w, guide::Sample* out, uint32_t* outCount)
+{
+    const uint32_t n = min(*w.trainCount, w.trainCap);
+    const uint32_t r = blockIdx.x * kThreads + threadIdx.x;
+    float wgt = 0.0f;
+    if (r < n) {
+        const float4 a0 = w.trainAux[2ull * r], a1 = w.trainAux[2ull * r + 1];
+        const uint32_t path = __float_as_uint(a0.w);
+        const float4 R = w.rad[path];
+        const float dx = R.x - a0.x, dy = R.y - a0.y, dz = R.z - a0.z;
+        const float lx = a1.x > 0.0f ? dx / a1.x : 0.0f;
+        const float ly = a1.y > 0.0f ? dy / a1.y : 0.0f;
+        const float lz = a1.z > 0.0f ? dz / a1.z : 0.0f;
+        wgt = 0.2126f * lx + 0.7152f * ly + 0.0722f * lz;
+        if (!(wgt > 0.0f && wgt < 3.0e38f)) wgt = 0.0f;
+    }
+    if (r >= ((n + 31u) & ~31u)) return;  // whole warps from here on
+    const bool keep = wgt > 0.0f;
+    const uint32_t slot = warp_append(outCount, keep);
+    if (keep) {
+        guide::Sample smp = w.trainRec[r];
+        smp.weight = wgt;
+        out[slot] = smp;
+    }
 }
 
 // Adds the wave's per-sample results to the per-pixel sums in sample order
@@ -378,7 +544,9 @@ void generate(const SceneView& sc, const WaveView& w, bool streamRng, cudaStream
 }
 void shade(const SceneView& sc, const WaveView& w, bool streamRng, uint32_t maxQueue, cudaStream_t st)
 {
-    if (maxQueue) k_shade<<<grid(maxQueue), kThreads, 0, st>>>(sc, w, streamRng);
+    if (!maxQueue) return;
+    if (w.guideQuery) k_shade<true><<<grid(maxQueue), kThreads, 0, st>>>(sc, w, streamRng);
+    else k_shade<false><<<grid(maxQueue), kThreads, 0, st>>>(sc, w, streamRng);
 }
 void resolve(const WaveView& w, uint32_t maxQueue, cudaStream_t st)
 {
@@ -387,6 +555,14 @@ void resolve(const WaveView& w, uint32_t maxQueue, cudaStream_t st)
 void accumulate(const WaveView& w, float* accum, double* accum64, bool streamRng, cudaStream_t st)
 {
     if (w.numPixels) k_accumulate<<<grid(w.numPixels), kThreads, 0, st>>>(w, accum, accum64, streamRng);
+}
+void guide_query(const SceneView& sc, const WaveView& w, uint32_t maxQueue, cudaStream_t st)
+{
+    if (maxQueue) k_guide_query<<<grid(maxQueue), kThreads, 0, st>>>(sc, w);
+}
+void train_finalize(const WaveView& w, guide::Sample* out, uint32_t* outCount, cudaStream_t st)
+{
+    if (w.trainCap) k_train_finalize<<<grid(w.trainCap), kThreads, 0, st>>>(w, out, outCount);
 }
 
 }  // namespace AG_INTEGRATOR_NS

@@ -8,7 +8,8 @@
 namespace ag {
 const IntegratorKernels& integrator_exact()
 {
-    static const IntegratorKernels k = {exact::generate, exact::shade, exact::resolve, exact::accumulate};
+    static const IntegratorKernels k = {exact::generate, exact::shade, exact::resolve, exact::accumulate,
+                                              exact::guide_query, exact::train_finalize};
     return k;
 }
 }  // namespace ag

@@ -5,7 +5,8 @@
 namespace ag {
 const IntegratorKernels& integrator_fast()
 {
-    static const IntegratorKernels k = {fast::generate, fast::shade, fast::resolve, fast::accumulate};
+    static const IntegratorKernels k = {fast::generate, fast::shade, fast::resolve, fast::accumulate,
+                                              fast::guide_query, fast::train_finalize};
     return k;
 }
 }  // namespace ag

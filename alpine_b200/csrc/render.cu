@@ -333,6 +333,40 @@ ag::WaveView carve_wave(alpine_gpu_ctx* c)
     return w;
 }
 
+// Guiding buffers for `paths` paths and `cap` training records.
+struct GuideWave {
+    ag::guide::Query* query;
+    float* raw;
+    int* slot;
+    ag::guide::Sample* rec;
+    float4* aux;
+    ag::guide::Sample* out;
+    uint32_t* counters;  // [0] records, [1] kept samples
+};
+
+bool reserve_guide_wave(alpine_gpu_ctx* c, uint32_t paths, uint32_t cap, GuideWave& g)
+{
+    size_t P = paths, R = cap;
+    size_t bytes = round256(P * sizeof(ag::guide::Query)) + round256(P * 40 * sizeof(float)) +
+                   round256(P * sizeof(int)) + round256(R * sizeof(ag::guide::Sample)) +
+                   round256(2 * R * sizeof(float4)) + round256(R * sizeof(ag::guide::Sample)) + 256;
+    if (!c->dGuideWave.reserve(bytes)) return false;
+    char* p = c->dGuideWave.as<char>();
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += round256(b);
+        return r;
+    };
+    g.query = (ag::guide::Query*)take(P * sizeof(ag::guide::Query));
+    g.raw = (float*)take(P * 40 * sizeof(float));
+    g.slot = (int*)take(P * sizeof(int));
+    g.rec = (ag::guide::Sample*)take(R * sizeof(ag::guide::Sample));
+    g.aux = (float4*)take(2 * R * sizeof(float4));
+    g.out = (ag::guide::Sample*)take(R * sizeof(ag::guide::Sample));
+    g.counters = (uint32_t*)take(256);
+    return true;
+}
+
 bool reserve_accum(alpine_gpu_ctx* c)
 {
     size_t pixels = (size_t)c->cfg.width * c->cfg.height;
@@ -375,6 +409,29 @@ __global__ void k_post(const float* a32, const double* a64, uint32_t pixels, uin
     }
 }
 
+// Turns the wave's recorded vertices into training samples and takes up to
+// `maxSteps` Adam steps; step i uses samples i, i + steps, i + 2 steps, ...
+// so that every batch spans the whole image.
+int train_guide(alpine_gpu_ctx* c, const ag::IntegratorKernels& K, const ag::WaveView& w, const GuideWave& gw,
+                uint32_t batch, uint32_t maxSteps, float lr)
+{
+    cudaStream_t st = c->stream;
+    K.train_finalize(w, gw.out, gw.counters + 1, st);
+    uint32_t kept = 0;
+    cudaError_t e = cudaMemcpyAsync(c->hStatus + 1, gw.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("guide training: ") + cudaGetErrorString(e));
+    kept = std::min(c->hStatus[1], w.trainCap);
+    if (kept == 0) return ALPINE_GPU_OK;
+    const uint32_t steps = std::min(maxSteps, (kept + batch - 1) / batch);
+    for (uint32_t i = 0; i < steps; ++i) {
+        const uint32_t n = (kept - i + steps - 1) / steps;
+        c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, steps);
+        c->guide.apply_adam(lr, st);
+    }
+    return ALPINE_GPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -386,17 +443,7 @@ int alpine_gpu_set_materials(alpine_gpu_ctx* c, const alpine_gpu_material* m, ui
     c->materials.clear();
     for (uint32_t i = 0; i < n; ++i) {
         ag::Material x{};
-        if (m[i].kind != ALPINE_GPU_MATERIAL_DIELECTRIC && m[i].kind != ALPINE_GPU_MATERIAL_CONDUCTOR)
-            return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_materials: unknown kind");
-        x.kind = m[i].kind == ALPINE_GPU_MATERIAL_CONDUCTOR ? ag::kMatConductor : ag::kMatDielectric;
-        x.r = m[i].base_color[0];
-        x.g = m[i].base_color[1];
-        x.b = m[i].base_color[2];
-        float a = m[i].roughness;  // alpha = roughness (gltf_loader.cpp:404-414)
-        x.ax = std::max(0.001f, a);  // Microfacet clamps alpha (microfacet.h:9-12)
-        x.ay = std::max(0.001f, a);
-        // Dielectric adds the microfacet lobe when dot(alpha, alpha) < 1
-        x.lobes = (a * a + a * a < 1.0f) ? 2u : 1u;
+        if (!ag::make_material(m[i], x)) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_materials: unknown kind");
         c->materials.push_back(x);
     }
     c->materialsDirty = true;
@@ -593,8 +640,34 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
     if (maxPaths < 1024) maxPaths = 1024;
     // samples per wave: one in stream mode (the per-pixel RNG is sequential)
     uint32_t S = stream ? 1u : std::max(1u, std::min(spp, maxPaths / std::max(1u, pixels)));
+    const alpine_gpu_render_options& o = c->options;
+    const bool guiding = !stream && o.guide != 0;
+    const bool training = guiding && o.guide_train != 0;
+    const uint32_t gBatch = o.guide_batch ? o.guide_batch : 16384u;
+    const uint32_t gSteps = o.guide_steps_per_wave ? o.guide_steps_per_wave : 8u;
+    const float gLr = o.guide_lr > 0.0f ? o.guide_lr : 1e-2f;
+    const float gFrac = o.guide_fraction > 0.0f ? std::min(o.guide_fraction, 1.0f) : 0.5f;
+    if (guiding) S = std::min(S, o.guide_spp_per_wave ? o.guide_spp_per_wave : 1u);
     uint32_t pixelChunk = std::min(pixels, maxPaths / S);
     if (!reserve_wave(c, S * pixelChunk)) return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "wave buffers");
+    GuideWave gw{};
+    const uint32_t trainCap = training ? std::min<uint32_t>(1u << 21, 2u * gSteps * gBatch) : 0u;
+    if (guiding) {
+        if (!c->guide.ready() && c->guide.reset(c->guideSeed, c->stream) != 0)
+            return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide: parameter allocation failed");
+        if (!c->guideBoxSet && !c->verts.empty()) {  // the scene's bounds
+            float3 lo = h3(c->verts[0], c->verts[1], c->verts[2]), hi = lo;
+            for (size_t i = 0; i + 2 < c->verts.size(); i += 3) {
+                float3 v = h3(c->verts[i], c->verts[i + 1], c->verts[i + 2]);
+                lo = hmin(lo, v);
+                hi = hmax(hi, v);
+            }
+            c->guide.set_scene_box(lo, hi);
+            c->guideBoxSet = true;
+        }
+        if (!reserve_guide_wave(c, S * pixelChunk, std::max(trainCap, 1u), gw))
+            return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide wave buffers");
+    }
 
     ag::SceneView sc{};
     sc.verts = c->dVerts.as<float>();
@@ -635,12 +708,34 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
             w.seed = c->options.seed;
             w.rrStart = stream ? 0u : c->options.russian_roulette_depth;
             w.pixelRng = c->dPixelRng.as<uint4>();
+            const bool sampleGuide = guiding && c->guide.steps() >= o.guide_warmup_steps;
+            if (guiding) {
+                w.guideQuery = gw.query;
+                w.guideRaw = sampleGuide ? gw.raw : nullptr;
+                w.guideFraction = gFrac;
+            }
+            if (training) {
+                // record about trainCap vertices: ~3 continuations per path
+                const uint64_t expected = 3ull * w.numPaths;
+                w.trainStride = (uint32_t)std::max<uint64_t>(1, (expected + trainCap - 1) / trainCap);
+                w.trainCap = trainCap;
+                w.trainRec = gw.rec;
+                w.trainAux = gw.aux;
+                w.trainSlot = gw.slot;
+                w.trainCount = gw.counters;
+                w.waveIndex = c->guideWaveIndex;
+                cudaMemsetAsync(gw.counters, 0, 2 * sizeof(uint32_t), st);
+            }
             K.generate(sc, w, stream, st);
             for (uint32_t depth = 0; depth < sc.maxDepth; ++depth) {
                 w.depth = depth;
                 ag::launch_trace_dyn(bvh, w.rays, w.queueCount, w.numPaths, false, w.hits, c->dStatus, st);
                 cudaMemsetAsync(w.queueCountNext, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(w.shadowCount, 0, sizeof(uint32_t), st);
+                if (guiding) {
+                    K.guide_query(sc, w, w.numPaths, st);
+                    if (sampleGuide) c->guide.infer_queue(gw.query, w.queueCount, w.numPaths, gw.raw, st);
+                }
                 K.shade(sc, w, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,
                                      c->dStatus, st);
@@ -650,6 +745,10 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
                 std::swap(w.queueCount, w.queueCountNext);
             }
             K.accumulate(w, acc32, acc64, stream, st);
+            if (guiding) ++c->guideWaveIndex;
+            if (training) {
+                if (int rc = train_guide(c, K, w, gw, gBatch, gSteps, gLr)) return rc;
+            }
         }
         done += s;
     }

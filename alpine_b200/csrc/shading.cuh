@@ -308,6 +308,91 @@ AG_HD float mat_pdf(const Material& m, float3 wo, float3 wi)
 }
 
 // ---------------------------------------------------------------------------
+// The plain continuation procedure (Material::sample) as a density over
+// directions, for one-sample MIS with another sampling technique. For wo and
+// wi in the upper hemisphere, writes the true density p of the procedure's
+// output direction and its effective integrand f_eff * cos = E[estimator | wi]
+// * p, so that f_eff * cos / q for any mixture density q containing p
+// estimates exactly what the plain estimator estimates, including the
+// reference's pdf conventions (VNDF sampling with a D / (4 wo.wh) pdf in the
+// dielectric mixture, dielectric.cpp:31-62).
+//   VNDF density of the reflected direction: G1(wo) D(wh) / (4 cos(theta_o))
+//   (Heitz 2018, "Sampling the GGX Distribution of Visible Normals"), times
+//   the indicator of the half-space the reference's sampler actually covers.
+//   Heitz's warp of the disk is exact when the frame's second axis T2 lies in
+//   the vertical plane of the stretched view direction Vh; then the warped
+//   half-disk is the projection of {N : N.z >= 0}. The reference builds the
+//   frame with getBasis(Vh), whose b2 is tilted, so the warped half-disk is
+//   the projection of {N : N . (r b2 + Vh.z Vh) >= 0}, r = sqrt(1 - Vh.z^2),
+//   uniformly covered with the same density; normals outside it are never
+//   produced (and those inside it below the horizon are clamped and then
+//   rejected as wi.z <= 0).
+AG_HD float mf_vndf_density(float3 wo, float3 wi, float ax, float ay)
+{
+    float3 wh = wo + wi;
+    float l = len3(wh);
+    if (l == 0.0f || wo.z <= 0.0f) return 0.0f;
+    wh = wh / l;
+    if (wh.z <= 0.0f || dot(wo, wh) <= 0.0f) return 0.0f;
+    const float3 vh = normalize3(mk3(ax * wo.x, ay * wo.y, wo.z));
+    float3 b1, b2;
+    get_basis(vh, b1, b2);
+    const float r = sqrtf(fmaxf(0.0f, 1.0f - vh.z * vh.z));
+    const float3 n2 = b2 * r + vh * vh.z;
+    const float3 nh = mk3(wh.x / ax, wh.y / ay, wh.z);  // un-stretched normal (unnormalised)
+    if (dot(nh, n2) < 0.0f) return 0.0f;
+    float g1 = 1.0f / (1.0f + mf_lambda(wo, ax, ay));
+    return g1 * mf_distribution(wh, ax, ay) / (4.0f * wo.z);
+}
+
+// Microfacet::sample's estimator F G2 / G1 as a function of wi.
+AG_HD float3 mf_estimator(float3 wo, float3 wi, float3 f0, float ax, float ay)
+{
+    float3 wh = wo + wi;
+    float l = len3(wh);
+    if (l == 0.0f) return mk3(0.0f, 0.0f, 0.0f);
+    wh = wh / l;
+    float3 f = schlick(f0, wi, wh);
+    float g1 = 1.0f / (1.0f + mf_lambda(wo, ax, ay));
+    return f * mf_g2(wo, wi, ax, ay) / g1;
+}
+
+AG_HD bool plain_eval(const Material& m, float3 wo, float3 wi, float& p, float3& fcos)
+{
+    p = 0.0f;
+    fcos = mk3(0.0f, 0.0f, 0.0f);
+    if (wo.z <= 0.0f || wi.z <= 0.0f) return false;
+    const float3 bc = mat_color(m);
+    if (m.kind == kMatConductor) {
+        p = mf_vndf_density(wo, wi, m.ax, m.ay);
+        fcos = mf_estimator(wo, wi, bc, m.ax, m.ay) * p;
+        return p > 0.0f;
+    }
+    const float pc = wi.z / kPi;  // cosine-weighted hemisphere
+    if (m.lobes == 1) {
+        p = pc;
+        fcos = bc * pc;  // estimator = base colour
+        return p > 0.0f;
+    }
+    const float3 f0 = mk3(kDielectricF0, kDielectricF0, kDielectricF0);
+    const float cosT = wi.z;
+    const float pmRep = mf_pdf(wo, wi, m.ax, m.ay);     // reference's reported microfacet pdf
+    const float3 fm = mf_bsdf(wo, wi, f0, m.ax, m.ay);
+    const float pv = mf_vndf_density(wo, wi, m.ax, m.ay);
+    // Lambertian lobe sampled wi: bsdf = bc/pi + f_m, pdf = (pc + pmRep) / 2
+    const float3 estL = (lambert_bsdf(bc) + fm) * cosT / ((pc + pmRep) / 2.0f);
+    fcos = estL * (0.5f * pc);
+    // microfacet lobe sampled wi: bsdf = est_m pmRep / cos + bc/pi
+    if (pv > 0.0f) {
+        const float3 estMf = mf_estimator(wo, wi, f0, m.ax, m.ay);
+        const float3 estM = (estMf * pmRep / cosT + lambert_bsdf(bc)) * cosT / ((pmRep + pc) / 2.0f);
+        fcos += estM * (0.5f * pv);
+    }
+    p = 0.5f * pc + 0.5f * pv;
+    return p > 0.0f;
+}
+
+// ---------------------------------------------------------------------------
 // Lights.
 enum LightKind : uint32_t { kLightPoint = 0, kLightDisk = 1, kLightQuad = 2 };
 

@@ -49,7 +49,10 @@ class BvhStats(C.Structure):
 
 class RenderOptions(C.Structure):
     _fields_ = [("sampler", C.c_uint32), ("max_paths_per_wave", C.c_uint32), ("russian_roulette_depth", C.c_uint32),
-                ("seed", C.c_uint32), ("accumulate_fp64", C.c_uint32)]
+                ("seed", C.c_uint32), ("accumulate_fp64", C.c_uint32), ("guide", C.c_uint32),
+                ("guide_fraction", C.c_float), ("guide_train", C.c_uint32), ("guide_batch", C.c_uint32),
+                ("guide_lr", C.c_float), ("guide_warmup_steps", C.c_uint32), ("guide_spp_per_wave", C.c_uint32),
+                ("guide_steps_per_wave", C.c_uint32)]
 
 
 MATERIAL_DTYPE = np.dtype([("kind", np.uint32), ("base_color", np.float32, 3), ("roughness", np.float32)])
@@ -91,6 +94,8 @@ def lib():
         f3 = C.POINTER(C.c_float)
         u32p = C.POINTER(C.c_uint32)
         L.alpine_gpu_set_materials.argtypes = [vp, vp, C.c_uint32]
+        L.alpine_gpu_material_sample.argtypes = [vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
+        L.alpine_gpu_material_eval.argtypes = [vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
         L.alpine_gpu_set_triangle_attributes.argtypes = [vp, C.c_uint32, vp, vp]
         L.alpine_gpu_add_point_light.argtypes = [vp, C.c_float, f3, f3, u32p]
         L.alpine_gpu_add_disk_light.argtypes = [vp, C.c_float, f3, f3, f3, C.c_float, u32p]
@@ -109,6 +114,7 @@ def lib():
         L.alpine_gpu_guide_dims.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32p]
         L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
+        L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p]
         L.alpine_gpu_guide_gradients.argtypes = [vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_guide_train.argtypes = [vp, vp, C.c_uint32, C.c_float, f3]
         L.alpine_gpu_guide_get_weights.argtypes = [vp, vp]
@@ -216,6 +222,49 @@ class Context:
             m[i] = (k, col, r)
         self._check(self.L.alpine_gpu_set_materials(self.h, _ptr(m) if len(m) else None, len(m)))
 
+    @staticmethod
+    def _material(material):
+        k, col, r = material
+        m = np.zeros(1, MATERIAL_DTYPE)
+        m[0] = (k, col, r)
+        return m
+
+    def material_sample(self, material, wo, u):
+        """Material::sample on the GPU. material: (kind, (r, g, b), roughness);
+        wo: (n, 3), u: (n, 2). Returns wi (n, 3), estimator (n, 3), pdf (n,),
+        ok (n,) bool."""
+        m = self._material(material)
+        wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        u = np.ascontiguousarray(u, np.float32).reshape(-1, 2)
+        n = wo.shape[0]
+        if u.shape[0] != n:
+            raise ValueError("wo and u differ in length")
+        wi = np.zeros((n, 3), np.float32)
+        est = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        ok = np.zeros(n, np.uint8)
+        self._check(self.L.alpine_gpu_material_sample(self.h, _ptr(m), _ptr(wo), _ptr(u), n, _ptr(wi), _ptr(est),
+                                                      _ptr(pdf), _ptr(ok)))
+        return wi, est, pdf, ok.astype(bool)
+
+    def material_eval(self, material, wo, wi):
+        """computeBsdf, computePdf and the sampling procedure's true density
+        and effective integrand at (wo, wi) pairs. Returns bsdf (n, 3),
+        pdf (n,), density (n,), integrand (n, 3)."""
+        m = self._material(material)
+        wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
+        n = wo.shape[0]
+        if wi.shape[0] != n:
+            raise ValueError("wo and wi differ in length")
+        bsdf = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        dens = np.zeros(n, np.float32)
+        integ = np.zeros((n, 3), np.float32)
+        self._check(self.L.alpine_gpu_material_eval(self.h, _ptr(m), _ptr(wo), _ptr(wi), n, _ptr(bsdf), _ptr(pdf),
+                                                    _ptr(dens), _ptr(integ)))
+        return bsdf, pdf, dens, integ
+
     def set_triangle_attributes(self, shape, normals=None, tri_material=None):
         n = None if normals is None else np.ascontiguousarray(normals, np.float32)
         t = None if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
@@ -252,8 +301,14 @@ class Context:
         self._check(self.L.alpine_gpu_set_camera(self.h, _f3(eye), _f3(target), _f3(up), fovy, aspect))
 
     def set_render_options(self, sampler=RNG_COUNTER, max_paths_per_wave=0, russian_roulette_depth=0, seed=0,
-                           accumulate_fp64=False):
-        o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64))
+                           accumulate_fp64=False, guide=False, guide_fraction=0.5, guide_train=True,
+                           guide_batch=16384, guide_lr=1e-2, guide_warmup_steps=0, guide_spp_per_wave=1,
+                           guide_steps_per_wave=8):
+        """Options of alpine_gpu_render_options; the guide_* fields apply when
+        guide is set (learned path guiding, counter sampler only)."""
+        o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64),
+                          int(guide), guide_fraction, int(guide_train), guide_batch, guide_lr, guide_warmup_steps,
+                          guide_spp_per_wave, guide_steps_per_wave)
         self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
 
     def reset_accumulation(self):
@@ -290,6 +345,12 @@ class Context:
 
     def guide_reset(self, seed, lo, hi):
         self._check(self.L.alpine_gpu_guide_reset(self.h, seed, _f3(lo), _f3(hi)))
+
+    def guide_steps(self):
+        """(Adam steps since the last reset, waves rendered with guiding)."""
+        a, b = C.c_uint32(), C.c_uint32()
+        self._check(self.L.alpine_gpu_guide_steps(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def guide_infer(self, queries):
         q = np.ascontiguousarray(queries, np.float32).reshape(-1, 12)

@@ -175,6 +175,24 @@ typedef struct alpine_gpu_material {
 ALPINE_GPU_API int alpine_gpu_set_materials(alpine_gpu_ctx* ctx, const alpine_gpu_material* materials,
                                             uint32_t count);
 
+/* Material probes on the GPU, for arrays in HOST memory, directions in the
+ * local shading frame (z = shading normal). Synchronous.
+ * alpine_gpu_material_sample: Material::sample (src/materials/material.h:18-19;
+ *   dielectric.cpp:31-62, conductor.cpp:18-25) for `count` (wo[3], u[2])
+ *   pairs; writes wi[3], estimator[3] (bsdf * cos / pdf), pdf and ok (0 when
+ *   the reference returns no sample; the other outputs are then 0).
+ * alpine_gpu_material_eval: Material::computeBsdf / computePdf
+ *   (material.h:21-24) at (wo[3], wi[3]) pairs, plus the true density of the
+ *   direction that Material::sample outputs and its effective integrand
+ *   E[estimator | wi] * density (3 floats): the quantities one-sample MIS with
+ *   the learned guide uses. Output pointers may be NULL. */
+ALPINE_GPU_API int alpine_gpu_material_sample(alpine_gpu_ctx* ctx, const alpine_gpu_material* material,
+                                              const float* wo, const float* u, uint32_t count, float* wi,
+                                              float* estimator, float* pdf, uint8_t* ok);
+ALPINE_GPU_API int alpine_gpu_material_eval(alpine_gpu_ctx* ctx, const alpine_gpu_material* material,
+                                            const float* wo, const float* wi, uint32_t count, float* bsdf,
+                                            float* pdf, float* sample_density, float* sample_integrand);
+
 /* Per-vertex shading normals (float[3 * vertex_count], may be NULL: the
  * geometric normal is used) and per-triangle material ids (may be NULL:
  * material 0) of one mesh (Mesh::Data normals / materials,
@@ -223,7 +241,26 @@ ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3]
  * max_paths_per_wave: 0 = 2^21.
  * russian_roulette_depth: 0 = off (the reference has none); d > 0 applies
  *   roulette to continuations from depth d on (COUNTER sampler only).
- * accumulate_fp64: per-pixel sums in FP64 (long convergence runs). */
+ * accumulate_fp64: per-pixel sums in FP64 (long convergence runs).
+ * guide: 1 = learned path guiding of the continuation direction (COUNTER
+ *   sampler only). At every vertex with the view direction above the shading
+ *   surface the direction comes from the guide's mixture with probability
+ *   guide_fraction, else from the material's own sampling procedure, and is
+ *   weighted by the one-sample MIS estimator f / (a p_guide + (1 - a) p_mat),
+ *   where f and p_mat are the effective integrand and the true density of the
+ *   material's procedure: the image converges to the same expectation as
+ *   without guiding.
+ * guide_fraction: a in (0, 1]; 0 = 0.5.
+ * guide_train: 1 = record path vertices and train the guide (Adam) between
+ *   waves on the radiance they received.
+ * guide_batch: samples per Adam step; 0 = 16384.
+ * guide_lr: Adam learning rate; 0 = 0.01.
+ * guide_warmup_steps: the guide is sampled only after this many Adam steps
+ *   (before that, vertices use the material's procedure and are recorded for
+ *   training).
+ * guide_spp_per_wave: samples per pixel per wave while guiding (training
+ *   happens between waves); 0 = 1.
+ * guide_steps_per_wave: at most this many Adam steps after a wave; 0 = 8. */
 #define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
 #define ALPINE_GPU_SAMPLER_COUNTER 1u
 typedef struct alpine_gpu_render_options {
@@ -232,6 +269,14 @@ typedef struct alpine_gpu_render_options {
     uint32_t russian_roulette_depth;
     uint32_t seed;
     uint32_t accumulate_fp64;
+    uint32_t guide;
+    float guide_fraction;
+    uint32_t guide_train;
+    uint32_t guide_batch;
+    float guide_lr;
+    uint32_t guide_warmup_steps;
+    uint32_t guide_spp_per_wave;
+    uint32_t guide_steps_per_wave;
 } alpine_gpu_render_options;
 ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
 
@@ -259,7 +304,7 @@ ALPINE_GPU_API int alpine_gpu_post_process(alpine_gpu_ctx* ctx, int tonemap, flo
  * Learned path guiding (no counterpart in the reference): a hash-grid encoded
  * MLP predicting an 8-lobe von Mises-Fisher mixture over incident directions,
  * trained online. These entry points expose the model for tests and tools;
- * the integrator uses it through alpine_gpu_set_guiding.
+ * the integrator uses it when alpine_gpu_render_options.guide is set.
  * Query record: 12 floats {pos[3], roughness, wo[3], 0, normal[3], 0}.
  * Sample record: 16 floats {query[12], dir[3], weight}.
  * Raw output: 40 floats = 8 lobes x {direction[3], log kappa, logit}. */
@@ -268,6 +313,8 @@ ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_
 ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],
                                           const float scene_hi[3]);
 ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw);
+/* Adam steps taken since the last reset and waves rendered with guiding. */
+ALPINE_GPU_API int alpine_gpu_guide_steps(alpine_gpu_ctx* ctx, uint32_t* adam_steps, uint32_t* guided_waves);
 ALPINE_GPU_API int alpine_gpu_guide_gradients(alpine_gpu_ctx* ctx, const float* samples, uint32_t count, float* dW,
                                               const uint64_t* grid_index, uint32_t grid_count, float* grid_grad,
                                               float* loss);

@@ -107,6 +107,8 @@ def ref():
         L.ref_render_read_accum.restype = C.c_uint32
         L.ref_render_post_process.argtypes = [C.c_int, _u8p]
         L.ref_render_read_sampler_state.argtypes = [_u32p]
+        L.ref_material_sample.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, _f32p, _f32p, _f32p, _u8p]
+        L.ref_material_eval.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, _f32p, _f32p]
         _ref = L
     return _ref
 
@@ -275,6 +277,38 @@ class RefRenderer:
 
     def close(self):
         self.L.ref_render_shutdown()
+
+
+def _material_record(material):
+    kind, col, rough = material
+    return np.array([float(kind), col[0], col[1], col[2], rough], np.float32)
+
+
+def ref_material_sample(material, wo, u):
+    """The reference's Material::sample (src/materials/material.h:18-19) for
+    (wo, u) pairs in the local frame. material: (kind, (r, g, b), roughness),
+    kind 0 = Dielectric, 1 = Conductor. Returns wi, estimator, pdf, ok."""
+    wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+    u = np.ascontiguousarray(u, np.float32).reshape(-1, 2)
+    n = wo.shape[0]
+    wi = np.empty((n, 3), np.float32)
+    est = np.empty((n, 3), np.float32)
+    pdf = np.empty(n, np.float32)
+    ok = np.empty(n, np.uint8)
+    ref().ref_material_sample(_material_record(material), wo.reshape(-1), u.reshape(-1), n, wi.reshape(-1),
+                              est.reshape(-1), pdf, ok)
+    return wi, est, pdf, ok.astype(bool)
+
+
+def ref_material_eval(material, wo, wi):
+    """The reference's Material::computeBsdf / computePdf (material.h:21-24)."""
+    wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+    wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
+    n = wo.shape[0]
+    bsdf = np.empty((n, 3), np.float32)
+    pdf = np.empty(n, np.float32)
+    ref().ref_material_eval(_material_record(material), wo.reshape(-1), wi.reshape(-1), n, bsdf.reshape(-1), pdf)
+    return bsdf, pdf
 
 
 class RefAccel:

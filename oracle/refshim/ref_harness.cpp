@@ -269,6 +269,16 @@ inline Ray makeRay(const float* r)
 }
 }
 
+// One material record {kind, r, g, b, roughness} as the reference class
+// (kind 0 = Dielectric, 1 = Conductor; the loaders' alpha = roughness).
+static std::shared_ptr<Material>
+make_ref_material(const float* r)
+{
+    float3 bc(r[1], r[2], r[3]);
+    if (r[0] == 1.0f) { return std::make_shared<Conductor>(float2(r[4]), bc, nullptr, nullptr); }
+    return std::make_shared<Dielectric>(float2(r[4]), bc, nullptr, nullptr);
+}
+
 extern "C" {
 // kind: 0 = Bvh (binary), 1 = WideBvh (8-wide, ISPC kernels restated).
 void*
@@ -379,13 +389,7 @@ ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, u
         for (uint32_t i = 0; i < nverts; ++i) { d.normals[i] = float3(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]); }
     }
     std::vector<std::shared_ptr<Material>> mats(nmat);
-    for (uint32_t m = 0; m < nmat; ++m)
-    {
-        const float* r = materials + 5 * m;
-        float3 bc(r[1], r[2], r[3]);
-        if (r[0] == 1.0f) { mats[m] = std::make_shared<Conductor>(float2(r[4]), bc, nullptr, nullptr); }
-        else { mats[m] = std::make_shared<Dielectric>(float2(r[4]), bc, nullptr, nullptr); }
-    }
+    for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 5 * m); }
     d.prims.resize(ntris);
     d.materials.resize(ntris);
     for (uint32_t i = 0; i < ntris; ++i)
@@ -474,4 +478,39 @@ ref_render_read_sampler_state(uint32_t* out)
 }
 
 void ref_render_shutdown() { shutdown(); }
+
+// Material::sample for n (wo, u) pairs in the local frame.
+void
+ref_material_sample(const float* rec, const float* wo, const float* u, uint32_t n, float* wi, float* est,
+    float* pdf, uint8_t* ok)
+{
+    auto m = make_ref_material(rec);
+    IntersectionAttributes ia{};
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        auto s = m->sample(float3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), float2(u[2 * i], u[2 * i + 1]), ia);
+        ok[i] = s.has_value() ? 1 : 0;
+        for (int k = 0; k < 3; ++k)
+        {
+            wi[3 * i + k] = s ? s->wi[k] : 0.0f;
+            est[3 * i + k] = s ? s->estimator[k] : 0.0f;
+        }
+        pdf[i] = s ? s->pdf : 0.0f;
+    }
+}
+
+// Material::computeBsdf / computePdf for n (wo, wi) pairs in the local frame.
+void
+ref_material_eval(const float* rec, const float* wo, const float* wi, uint32_t n, float* bsdf, float* pdf)
+{
+    auto m = make_ref_material(rec);
+    IntersectionAttributes ia{};
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        float3 a(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), b(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        float3 f = m->computeBsdf(a, b, ia);
+        for (int k = 0; k < 3; ++k) { bsdf[3 * i + k] = f[k]; }
+        pdf[i] = m->computePdf(a, b);
+    }
+}
 }
