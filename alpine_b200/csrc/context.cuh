@@ -127,7 +127,7 @@ struct alpine_gpu_ctx {
     ag::DeviceBuffer dGuideWave;     // queries, mixture parameters, training records
     uint32_t guideWavePaths = 0, guideTrainCap = 0;
     uint32_t guideWaveIndex = 0;     // waves rendered with guiding (record selection hash)
-    float guideLastLoss = 0.0f;
+    uint32_t guideLastLossSteps = 0;  // Adam steps behind the loss sum in hStatus[2]
 
     // Reads and clears the device status word (stream must be idle).
     int check_device_status()

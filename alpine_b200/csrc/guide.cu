@@ -2,6 +2,7 @@
 // guide.cuh for the model and the published methods it restates).
 #include "guide_host.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -10,62 +11,135 @@ namespace ag {
 namespace guide {
 namespace {
 
-constexpr int kInferWarps = 4;
+constexpr int kInferWarps = 8;
 constexpr int kTrainWarps = 2;
+
+// Shared-memory strides, padded so that the mma fragment loads of a warp
+// (8 rows x 4 words) fall in 32 different banks: activation rows of 72 bf16
+// (36 words, rows 4 banks apart), weight rows of in + 8, and rows of 40 bf16
+// for the transposed [64][32] buffers (20 words).
+constexpr int kLd = kHidden + 8;
+constexpr int kLdT = 32 + 8;
+__host__ __device__ constexpr int wld(int l) { return layer_in(l) + 8; }
+__host__ __device__ constexpr int wsm_offset(int l)
+{
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_out(i) * wld(i);
+    return o;
+}
+constexpr int kWsm = wsm_offset(kLayers);  // bf16 elements of the padded weight copy
 
 AG_D __nv_bfloat16 bf(float x) { return __float2bfloat16_rn(x); }
 AG_D float fl(__nv_bfloat16 x) { return __bfloat162float(x); }
+AG_D uint32_t pack_bf2(float a, float b)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
 
-// Encodes the 64 inputs of one query into a bf16 row.
+// Packed [out][in] weights of every layer into the padded shared copy.
+AG_D void load_weights(const __nv_bfloat16* __restrict__ g, __nv_bfloat16* s)
+{
+    for (int l = 0; l < kLayers; ++l) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(g + layer_offset(l));
+        uint32_t* dst = reinterpret_cast<uint32_t*>(s + wsm_offset(l));
+        const int words = layer_in(l) / 2, rows = layer_out(l);
+        for (int i = threadIdx.x; i < rows * words; i += blockDim.x) dst[(i / words) * (wld(l) / 2) + i % words] = src[i];
+    }
+}
+
+// Encodes the 64 inputs of one query into a bf16 row. Levels are processed
+// two at a time with their 16 corner loads issued together: the encoding is
+// bound by the latency of these gathers.
 AG_D void encode_row(const Params& g, const Query& q, __nv_bfloat16* row)
 {
-    float3 p = normalise_position(g, mk3(q.pos[0], q.pos[1], q.pos[2]));
-    for (int l = 0; l < kLevels; ++l) {
-        float f0 = 0.0f, f1 = 0.0f;
-        for (int c = 0; c < 8; ++c) {
-            uint32_t idx;
-            float w;
-            grid_corner(g.res[l], p, c, idx, w);
-            const __half2 v = *reinterpret_cast<const __half2*>(g.grid + ((uint64_t)l * kTableSize + idx) * kFeatures);
-            f0 += w * __low2float(v);
-            f1 += w * __high2float(v);
+    const float3 p = normalise_position(g, mk3(q.pos[0], q.pos[1], q.pos[2]));
+#pragma unroll
+    for (int l0 = 0; l0 < kLevels; l0 += 2) {
+        uint32_t idx[2][8];
+        float w[2][8];
+        __half2 v[2][8];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) grid_corner(g.res[l0 + j], p, c, idx[j][c], w[j][c]);
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                v[j][c] = *reinterpret_cast<const __half2*>(g.grid + ((uint64_t)(l0 + j) * kTableSize + idx[j][c]) * kFeatures);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                f0 += w[j][c] * __low2float(v[j][c]);
+                f1 += w[j][c] * __high2float(v[j][c]);
+            }
+            row[2 * (l0 + j)] = bf(f0);
+            row[2 * (l0 + j) + 1] = bf(f1);
         }
-        row[2 * l] = bf(f0);
-        row[2 * l + 1] = bf(f1);
     }
     float ex[8];
     extra_inputs(mk3(q.wo[0], q.wo[1], q.wo[2]), mk3(q.n[0], q.n[1], q.n[2]), q.rough, ex);
+#pragma unroll
     for (int k = 0; k < 8; ++k) row[kGridDims + k] = bf(ex[k]);
     for (int k = kGridDims + 8; k < kIn; ++k) row[k] = bf(0.0f);
 }
 
-// Forward of one warp's 32 rows. X: [32][64] input rows; ping/pong buffers
-// [32][64]; out: [32][48] fp32. saved (optional): the input of every layer.
-AG_D void forward32(const __nv_bfloat16* W, __nv_bfloat16* X, __nv_bfloat16* tmp, float* out,
-                    __nv_bfloat16* saved)
+// acc = X[32 x K] * Wl^T for one warp's 32 rows: X row-major (stride kLd),
+// Wl [N][K] row-major (stride ldw), fragments as mma m16n8k16 leaves them.
+template <int N, int K>
+AG_D void warp_layer(const __nv_bfloat16* X, const __nv_bfloat16* Wl, int ldw, float (&acc)[2][N / 8][4])
 {
-    __nv_bfloat16* cur = X;
-    __nv_bfloat16* nxt = tmp;
-    for (int l = 0; l < kLayers; ++l) {
-        if (saved) {
-            __syncwarp();
-            for (int i = threadIdx.x & 31; i < 32 * kHidden / 2; i += 32)
-                reinterpret_cast<uint32_t*>(saved + l * 32 * kHidden)[i] = reinterpret_cast<const uint32_t*>(cur)[i];
-        }
-        __syncwarp();
-        const __nv_bfloat16* Wl = W + layer_offset(l);
-        if (l < kLayers - 1) {
-            warp_gemm<32, kHidden, kHidden>(cur, kHidden, Wl, layer_in(l),
-                                            [&](int r, int c, float v) { nxt[r * kHidden + c] = bf(fmaxf(v, 0.0f)); });
-            __nv_bfloat16* t = cur;
-            cur = nxt;
-            nxt = t;
-        } else {
-            warp_gemm<32, kOut, kHidden>(cur, kHidden, Wl, layer_in(l),
-                                         [&](int r, int c, float v) { out[r * kOut + c] = v; });
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+        for (int nt = 0; nt < N / 8; ++nt) {
+            float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int ks = 0; ks < K / 16; ++ks) {
+                const __nv_bfloat16* a = X + (mt * 16 + g) * kLd + ks * 16 + 2 * t;
+                const __nv_bfloat16* b = Wl + (nt * 8 + g) * ldw + ks * 16 + 2 * t;
+                mma_bf16(c, ld32(a), ld32(a + 8 * kLd), ld32(a + 8), ld32(a + 8 * kLd + 8), ld32(b), ld32(b + 8));
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[mt][nt][k] = c[k];
         }
     }
-    __syncwarp();
+}
+
+// X = bf16(relu(acc)) (call after every lane has finished reading X).
+template <int N>
+AG_D void store_relu(__nv_bfloat16* X, const float (&acc)[2][N / 8][4])
+{
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < N / 8; ++nt) {
+            const int r = mt * 16 + g, col = nt * 8 + 2 * t;
+            *reinterpret_cast<uint32_t*>(X + r * kLd + col) =
+                pack_bf2(fmaxf(acc[mt][nt][0], 0.0f), fmaxf(acc[mt][nt][1], 0.0f));
+            *reinterpret_cast<uint32_t*>(X + (r + 8) * kLd + col) =
+                pack_bf2(fmaxf(acc[mt][nt][2], 0.0f), fmaxf(acc[mt][nt][3], 0.0f));
+        }
+}
+
+// Hidden layers of one warp's 32 rows in place; saved (optional) receives
+// the input of every layer ([kLayers][32][kLd]). Leaves the input of the
+// output layer in X.
+AG_D void hidden_layers(const __nv_bfloat16* W, __nv_bfloat16* X, __nv_bfloat16* saved)
+{
+    for (int l = 0; l < kLayers - 1; ++l) {
+        float acc[2][kHidden / 8][4];
+        warp_layer<kHidden, kHidden>(X, W + wsm_offset(l), wld(l), acc);
+        __syncwarp();
+        store_relu<kHidden>(saved ? saved + (l + 1) * 32 * kLd : X, acc);
+        if (saved) X = saved + (l + 1) * 32 * kLd;
+        __syncwarp();
+    }
 }
 
 // n queries, or *nDev when nDev is not null (a queue length written on the device).
@@ -75,52 +149,58 @@ __global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Quer
     if (nDev) n = min(n, *nDev);
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wbase = smem + kWeightCount * 2 + warp * (2 * 32 * kHidden * 2 + 32 * kOut * 4);
-    __nv_bfloat16* X = reinterpret_cast<__nv_bfloat16*>(wbase);
-    __nv_bfloat16* T = X + 32 * kHidden;
-    float* out = reinterpret_cast<float*>(T + 32 * kHidden);
-    for (int i = threadIdx.x; i < kWeightCount / 2; i += blockDim.x)
-        reinterpret_cast<uint32_t*>(W)[i] = reinterpret_cast<const uint32_t*>(g.W)[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+    __nv_bfloat16* X = W + kWsm + warp * 32 * kLd;
+    load_weights(g.W, W);
     __syncthreads();
     const uint32_t chunks = (n + 31) / 32;
     for (uint32_t ch = blockIdx.x * kInferWarps + warp; ch < chunks; ch += gridDim.x * kInferWarps) {
         const uint32_t i = ch * 32 + lane;
         if (i < n) {
-            encode_row(g, q[i], X + lane * kHidden);
+            encode_row(g, q[i], X + lane * kLd);
         } else {
-            for (int k = 0; k < kIn; ++k) X[lane * kHidden + k] = bf(0.0f);
+            for (int k = 0; k < kIn; ++k) X[lane * kLd + k] = bf(0.0f);
         }
-        forward32(W, X, T, out, nullptr);
-        if (i < n)
-            for (int k = 0; k < 40; ++k) raw[(uint64_t)i * 40 + k] = out[lane * kOut + k];
+        __syncwarp();
+        hidden_layers(W, X, nullptr);
+        float acc[2][kOut / 8][4];
+        warp_layer<kOut, kHidden>(X, W + wsm_offset(kLayers - 1), wld(kLayers - 1), acc);
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 5; ++nt) {  // columns 0..39
+                const int col = nt * 8 + 2 * t4;
+                const uint32_t r0 = ch * 32 + mt * 16 + g4, r1 = r0 + 8;
+                if (r0 < n) *reinterpret_cast<float2*>(raw + (uint64_t)r0 * 40 + col) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
+                if (r1 < n) *reinterpret_cast<float2*>(raw + (uint64_t)r1 * 40 + col) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
+            }
         __syncwarp();
     }
 }
 
 // Training: forward with saved activations, mixture gradient, backward with
-// tensor cores; dW accumulated per block in shared memory then merged into
-// the global gradient with atomics; grid gradients scattered with atomics.
-// Sample i of the batch is s[offset + i * stride].
+// tensor cores. dW is accumulated per block in shared memory and written to
+// the block's slice of `partial` (reduced by k_reduce_dw); grid gradients
+// are scattered with float2 atomics. Sample i of the batch is
+// s[offset + i * stride].
 __global__ void __launch_bounds__(32 * kTrainWarps) k_train(Params g, const Sample* __restrict__ s, uint32_t n,
-                                                          uint32_t offset, uint32_t stride,
-                                                          float invBatch, float* __restrict__ dW,
-                                                          float* __restrict__ dGrid, float* __restrict__ loss)
+                                                          uint32_t offset, uint32_t stride, float invBatch,
+                                                          float* __restrict__ partial, float* __restrict__ dGrid,
+                                                          float* __restrict__ loss)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(smem);
-    float* accW = reinterpret_cast<float*>(smem + kWeightCount * 2);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t perWarp = (size_t)kLayers * 32 * kHidden * 2 + 2 * 32 * kHidden * 2 + 2 * kHidden * 32 * 2;
-    unsigned char* wb = smem + kWeightCount * 2 + kWeightCount * 4 + warp * perWarp;
-    __nv_bfloat16* saved = reinterpret_cast<__nv_bfloat16*>(wb);       // [5][32][64]
-    __nv_bfloat16* G0 = saved + kLayers * 32 * kHidden;                // [32][64]
-    __nv_bfloat16* G1 = G0 + 32 * kHidden;                             // [32][64]
-    __nv_bfloat16* GT = G1 + 32 * kHidden;                             // [64][32] transposed gradient
-    __nv_bfloat16* XT = GT + kHidden * 32;                             // [64][32] transposed input
-    float* outF = reinterpret_cast<float*>(G0);                        // [32][48] fp32, aliases G0/G1
-    for (int i = threadIdx.x; i < kWeightCount / 2; i += blockDim.x)
-        reinterpret_cast<uint32_t*>(W)[i] = reinterpret_cast<const uint32_t*>(g.W)[i];
+    float* accW = reinterpret_cast<float*>(smem + kWsm * 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+    constexpr size_t perWarp = (size_t)kLayers * 32 * kLd * 2 + 32 * kLd * 2 + 2 * kHidden * kLdT * 2;
+    unsigned char* wb = smem + kWsm * 2 + kWeightCount * 4 + warp * perWarp;
+    __nv_bfloat16* saved = reinterpret_cast<__nv_bfloat16*>(wb);       // [5][32][kLd] layer inputs
+    __nv_bfloat16* G0 = saved + kLayers * 32 * kLd;                    // [32][kLd] gradient
+    __nv_bfloat16* GT = G0 + 32 * kLd;                                 // [64][kLdT] gradient, transposed
+    __nv_bfloat16* XT = GT + kHidden * kLdT;                           // [64][kLdT] layer input, transposed
+    float* outF = reinterpret_cast<float*>(G0);                        // [32][48] fp32 over G0 and GT
+    float* dIn = reinterpret_cast<float*>(XT);                         // [32][32] fp32 (after dW_0)
+    load_weights(g.W, W);
     for (int i = threadIdx.x; i < kWeightCount; i += blockDim.x) accW[i] = 0.0f;
     __syncthreads();
     float lossSum = 0.0f;
@@ -130,26 +210,25 @@ __global__ void __launch_bounds__(32 * kTrainWarps) k_train(Params g, const Samp
         const bool valid = i < n;
         Sample smp;
         if (valid) smp = s[offset + (uint64_t)i * stride];
-        __nv_bfloat16* X0 = saved;  // the encoded input is layer 0's saved input
-        if (valid) encode_row(g, smp.q, X0 + lane * kHidden);
+        if (valid) encode_row(g, smp.q, saved + lane * kLd);
         else
-            for (int k = 0; k < kIn; ++k) X0[lane * kHidden + k] = bf(0.0f);
-        // forward; saved[l] = input of layer l (saved[0] already holds X0)
+            for (int k = 0; k < kIn; ++k) saved[lane * kLd + k] = bf(0.0f);
+        __syncwarp();
+        hidden_layers(W, saved, saved);
         {
-            __nv_bfloat16* cur = X0;
-            for (int l = 0; l < kLayers; ++l) {
-                __syncwarp();
-                const __nv_bfloat16* Wl = W + layer_offset(l);
-                if (l < kLayers - 1) {
-                    __nv_bfloat16* nxt = saved + (l + 1) * 32 * kHidden;
-                    warp_gemm<32, kHidden, kHidden>(cur, kHidden, Wl, layer_in(l),
-                                                    [&](int r, int c, float v) { nxt[r * kHidden + c] = bf(fmaxf(v, 0.0f)); });
-                    cur = nxt;
-                } else {
-                    warp_gemm<32, kOut, kHidden>(cur, kHidden, Wl, layer_in(l),
-                                                 [&](int r, int c, float v) { outF[r * kOut + c] = v; });
+            float acc[2][kOut / 8][4];
+            warp_layer<kOut, kHidden>(saved + (kLayers - 1) * 32 * kLd, W + wsm_offset(kLayers - 1),
+                                      wld(kLayers - 1), acc);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < kOut / 8; ++nt) {
+                    const int r = mt * 16 + g4, col = nt * 8 + 2 * t4;
+                    outF[r * kOut + col] = acc[mt][nt][0];
+                    outF[r * kOut + col + 1] = acc[mt][nt][1];
+                    outF[(r + 8) * kOut + col] = acc[mt][nt][2];
+                    outF[(r + 8) * kOut + col + 1] = acc[mt][nt][3];
                 }
-            }
         }
         __syncwarp();
         // output gradient (lane = sample)
@@ -168,79 +247,83 @@ __global__ void __launch_bounds__(32 * kTrainWarps) k_train(Params g, const Samp
         __syncwarp();
         for (int k = 0; k < kOut; ++k) {
             __nv_bfloat16 v = bf(k < 40 ? grad[k] : 0.0f);
-            G0[lane * kHidden + k] = v;
-            GT[k * 32 + lane] = v;
+            G0[lane * kLd + k] = v;
+            GT[k * kLdT + lane] = v;
         }
-        // backward through the layers
-        __nv_bfloat16* dY = G0;
-        __nv_bfloat16* dX = G1;
+        // backward through the layers; G0 / GT hold dY of layer l
         for (int l = kLayers - 1; l >= 0; --l) {
             const int outDim = layer_out(l), inDim = layer_in(l);
-            const __nv_bfloat16* Xl = saved + l * 32 * kHidden;
+            const __nv_bfloat16* Xl = saved + l * 32 * kLd;
             __syncwarp();
             for (int e = lane; e < 32 * kHidden; e += 32) {  // XT = Xl^T
                 int r = e / kHidden, c = e % kHidden;
-                XT[c * 32 + r] = Xl[e];
+                XT[c * kLdT + r] = Xl[r * kLd + c];
             }
             __syncwarp();
             float* accL = accW + layer_offset(l);
             // dW_l[m][k] += sum_s dY[s][m] X_l[s][k]
             if (outDim == kOut)
-                warp_gemm<kOut, kHidden, 32>(GT, 32, XT, 32, [&](int r, int c, float v) { atomicAdd(&accL[r * inDim + c], v); });
+                warp_gemm<kOut, kHidden, 32>(GT, kLdT, XT, kLdT, [&](int r, int c, float v) { atomicAdd(&accL[r * inDim + c], v); });
             else
-                warp_gemm<kHidden, kHidden, 32>(GT, 32, XT, 32, [&](int r, int c, float v) { atomicAdd(&accL[r * inDim + c], v); });
+                warp_gemm<kHidden, kHidden, 32>(GT, kLdT, XT, kLdT, [&](int r, int c, float v) { atomicAdd(&accL[r * inDim + c], v); });
             if (l == 0) {
                 // input gradient of the grid features: dX0[s][k] = sum_m dY[s][m] W0[m][k], k < 32
-                float* dIn = reinterpret_cast<float*>(dX);  // [32][32] fp32 in the spare buffer
                 __syncwarp();
                 const __nv_bfloat16* WT0 = g.WT + layer_offset(0);
-                warp_gemm<32, kGridDims, kHidden>(dY, kHidden, WT0, layer_out(0),
+                warp_gemm<32, kGridDims, kHidden>(G0, kLd, WT0, layer_out(0),
                                                   [&](int r, int c, float v) { dIn[r * kGridDims + c] = v; });
                 __syncwarp();
                 if (valid) {
                     float3 p = normalise_position(g, mk3(smp.q.pos[0], smp.q.pos[1], smp.q.pos[2]));
                     for (int lv = 0; lv < kLevels; ++lv) {
                         float d0 = dIn[lane * kGridDims + 2 * lv], d1 = dIn[lane * kGridDims + 2 * lv + 1];
+#pragma unroll
                         for (int c = 0; c < 8; ++c) {
                             uint32_t idx;
                             float w;
                             grid_corner(g.res[lv], p, c, idx, w);
-                            float* dst = dGrid + ((uint64_t)lv * kTableSize + idx) * kFeatures;
-                            atomicAdd(dst, w * d0);
-                            atomicAdd(dst + 1, w * d1);
+                            float2* dst = reinterpret_cast<float2*>(dGrid + ((uint64_t)lv * kTableSize + idx) * kFeatures);
+                            atomicAdd(dst, make_float2(w * d0, w * d1));
                         }
                     }
                 }
                 break;
             }
-            // dX = dY W_l (through B^t = W_l^T, read from global), then ReLU'
+            // dX = dY W_l (B^t = W_l^T, read from global), then ReLU' of layer l-1
             const __nv_bfloat16* WTl = g.WT + layer_offset(l);
-            const __nv_bfloat16* Xrelu = Xl;  // input of layer l = relu output of layer l-1
+            float acc[2][kHidden / 8][4];
+            if (outDim == kOut) warp_layer<kHidden, kOut>(G0, WTl, kOut, acc);
+            else warp_layer<kHidden, kHidden>(G0, WTl, kHidden, acc);
             __syncwarp();
-            if (outDim == kOut)
-                warp_gemm<32, kHidden, kOut>(dY, kHidden, WTl, kOut, [&](int r, int c, float v) {
-                    dX[r * kHidden + c] = bf(fl(Xrelu[r * kHidden + c]) > 0.0f ? v : 0.0f);
-                });
-            else
-                warp_gemm<32, kHidden, kHidden>(dY, kHidden, WTl, kHidden, [&](int r, int c, float v) {
-                    dX[r * kHidden + c] = bf(fl(Xrelu[r * kHidden + c]) > 0.0f ? v : 0.0f);
-                });
-            __syncwarp();
-            for (int e = lane; e < 32 * kHidden; e += 32) {  // GT = dX^T
-                int r = e / kHidden, c = e % kHidden;
-                GT[c * 32 + r] = dX[e];
-            }
-            __nv_bfloat16* t = dY;
-            dY = dX;
-            dX = t;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < kHidden / 8; ++nt)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = mt * 16 + g4 + (k >> 1) * 8, c = nt * 8 + 2 * t4 + (k & 1);
+                        const __nv_bfloat16 v = bf(fl(Xl[r * kLd + c]) > 0.0f ? acc[mt][nt][k] : 0.0f);
+                        G0[r * kLd + c] = v;
+                        GT[c * kLdT + r] = v;
+                    }
         }
         __syncwarp();
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kWeightCount; i += blockDim.x)
-        if (accW[i] != 0.0f) atomicAdd(&dW[i], accW[i]);
+    float* mine = partial + (uint64_t)blockIdx.x * kWeightCount;
+    for (int i = threadIdx.x; i < kWeightCount; i += blockDim.x) mine[i] = accW[i];
     for (int o = 16; o; o >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, o);
     if (lane == 0 && loss) atomicAdd(loss, lossSum);
+}
+
+// dW[i] += sum over blocks of the blocks' partial dW (fixed order).
+__global__ void k_reduce_dw(const float* __restrict__ partial, uint32_t blocks, float* __restrict__ dW)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint32_t)kWeightCount) return;
+    float sum = 0.0f;
+    for (uint32_t b = 0; b < blocks; ++b) sum += partial[(uint64_t)b * kWeightCount + i];
+    dW[i] += sum;
 }
 
 // Adam (Kingma & Ba 2015) on fp32 master parameters; writes the compute copies.
@@ -298,12 +381,13 @@ __global__ void k_publish(const float* pw, uint32_t nw, __nv_bfloat16* W, __nv_b
     if (i < ng) h[i] = __float2half_rn(pg[i]);
 }
 
-size_t infer_smem() { return (size_t)kWeightCount * 2 + kInferWarps * (2 * 32 * kHidden * 2 + 32 * kOut * 4); }
+size_t infer_smem() { return (size_t)kWsm * 2 + (size_t)kInferWarps * 32 * kLd * 2; }
 size_t train_smem()
 {
-    size_t perWarp = (size_t)kLayers * 32 * kHidden * 2 + 2 * 32 * kHidden * 2 + 2 * kHidden * 32 * 2;
-    return (size_t)kWeightCount * 2 + (size_t)kWeightCount * 4 + kTrainWarps * perWarp;
+    size_t perWarp = (size_t)kLayers * 32 * kLd * 2 + 32 * kLd * 2 + 2 * kHidden * kLdT * 2;
+    return (size_t)kWsm * 2 + (size_t)kWeightCount * 4 + kTrainWarps * perWarp;
 }
+constexpr uint32_t kMaxTrainBlocks = 296;
 
 uint64_t splitmix(uint64_t& s)
 {
@@ -333,6 +417,7 @@ bool Guide::allocate()
     bytes += kGridParams * sizeof(__half);                // grid compute copy
     bytes += 4 * (size_t)kWeightCount * sizeof(float);    // W master, m, v, grad
     bytes += 2 * (size_t)kWeightCount * sizeof(__nv_bfloat16);
+    bytes += (size_t)kMaxTrainBlocks * kWeightCount * sizeof(float);  // per-block dW partials
     bytes += 256 * 8;
     if (cudaMalloc(&mem_, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -356,6 +441,7 @@ bool Guide::allocate()
     wG_ = (float*)take(kWeightCount * 4);
     wB_ = (__nv_bfloat16*)take(kWeightCount * 2);
     wT_ = (__nv_bfloat16*)take(kWeightCount * 2);
+    partial_ = (float*)take((size_t)kMaxTrainBlocks * kWeightCount * 4);
     loss_ = (float*)take(256);
     return true;
 }
@@ -425,7 +511,7 @@ void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, fl
     cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
     uint32_t chunks = (maxN + 31) / 32;
     uint32_t blocks = (chunks + kInferWarps - 1) / kInferWarps;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > 148 * 2) blocks = 148 * 2;  // two resident blocks per SM; each loads the weights once
     k_infer<<<blocks, 32 * kInferWarps, infer_smem(), st>>>(params(), q, maxN, count, raw);
 }
 
@@ -433,12 +519,16 @@ void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cu
                                  uint32_t stride)
 {
     if (n == 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
     uint32_t chunks = (n + 31) / 32;
     uint32_t blocks = (chunks + kTrainWarps - 1) / kTrainWarps;
-    if (blocks > 148 * 4) blocks = 148 * 4;
-    k_train<<<blocks, 32 * kTrainWarps, train_smem(), st>>>(params(), s, n, offset, stride, invBatch, wG_, gridG_,
-                                                            loss_);
+    blocks = std::min<uint32_t>(blocks, std::min<uint32_t>((uint32_t)sms, kMaxTrainBlocks));
+    k_train<<<blocks, 32 * kTrainWarps, train_smem(), st>>>(params(), s, n, offset, stride, invBatch, partial_,
+                                                            gridG_, loss_);
+    k_reduce_dw<<<(kWeightCount + 255) / 256, 256, 0, st>>>(partial_, blocks, wG_);
 }
 
 void Guide::apply_adam(float lr, cudaStream_t st)

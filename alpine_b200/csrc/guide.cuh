@@ -163,18 +163,35 @@ AG_HD float mixture_pdf(const Mixture& m, float3 w)
 
 AG_HD float3 mixture_sample(const Mixture& m, float u0, float u1, float u2)
 {
-    int k = 0;
-    float c = m.lambda[0];
-    while (k < kLobes - 1 && u0 >= c) c += m.lambda[++k];
-    const float kappa = m.kappa[k];
+    // lobe: the first k with u0 < lambda_0 + ... + lambda_k (the last one if
+    // rounding leaves u0 above the total), selected without dynamic indexing
+    int k = kLobes - 1;
+    float c = 0.0f;
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < kLobes; ++j) {
+        c += m.lambda[j];
+        if (!found && u0 < c) {
+            k = j;
+            found = true;
+        }
+    }
+    float kappa = m.kappa[0];
+    float3 mu = m.mu[0];
+#pragma unroll
+    for (int j = 1; j < kLobes; ++j)
+        if (k == j) {
+            kappa = m.kappa[j];
+            mu = m.mu[j];
+        }
     // cos(theta) by inverting the CDF (Jakob 2012)
     float wc = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
     wc = fminf(fmaxf(wc, -1.0f), 1.0f);
     float st = sqrtf(fmaxf(0.0f, 1.0f - wc * wc));
     float phi = 2.0f * kPi * u2;
     float3 t1, t2;
-    get_basis(m.mu[k], t1, t2);
-    return t1 * (st * cosf(phi)) + t2 * (st * sinf(phi)) + m.mu[k] * wc;
+    get_basis(mu, t1, t2);
+    return t1 * (st * cosf(phi)) + t2 * (st * sinf(phi)) + mu * wc;
 }
 
 // d(-w log q)/d raw for one sample direction w (q = mixture pdf).

@@ -68,17 +68,25 @@ int alpine_gpu_guide_reset(alpine_gpu_ctx* c, uint32_t seed, const float lo[3], 
     if (!c || !lo || !hi) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     c->guideSeed = seed;
+    c->guideLastLossSteps = 0;
     if (c->guide.reset(seed, c->stream) != 0) return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide: reset failed");
     c->guide.set_scene_box(make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]));
     c->guideBoxSet = true;
     return ALPINE_GPU_OK;
 }
 
-int alpine_gpu_guide_steps(alpine_gpu_ctx* c, uint32_t* adam_steps, uint32_t* guided_waves)
+int alpine_gpu_guide_steps(alpine_gpu_ctx* c, uint32_t* adam_steps, uint32_t* guided_waves, float* last_loss)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (adam_steps) *adam_steps = c->guide.steps();
     if (guided_waves) *guided_waves = c->guideWaveIndex;
+    if (last_loss) {
+        // hStatus[2] is written by the render's last training pass, complete
+        // once the render has synchronised
+        float sum;
+        std::memcpy(&sum, c->hStatus + 2, sizeof(float));
+        *last_loss = c->guideLastLossSteps ? sum / (float)c->guideLastLossSteps : 0.0f;
+    }
     return ALPINE_GPU_OK;
 }
 

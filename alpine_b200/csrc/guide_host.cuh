@@ -29,6 +29,12 @@ public:
     void apply_adam(float lr, cudaStream_t st);
     // gradients + Adam; returns the batch loss (synchronises).
     float train_step(const Sample* s, uint32_t n, float lr, cudaStream_t st);
+    // Sum of the batch losses of the gradient passes since reset_loss.
+    void reset_loss(cudaStream_t st) { cudaMemsetAsync(loss_, 0, 4, st); }
+    void read_loss_async(float* hostPinned, cudaStream_t st) const
+    {
+        cudaMemcpyAsync(hostPinned, loss_, 4, cudaMemcpyDeviceToHost, st);
+    }
     // Recomputes the BF16 / FP16 compute copies from the FP32 masters.
     void publish(cudaStream_t st);
 
@@ -56,6 +62,7 @@ private:
     float* wG_ = nullptr;
     __nv_bfloat16* wB_ = nullptr;
     __nv_bfloat16* wT_ = nullptr;
+    float* partial_ = nullptr;
     float* loss_ = nullptr;
     float3 bmin_ = make_float3(0.0f, 0.0f, 0.0f);
     float3 invExtent_ = make_float3(1.0f, 1.0f, 1.0f);

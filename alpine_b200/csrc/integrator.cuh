@@ -73,9 +73,12 @@ struct WaveView {
     // persistent per-pixel reference RNG state (stream mode)
     uint4* pixelRng;
     // learned guiding (counter RNG only)
-    guide::Query* guideQuery;  // per queue entry; null = guiding off
-    const float* guideRaw;     // per queue entry: 40 mixture parameters; null = material sampling only
+    guide::Query* guideQuery;  // compacted queries of the guided vertices; null = guiding off
+    int* guideSlot;            // per queue entry: index into guideQuery / guideRaw, -1 = not guided
+    uint32_t* guideCount;      // number of guided vertices of the current queue
+    const float* guideRaw;     // per guided vertex: 40 mixture parameters; null = material sampling only
     float guideFraction;       // probability of sampling the guide at an eligible vertex
+    float guideMinRough;       // eligible vertices: material alpha >= this
     guide::Sample* trainRec;   // recorded vertices: query, direction (weight filled by finalize)
     float4* trainAux;          // 2 per record: (radiance after the vertex, path bits), (throughput at it, 0)
     int* trainSlot;            // per path: record waiting for its radiance-after value, -1 = none
@@ -264,30 +267,39 @@ AG_D bool guided_continuation(const Material& mat, float3 wo, const float* raw, 
     return true;
 }
 
-// Guide queries of the current queue: shading position, roughness, direction
-// towards the previous vertex and shading normal (zeros for misses).
+// Guide queries of the vertices of the current queue that will be guided
+// (a hit, the view direction above the shading surface, material alpha >=
+// guideMinRough), compacted: shading position, roughness, direction towards
+// the previous vertex and shading normal.
 __global__ void __launch_bounds__(kThreads) k_guide_query(SceneView sc, WaveView w)
 {
     const uint32_t n = *w.queueCount;
     uint32_t q = blockIdx.x * kThreads + threadIdx.x;
     if (q >= n) return;
     const uint4 h = w.hits[q];
+    bool guided = false;
     guide::Query gq = {};
     if (h.x != 0xffffffffu) {
         const alpine_gpu_ray ray = w.rays[q];
         Surface sf;
         surface_at(sc, h, sf);
-        const float t = __uint_as_float(h.y);
-        const float3 ro = mk3(ray.org[0], ray.org[1], ray.org[2]);
         const float3 rd = mk3(ray.dir[0], ray.dir[1], ray.dir[2]);
-        const float3 hit = ro + rd * t;
-        const float3 wo = normalize3(-rd);
-        gq.pos[0] = hit.x; gq.pos[1] = hit.y; gq.pos[2] = hit.z;
-        gq.rough = sf.mat.ax;
-        gq.wo[0] = wo.x; gq.wo[1] = wo.y; gq.wo[2] = wo.z;
-        gq.n[0] = sf.ns.x; gq.n[1] = sf.ns.y; gq.n[2] = sf.ns.z;
+        // wo.z of the shading frame: to_local(-rd, ss, ts, ns).z
+        guided = dot(sf.ns, -rd) > 0.0f && sf.mat.ax >= w.guideMinRough;
+        if (guided) {
+            const float t = __uint_as_float(h.y);
+            const float3 ro = mk3(ray.org[0], ray.org[1], ray.org[2]);
+            const float3 hit = ro + rd * t;
+            const float3 wo = normalize3(-rd);
+            gq.pos[0] = hit.x; gq.pos[1] = hit.y; gq.pos[2] = hit.z;
+            gq.rough = sf.mat.ax;
+            gq.wo[0] = wo.x; gq.wo[1] = wo.y; gq.wo[2] = wo.z;
+            gq.n[0] = sf.ns.x; gq.n[1] = sf.ns.y; gq.n[2] = sf.ns.z;
+        }
     }
-    w.guideQuery[q] = gq;
+    const uint32_t slot = warp_append(w.guideCount, guided);
+    if (guided) w.guideQuery[slot] = gq;
+    w.guideSlot[q] = guided ? (int)slot : -1;
 }
 
 template <bool kGuided>
@@ -386,8 +398,12 @@ __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bo
         // between the guide and the material's procedure
         bool ok;
         float3 wiL, est;
-        if (kGuided && w.guideRaw && wo.z > 0.0f) {
-            ok = guided_continuation(mat, wo, w.guideRaw + 40ull * q, w.guideFraction, ss, ts, ns, rng, wiL, est);
+        // guided when the query kernel selected the vertex (and wo.z > 0 here
+        // as well, should contraction round the two tests differently)
+        const int gslot = kGuided ? w.guideSlot[q] : -1;
+        const bool guidable = gslot >= 0 && wo.z > 0.0f;
+        if (guidable && w.guideRaw) {
+            ok = guided_continuation(mat, wo, w.guideRaw + 40ull * gslot, w.guideFraction, ss, ts, ns, rng, wiL, est);
         } else {
             BsdfSample ms;
             float cu0 = rng.next();
@@ -415,13 +431,13 @@ __global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bo
                 }
                 // training record: the radiance this direction brings is
                 // (R_final - R_after) / throughput at the vertex
-                const bool rec = cont && w.trainStride &&
+                const bool rec = cont && guidable && w.trainStride &&
                                  (uint32_t)(splitmix64(((uint64_t)w.waveIndex << 32) | p) % w.trainStride) == 0u;
                 if (kGuided && w.trainStride) {
                     const uint32_t r = warp_append(w.trainCount, rec);
                     if (rec && r < w.trainCap) {
                         guide::Sample smp;
-                        smp.q = w.guideQuery[q];
+                        smp.q = w.guideQuery[gslot];
                         const float3 d = normalize3(wiW);
                         smp.dir[0] = d.x; smp.dir[1] = d.y; smp.dir[2] = d.z;
                         smp.weight = 0.0f;

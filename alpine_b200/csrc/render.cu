@@ -336,18 +336,19 @@ ag::WaveView carve_wave(alpine_gpu_ctx* c)
 // Guiding buffers for `paths` paths and `cap` training records.
 struct GuideWave {
     ag::guide::Query* query;
+    int* querySlot;      // per queue entry
     float* raw;
     int* slot;
     ag::guide::Sample* rec;
     float4* aux;
     ag::guide::Sample* out;
-    uint32_t* counters;  // [0] records, [1] kept samples
+    uint32_t* counters;  // [0] records, [1] kept samples, [2] guided vertices of the queue
 };
 
 bool reserve_guide_wave(alpine_gpu_ctx* c, uint32_t paths, uint32_t cap, GuideWave& g)
 {
     size_t P = paths, R = cap;
-    size_t bytes = round256(P * sizeof(ag::guide::Query)) + round256(P * 40 * sizeof(float)) +
+    size_t bytes = round256(P * sizeof(ag::guide::Query)) + round256(P * sizeof(int)) + round256(P * 40 * sizeof(float)) +
                    round256(P * sizeof(int)) + round256(R * sizeof(ag::guide::Sample)) +
                    round256(2 * R * sizeof(float4)) + round256(R * sizeof(ag::guide::Sample)) + 256;
     if (!c->dGuideWave.reserve(bytes)) return false;
@@ -358,6 +359,7 @@ bool reserve_guide_wave(alpine_gpu_ctx* c, uint32_t paths, uint32_t cap, GuideWa
         return r;
     };
     g.query = (ag::guide::Query*)take(P * sizeof(ag::guide::Query));
+    g.querySlot = (int*)take(P * sizeof(int));
     g.raw = (float*)take(P * 40 * sizeof(float));
     g.slot = (int*)take(P * sizeof(int));
     g.rec = (ag::guide::Sample*)take(R * sizeof(ag::guide::Sample));
@@ -424,11 +426,14 @@ int train_guide(alpine_gpu_ctx* c, const ag::IntegratorKernels& K, const ag::Wav
     kept = std::min(c->hStatus[1], w.trainCap);
     if (kept == 0) return ALPINE_GPU_OK;
     const uint32_t steps = std::min(maxSteps, (kept + batch - 1) / batch);
+    c->guide.reset_loss(st);
     for (uint32_t i = 0; i < steps; ++i) {
         const uint32_t n = (kept - i + steps - 1) / steps;
         c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, steps);
         c->guide.apply_adam(lr, st);
     }
+    c->guideLastLossSteps = steps;
+    c->guide.read_loss_async(reinterpret_cast<float*>(c->hStatus + 2), st);  // read after the next synchronisation
     return ALPINE_GPU_OK;
 }
 
@@ -642,16 +647,18 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
     uint32_t S = stream ? 1u : std::max(1u, std::min(spp, maxPaths / std::max(1u, pixels)));
     const alpine_gpu_render_options& o = c->options;
     const bool guiding = !stream && o.guide != 0;
-    const bool training = guiding && o.guide_train != 0;
+    const bool trainEnabled = guiding && o.guide_train != 0;
     const uint32_t gBatch = o.guide_batch ? o.guide_batch : 16384u;
     const uint32_t gSteps = o.guide_steps_per_wave ? o.guide_steps_per_wave : 8u;
     const float gLr = o.guide_lr > 0.0f ? o.guide_lr : 1e-2f;
     const float gFrac = o.guide_fraction > 0.0f ? std::min(o.guide_fraction, 1.0f) : 0.5f;
-    if (guiding) S = std::min(S, o.guide_spp_per_wave ? o.guide_spp_per_wave : 1u);
+    // waves while the guide trains hold few samples per pixel, so that
+    // training happens often; afterwards they are as large as unguided ones
+    const uint32_t sTrain = std::min(S, o.guide_spp_per_wave ? o.guide_spp_per_wave : 1u);
     uint32_t pixelChunk = std::min(pixels, maxPaths / S);
     if (!reserve_wave(c, S * pixelChunk)) return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "wave buffers");
     GuideWave gw{};
-    const uint32_t trainCap = training ? std::min<uint32_t>(1u << 21, 2u * gSteps * gBatch) : 0u;
+    const uint32_t trainCap = trainEnabled ? std::min<uint32_t>(1u << 21, 2u * gSteps * gBatch) : 0u;
     if (guiding) {
         if (!c->guide.ready() && c->guide.reset(c->guideSeed, c->stream) != 0)
             return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide: parameter allocation failed");
@@ -697,7 +704,8 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
     double* acc64 = fp64 ? c->dAccum.as<double>() : nullptr;
     cudaStream_t st = c->stream;
     for (uint32_t done = 0; done < spp;) {
-        const uint32_t s = std::min(S, spp - done);
+        const bool trainNow = trainEnabled && (o.guide_train_steps == 0 || c->guide.steps() < o.guide_train_steps);
+        const uint32_t s = std::min(trainNow ? sTrain : S, spp - done);
         for (uint32_t px = 0; px < pixels; px += pixelChunk) {
             ag::WaveView w = carve_wave(c);
             w.numPixels = std::min(pixelChunk, pixels - px);
@@ -709,10 +717,14 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
             w.rrStart = stream ? 0u : c->options.russian_roulette_depth;
             w.pixelRng = c->dPixelRng.as<uint4>();
             const bool sampleGuide = guiding && c->guide.steps() >= o.guide_warmup_steps;
+            const bool training = trainNow && (o.guide_train_steps == 0 || c->guide.steps() < o.guide_train_steps);
             if (guiding) {
                 w.guideQuery = gw.query;
+                w.guideSlot = gw.querySlot;
+                w.guideCount = gw.counters + 2;
                 w.guideRaw = sampleGuide ? gw.raw : nullptr;
                 w.guideFraction = gFrac;
+                w.guideMinRough = o.guide_min_roughness;
             }
             if (training) {
                 // record about trainCap vertices: ~3 continuations per path
@@ -733,8 +745,9 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
                 cudaMemsetAsync(w.queueCountNext, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(w.shadowCount, 0, sizeof(uint32_t), st);
                 if (guiding) {
+                    cudaMemsetAsync(w.guideCount, 0, sizeof(uint32_t), st);
                     K.guide_query(sc, w, w.numPaths, st);
-                    if (sampleGuide) c->guide.infer_queue(gw.query, w.queueCount, w.numPaths, gw.raw, st);
+                    if (sampleGuide) c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.raw, st);
                 }
                 K.shade(sc, w, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,
@@ -747,7 +760,9 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
             K.accumulate(w, acc32, acc64, stream, st);
             if (guiding) ++c->guideWaveIndex;
             if (training) {
-                if (int rc = train_guide(c, K, w, gw, gBatch, gSteps, gLr)) return rc;
+                uint32_t steps = gSteps;
+                if (o.guide_train_steps) steps = std::min(steps, o.guide_train_steps - c->guide.steps());
+                if (int rc = train_guide(c, K, w, gw, gBatch, steps, gLr)) return rc;
             }
         }
         done += s;

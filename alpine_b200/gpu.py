@@ -52,7 +52,8 @@ class RenderOptions(C.Structure):
                 ("seed", C.c_uint32), ("accumulate_fp64", C.c_uint32), ("guide", C.c_uint32),
                 ("guide_fraction", C.c_float), ("guide_train", C.c_uint32), ("guide_batch", C.c_uint32),
                 ("guide_lr", C.c_float), ("guide_warmup_steps", C.c_uint32), ("guide_spp_per_wave", C.c_uint32),
-                ("guide_steps_per_wave", C.c_uint32)]
+                ("guide_steps_per_wave", C.c_uint32), ("guide_min_roughness", C.c_float),
+                ("guide_train_steps", C.c_uint32)]
 
 
 MATERIAL_DTYPE = np.dtype([("kind", np.uint32), ("base_color", np.float32, 3), ("roughness", np.float32)])
@@ -114,7 +115,7 @@ def lib():
         L.alpine_gpu_guide_dims.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32p]
         L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
-        L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p]
+        L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p, C.POINTER(C.c_float)]
         L.alpine_gpu_guide_gradients.argtypes = [vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_guide_train.argtypes = [vp, vp, C.c_uint32, C.c_float, f3]
         L.alpine_gpu_guide_get_weights.argtypes = [vp, vp]
@@ -303,12 +304,12 @@ class Context:
     def set_render_options(self, sampler=RNG_COUNTER, max_paths_per_wave=0, russian_roulette_depth=0, seed=0,
                            accumulate_fp64=False, guide=False, guide_fraction=0.5, guide_train=True,
                            guide_batch=16384, guide_lr=1e-2, guide_warmup_steps=0, guide_spp_per_wave=1,
-                           guide_steps_per_wave=8):
+                           guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0):
         """Options of alpine_gpu_render_options; the guide_* fields apply when
         guide is set (learned path guiding, counter sampler only)."""
         o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64),
                           int(guide), guide_fraction, int(guide_train), guide_batch, guide_lr, guide_warmup_steps,
-                          guide_spp_per_wave, guide_steps_per_wave)
+                          guide_spp_per_wave, guide_steps_per_wave, guide_min_roughness, guide_train_steps)
         self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
 
     def reset_accumulation(self):
@@ -346,11 +347,12 @@ class Context:
     def guide_reset(self, seed, lo, hi):
         self._check(self.L.alpine_gpu_guide_reset(self.h, seed, _f3(lo), _f3(hi)))
 
-    def guide_steps(self):
-        """(Adam steps since the last reset, waves rendered with guiding)."""
-        a, b = C.c_uint32(), C.c_uint32()
-        self._check(self.L.alpine_gpu_guide_steps(self.h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+    def guide_steps(self, with_loss=False):
+        """(Adam steps since the last reset, waves rendered with guiding[, mean
+        loss of the last trained wave])."""
+        a, b, l = C.c_uint32(), C.c_uint32(), C.c_float()
+        self._check(self.L.alpine_gpu_guide_steps(self.h, C.byref(a), C.byref(b), C.byref(l)))
+        return (a.value, b.value, l.value) if with_loss else (a.value, b.value)
 
     def guide_infer(self, queries):
         q = np.ascontiguousarray(queries, np.float32).reshape(-1, 12)

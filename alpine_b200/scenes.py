@@ -158,25 +158,21 @@ def rotate_y(v, angle, center):
 
 
 def uv_sphere(center, radius, segments=64, bands=32):
-    """UV sphere with smooth per-vertex normals; pole bands are triangle fans."""
-    verts, norms = [], []
-    for j in range(bands + 1):
-        th = math.pi * j / bands
-        for i in range(segments):
-            ph = 2 * math.pi * i / segments
-            n = (math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph))
-            norms.append(n)
-            verts.append([center[k] + radius * n[k] for k in range(3)])
-    tris = []
-    idx = lambda j, i: j * segments + (i % segments)
-    for j in range(bands):
-        for i in range(segments):
-            a, b, c, d = idx(j, i), idx(j, i + 1), idx(j + 1, i + 1), idx(j + 1, i)
-            if j != 0:
-                tris.append((a, b, c))
-            if j != bands - 1:
-                tris.append((a, c, d))
-    return (np.array(verts, np.float32), np.array(tris, np.uint32), np.array(norms, np.float32))
+    """UV sphere with smooth per-vertex normals; pole bands are triangle fans.
+    Vertex (band j, segment i) is number j * segments + i."""
+    th = math.pi * np.arange(bands + 1, dtype=np.float64) / bands
+    ph = 2 * math.pi * np.arange(segments, dtype=np.float64) / segments
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    n = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], -1).reshape(-1, 3)
+    verts = (np.asarray(center, np.float64) + radius * n).astype(np.float32)
+    J, I = np.meshgrid(np.arange(bands), np.arange(segments), indexing="ij")
+    a, b = J * segments + I, J * segments + (I + 1) % segments
+    c, d = (J + 1) * segments + (I + 1) % segments, (J + 1) * segments + I
+    t1 = np.stack([a, b, c], -1)
+    t2 = np.stack([a, c, d], -1)
+    keep = np.stack([J != 0, J != bands - 1], -1)        # per (j, i): first, second triangle
+    tris = np.stack([t1, t2], 2)[keep]                   # row-major: (j, i, k) order
+    return verts, tris.astype(np.uint32), n.astype(np.float32)
 
 
 def room_scene(seed=1, light="disk", sphere_segments=64, sphere_bands=32):
@@ -225,6 +221,97 @@ def room_scene(seed=1, light="disk", sphere_segments=64, sphere_bands=32):
     camera = ((0.0, 0.0, -0.95), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), math.radians(70.0))
     return {"meshes": meshes, "materials": materials, "lights": lights, "camera": camera,
             "background": (0.0, 0.0, 0.0)}
+
+
+def wall_with_openings(x, z_range, y_range, openings):
+    """Quads of the plane x = const over z_range x y_range minus the
+    rectangular openings [(z0, z1, y0, y1), ...]; normals cross(e0, e1)
+    point to +x."""
+    zs = sorted({z_range[0], z_range[1], *[o[0] for o in openings], *[o[1] for o in openings]})
+    ys = sorted({y_range[0], y_range[1], *[o[2] for o in openings], *[o[3] for o in openings]})
+    verts, tris = [], []
+    for i in range(len(zs) - 1):
+        for j in range(len(ys) - 1):
+            zc, yc = 0.5 * (zs[i] + zs[i + 1]), 0.5 * (ys[j] + ys[j + 1])
+            if any(o[0] < zc < o[1] and o[2] < yc < o[3] for o in openings):
+                continue
+            b = len(verts)
+            verts += [(x, ys[j], zs[i]), (x, ys[j], zs[i + 1]), (x, ys[j + 1], zs[i + 1]), (x, ys[j + 1], zs[i])]
+            tris += [(b, b + 2, b + 1), (b, b + 3, b + 2)]
+    return np.array(verts, np.float32), np.array(tris, np.uint32)
+
+
+def glossy_interior_scene(seed=1, target_tris=2_000_000, n_boxes=80, n_spheres=24, glossy_fraction=0.7,
+                          sky=5.0, roughness=(0.02, 0.4), glossy_floor=True):
+    """Glossy interior: a closed 20 x 4 x 12 m room (x in [-10, 10], y in
+    [0, 4], z in [-6, 6]) of about `target_tris` triangles made of seeded
+    furniture boxes and subdivided UV spheres (`roughness`: the GGX range,
+    `glossy_floor`: whether the floor is GGX). Light comes only through two
+    1 x 2 m window openings in the x = -10 wall, from a constant sky of
+    radiance `sky` (the background radiance of rays that escape, added at any
+    depth; there are no light sources, so next-event estimation finds none of
+    it). A `glossy_fraction` of the objects, and the floor, are GGX conductors
+    with roughness uniform in [0.02, 0.4]; the rest, walls and ceiling are
+    Lambertian."""
+    rng = np.random.default_rng(seed)
+    meshes, materials = [], []
+
+    def surface():
+        if rng.random() < glossy_fraction:
+            return (1, tuple(float(x) for x in rng.uniform(0.5, 0.95, 3)), float(rng.uniform(*roughness)))
+        return (0, tuple(float(x) for x in rng.uniform(0.3, 0.8, 3)), 1.0)
+
+    rv, ri = box_mesh((-10.0, 0.0, -6.0), (10.0, 4.0, 6.0), inward=True)
+    # box_mesh face order: z0, z1, x0, x1, y0 (floor), y1 (ceiling); x0 is
+    # replaced by the wall with the window openings
+    keep = [0, 1, 3, 4, 5]
+    face_mats = {}
+    for f in keep:
+        if f == 4 and glossy_floor:
+            materials.append((1, (0.8, 0.8, 0.8), float(rng.uniform(*roughness))))
+        else:
+            materials.append((0, tuple(float(x) for x in rng.uniform(0.5, 0.8, 3)), 1.0))
+        face_mats[f] = len(materials) - 1
+    sel = np.concatenate([[2 * f, 2 * f + 1] for f in keep])
+    meshes.append({"verts": rv, "idx": ri[sel], "normals": None,
+                   "tri_material": np.repeat(np.array([face_mats[f] for f in keep], np.uint32), 2)})
+    openings = [(zc - 0.5, zc + 0.5, 1.0, 3.0) for zc in (-3.0, 2.0)]
+    wv, wi = wall_with_openings(-10.0, (-6.0, 6.0), (0.0, 4.0), openings)
+    materials.append((0, tuple(float(x) for x in rng.uniform(0.5, 0.8, 3)), 1.0))
+    meshes.append({"verts": wv, "idx": wi, "normals": None,
+                   "tri_material": np.full(wi.shape[0], len(materials) - 1, np.uint32)})
+    eye = (9.6, 3.5, 5.6)
+
+    def placed(lo_x, hi_x, lo_z, hi_z):  # a centre at least 3 m (x-z) from the camera
+        while True:
+            x, z = rng.uniform(lo_x, hi_x), rng.uniform(lo_z, hi_z)
+            if (x - eye[0]) ** 2 + (z - eye[2]) ** 2 > 9.0:
+                return x, z
+
+    for _ in range(n_boxes):
+        w, dpt = rng.uniform(0.4, 2.5, 2)
+        h = rng.uniform(0.3, 2.2)
+        cx, cz = placed(-8.5, 9.0, -5.0, 5.0)
+        lo, hi = (cx - w / 2, 0.0, cz - dpt / 2), (cx + w / 2, h, cz + dpt / 2)
+        bv, bi = box_mesh(lo, hi)
+        bv = rotate_y(bv, float(rng.uniform(0, math.pi / 2)), np.array([cx, 0.0, cz]))
+        materials.append(surface())
+        meshes.append({"verts": bv, "idx": bi, "normals": None,
+                       "tri_material": np.full(bi.shape[0], len(materials) - 1, np.uint32)})
+    used = sum(m["idx"].shape[0] for m in meshes)
+    per = max(64, (target_tris - used) // max(1, n_spheres))
+    bands = max(4, int(round(math.sqrt(per / 4.0))))
+    for _ in range(n_spheres):
+        r = float(rng.uniform(0.2, 0.9))
+        x, z = placed(-8.5, 9.0, -5.0, 5.0)
+        ctr = (float(x), r + float(rng.uniform(0.0, 1.5)), float(z))
+        sv, si, sn = uv_sphere(ctr, r, 2 * bands, bands)
+        materials.append(surface())
+        meshes.append({"verts": sv, "idx": si, "normals": sn,
+                       "tri_material": np.full(si.shape[0], len(materials) - 1, np.uint32)})
+    camera = (eye, (-10.0, 1.0, -1.0), (0.0, 1.0, 0.0), math.radians(60.0))
+    return {"meshes": meshes, "materials": materials, "lights": [], "camera": camera,
+            "background": (sky, sky, sky)}
 
 
 def add_random_lights(scene, n, seed=5, kinds=("disk", "point")):

@@ -258,9 +258,16 @@ ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3]
  * guide_warmup_steps: the guide is sampled only after this many Adam steps
  *   (before that, vertices use the material's procedure and are recorded for
  *   training).
- * guide_spp_per_wave: samples per pixel per wave while guiding (training
- *   happens between waves); 0 = 1.
- * guide_steps_per_wave: at most this many Adam steps after a wave; 0 = 8. */
+ * guide_spp_per_wave: samples per pixel per wave while the guide trains
+ *   (training happens between waves); 0 = 1. Later waves are as large as
+ *   unguided ones.
+ * guide_steps_per_wave: at most this many Adam steps after a wave; 0 = 8.
+ * guide_min_roughness: vertices whose microfacet alpha is below this use the
+ *   material's procedure only and are not recorded for training (a
+ *   near-specular lobe is already sampled well and is narrower than the
+ *   guide's lobes); 0 = guide every vertex.
+ * guide_train_steps: stop training after this many Adam steps since the
+ *   guide's last reset (the guide is then used as it is); 0 = no limit. */
 #define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
 #define ALPINE_GPU_SAMPLER_COUNTER 1u
 typedef struct alpine_gpu_render_options {
@@ -277,6 +284,8 @@ typedef struct alpine_gpu_render_options {
     uint32_t guide_warmup_steps;
     uint32_t guide_spp_per_wave;
     uint32_t guide_steps_per_wave;
+    float guide_min_roughness;
+    uint32_t guide_train_steps;
 } alpine_gpu_render_options;
 ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
 
@@ -313,8 +322,11 @@ ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_
 ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],
                                           const float scene_hi[3]);
 ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw);
-/* Adam steps taken since the last reset and waves rendered with guiding. */
-ALPINE_GPU_API int alpine_gpu_guide_steps(alpine_gpu_ctx* ctx, uint32_t* adam_steps, uint32_t* guided_waves);
+/* Adam steps taken since the last reset, waves rendered with guiding, and the
+ * mean training loss (KL divergence up to a constant) of the last trained
+ * wave's steps (0 before any). Any pointer may be NULL. */
+ALPINE_GPU_API int alpine_gpu_guide_steps(alpine_gpu_ctx* ctx, uint32_t* adam_steps, uint32_t* guided_waves,
+                                          float* last_loss);
 ALPINE_GPU_API int alpine_gpu_guide_gradients(alpine_gpu_ctx* ctx, const float* samples, uint32_t count, float* dW,
                                               const uint64_t* grid_index, uint32_t grid_count, float* grid_grad,
                                               float* loss);
