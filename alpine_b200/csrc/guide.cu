@@ -381,6 +381,15 @@ __global__ void k_publish(const float* pw, uint32_t nw, __nv_bfloat16* W, __nv_b
     if (i < ng) h[i] = __float2half_rn(pg[i]);
 }
 
+// Grid parameters uniform in [-1e-4, 1e-4], from a hash of (seed, index).
+__global__ void k_init_grid(float* p, uint64_t n, uint64_t seed)
+{
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t h = splitmix64(seed * 0x9e3779b97f4a7c15ull + i);
+    p[i] = (2.0f * ((float)(h >> 40) * (1.0f / 16777216.0f)) - 1.0f) * 1e-4f;
+}
+
 size_t infer_smem() { return (size_t)kWsm * 2 + (size_t)kInferWarps * 32 * kLd * 2; }
 size_t train_smem()
 {
@@ -456,10 +465,11 @@ int Guide::reset(uint32_t seed, cudaStream_t st)
         float a = std::sqrt(6.0f / (float)layer_in(l));
         for (int i = 0; i < layer_out(l) * layer_in(l); ++i) w[layer_offset(l) + i] = (2.0f * uniform(s) - 1.0f) * a;
     }
-    std::vector<float> gp(kGridParams);
-    for (uint64_t i = 0; i < kGridParams; ++i) gp[i] = (2.0f * uniform(s) - 1.0f) * 1e-4f;
     cudaError_t e = cudaMemcpyAsync(wP_, w.data(), w.size() * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(gridP_, gp.data(), gp.size() * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_init_grid<<<(unsigned)((kGridParams + 255) / 256), 256, 0, st>>>(gridP_, kGridParams, 0x6d1d0000ull + seed);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(wM_, 0, kWeightCount * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(wV_, 0, kWeightCount * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(wG_, 0, kWeightCount * 4, st);

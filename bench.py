@@ -13,6 +13,14 @@ shadow rays with tmax uniform in (0, 1]. A step traces all 8,388,608 queries.
 the C ABI with pinned host buffers (host->device copy of the rays and
 device->host copy of the results inside the timed region).
 
+`guiding` (rank 0, one GPU): time to relMSE 0.01, guided vs plain MIS, on the
+glossy interior (20 x 4 x 12 m room, 2.0M triangles, 70% GGX with roughness
+in [0.02, 0.4], sky of radiance 5 through two 1 x 2 m window openings, depth
+12) at 320 x 180 against a 65,536-spp plain image rendered in the same run.
+relMSE = mean over pixels and channels of (x - r)^2 / (r^2 + 0.01 mean(r)^2).
+Time is the wall time of the render calls (synchronous), guided training
+included; both curves are sampled at doubling spp and interpolated in log-log.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one process per GPU under torchrun; each rank is an independent
 replica of the workload (weak scaling), timed as the max over ranks.
@@ -49,6 +57,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-guiding", action="store_true", help="skip the guided vs plain time-to-relMSE measurement")
+    p.add_argument("--guiding-ref-spp", type=int, default=65536)
     p.add_argument("--profile", action="store_true",
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     return p.parse_args()
@@ -160,6 +170,122 @@ def cpu_baseline(verts, idx, closest, shadow, budget_s):
             "sample": f"{done // 2} random rays of the workload (primary+incoherent mix), closest + any hit each; "
                       f"reference WideBvh build {acc.build_ms:.0f} ms (not in the rate)",
             "seconds": t_total}
+
+
+GUIDING_RES = (320, 180)
+GUIDING_DEPTH = 12
+GUIDE_OPTIONS = dict(guide=True, guide_fraction=0.5, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
+                     guide_lr=1e-2, guide_min_roughness=0.2, guide_train_steps=128)
+
+
+def relmse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2 * ref.mean() ** 2)))
+
+
+def guiding_benchmark(device, ref_spp, target=0.01):
+    """Time to relMSE `target` of plain and guided rendering on the glossy
+    interior (see the module docstring), and the reference CPU renderer's
+    projected time for the plain estimator (its measured samples/s on the
+    same scene x the spp the plain estimator needs)."""
+    import math
+
+    from alpine_b200 import gpu, scenes
+
+    W, H = GUIDING_RES
+    scene = scenes.glossy_interior_scene()
+
+    def context(**opts):
+        c = gpu.Context(device, W, H, GUIDING_DEPTH)
+        scenes.load_scene(c, scene, W, H)
+        c.set_render_options(sampler=gpu.RNG_COUNTER, accumulate_fp64=True, **opts)
+        c.reset_accumulation()
+        return c
+
+    def mean(c):
+        a, n = c.read_accumulation(W, H, fp64=True)
+        return a[..., :3].astype(np.float64) / n
+
+    t0 = time.perf_counter()
+    halves = []
+    for seed in (1000, 2000):
+        c = context(seed=seed)
+        c.render(ref_spp // 2)
+        halves.append(mean(c))
+        c.close()
+    ref = 0.5 * (halves[0] + halves[1])
+    ref_s = time.perf_counter() - t0
+    ref_err = relmse(halves[0], halves[1]) / 4  # relMSE of the average against the truth, estimated
+
+    def curve(opts, max_spp=1 << 16):
+        c = context(**opts)
+        done, elapsed, pts = 0, 0.0, []
+        spp = 4
+        while done < max_spp:
+            t1 = time.perf_counter()
+            c.render(spp)
+            elapsed += time.perf_counter() - t1
+            done += spp
+            pts.append((done, elapsed, relmse(mean(c), ref)))
+            if pts[-1][2] < 0.7 * target:
+                break
+            spp = done
+        steps = c.guide_steps()[0] if opts.get("guide") else 0
+        c.close()
+        at = None
+        for i in range(1, len(pts)):
+            (s0, t_0, e0), (s1, t_1, e1) = pts[i - 1], pts[i]
+            if e1 <= target < e0:
+                f = (math.log(target) - math.log(e0)) / (math.log(e1) - math.log(e0))
+                at = (t_0 + f * (t_1 - t_0), math.exp(math.log(s0) + f * (math.log(s1) - math.log(s0))))
+                break
+        return at, pts, steps
+
+    warm = context(seed=5, **GUIDE_OPTIONS)  # module loading, allocations
+    warm.render(4)
+    warm.close()
+    plain_at, plain_pts, _ = curve(dict(seed=1))
+    guided_at, guided_pts, steps = curve(dict(seed=2, **GUIDE_OPTIONS))
+    out = {
+        "metric": "time to relMSE 0.01, guided vs plain MIS", "unit": "s", "target_relmse": target,
+        "scene": "glossy interior, 2.0M triangles, sky 5 through two 1x2 m windows, depth 12, no lights",
+        "resolution": [W, H], "reference_spp": ref_spp, "reference_s": ref_s,
+        "reference_relmse_estimate": ref_err,
+        "relmse": "mean((x - r)^2 / (r^2 + 0.01 mean(r)^2))",
+        "plain_s": plain_at[0] if plain_at else None, "plain_spp": plain_at[1] if plain_at else None,
+        "guided_s": guided_at[0] if guided_at else None, "guided_spp": guided_at[1] if guided_at else None,
+        "speedup": (plain_at[0] / guided_at[0]) if plain_at and guided_at else None,
+        "guide": {k: v for k, v in GUIDE_OPTIONS.items() if k != "guide"} | {"adam_steps": steps},
+        "plain_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in plain_pts],
+        "guided_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in guided_pts],
+    }
+    out["cpu_reference"] = cpu_render_baseline(scene, W, H, out["plain_spp"])
+    return out
+
+
+def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
+    """The reference renderer (oracle/_ref: class Alpine with its WideBvh) on
+    all host cores: samples/s on the same scene and image, and the time the
+    plain estimator (the same algorithm) would need for plain_spp."""
+    import oracle
+
+    from alpine_b200 import scenes
+
+    if not oracle.ref_available():
+        return None
+    r = oracle.RefRenderer(W, H, GUIDING_DEPTH, accelerator=oracle.RefRenderer.ACC_WIDE_BVH)
+    t0 = time.perf_counter()
+    scenes.load_scene(r, scene, W, H)
+    load_s = time.perf_counter() - t0
+    r.reset_accumulation()
+    r.render(1)
+    t0 = time.perf_counter()
+    r.render(spp)
+    dt = time.perf_counter() - t0
+    r.close()
+    rate = spp * W * H / dt
+    return {"samples_per_s": rate, "cores": os.cpu_count() or 1, "kind": "reference",
+            "sample": f"{spp} spp at {W}x{H} after 1 warm-up spp; scene load + BVH build {load_s:.1f} s",
+            "projected_time_to_target_s": (plain_spp * W * H / rate) if plain_spp else None}
 
 
 def run_reference(args):
@@ -328,6 +454,11 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
+    guiding = None
+    if rank == 0 and world == 1 and not args.no_guiding:
+        ctx.close()
+        ctx = None
+        guiding = guiding_benchmark(local, args.guiding_ref_spp)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -347,9 +478,11 @@ def run_ours(args):
             "cpu_baseline": base,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),
+            "guiding": guiding,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     if dist is not None:
         dist.destroy_process_group()
 
