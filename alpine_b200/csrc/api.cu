@@ -44,7 +44,7 @@ int check_status(alpine_gpu_ctx* c)
     return ALPINE_GPU_OK;
 }
 
-int upload_geometry(alpine_gpu_ctx* c)
+int upload_geometry_now(alpine_gpu_ctx* c)
 {
     if (!c->geometryDirty) return ALPINE_GPU_OK;
     size_t vb = c->verts.size() * sizeof(float), ib = c->idx.size() * sizeof(uint32_t);
@@ -201,6 +201,9 @@ int alpine_gpu_reset_scene(alpine_gpu_ctx* c)
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     c->verts.clear();
     c->idx.clear();
+    c->morphs.clear();
+    c->channels.clear();
+    c->hostVertsStale = c->hostNormalsStale = false;
     c->shapeVertBase.clear();
     c->shapeVertCount.clear();
     c->shapeTriBase.clear();
@@ -232,6 +235,7 @@ int alpine_gpu_add_mesh(alpine_gpu_ctx* c, const float* vertices, uint32_t vcoun
         return c->fail(ALPINE_GPU_ERR_LIMIT, "add_mesh: more than 2^31 - 1 triangles or vertices");
     for (uint64_t i = 0; i < 3ull * tcount; ++i)
         if (indices[i] >= vcount) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_mesh: vertex index out of range");
+    if (int rc = c->pull_host_geometry()) return rc;
     uint32_t vbase = (uint32_t)(c->verts.size() / 3);
     c->shapeVertBase.push_back(vbase);
     c->shapeVertCount.push_back(vcount);
@@ -251,6 +255,7 @@ int alpine_gpu_update_vertices(alpine_gpu_ctx* c, uint32_t shape, const float* v
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (shape >= c->shapeVertBase.size() || !vertices)
         return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "update_vertices: bad shape id or null array");
+    if (int rc = c->pull_host_geometry()) return rc;
     std::memcpy(c->verts.data() + 3ull * c->shapeVertBase[shape], vertices,
                 3ull * c->shapeVertCount[shape] * sizeof(float));
     c->geometryDirty = true;
@@ -262,7 +267,7 @@ int alpine_gpu_build(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
-    if (int rc = upload_geometry(c)) return rc;
+    if (int rc = upload_geometry_now(c)) return rc;
     uint32_t n = (uint32_t)(c->idx.size() / 3);
     if (!c->dNodes.reserve((size_t(n) + 1) * sizeof(ag::WideNode)) || !c->dTris.reserve(size_t(n) * sizeof(ag::TriRecord)))
         return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "build: cudaMalloc failed");
@@ -344,3 +349,7 @@ int alpine_gpu_synchronize(alpine_gpu_ctx* c)
 }
 
 }  // extern "C"
+
+namespace ag {
+int upload_geometry(alpine_gpu_ctx* c) { return upload_geometry_now(c); }
+}  // namespace ag

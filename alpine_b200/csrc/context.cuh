@@ -6,6 +6,7 @@
 #include "guide_host.cuh"
 #include "shading.cuh"
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -41,6 +42,9 @@ struct DeviceBuffer {
 };
 
 constexpr int kCopyStreams = 4;
+
+int upload_render_scene(alpine_gpu_ctx* c);  // render.cu: materials, attributes, lights to the device
+int upload_geometry(alpine_gpu_ctx* c);      // api.cu: vertices and indices to the device
 
 // A material record of the C ABI as the device Material: Dielectric or
 // Conductor with alpha = roughness (gltf_loader.cpp:404-414), alpha clamped
@@ -93,7 +97,7 @@ struct alpine_gpu_ctx {
     ag::DeviceBuffer dRays, dOut;
 
     // rendering: per-triangle material/normal flags and per-vertex normals
-    std::vector<uint32_t> triInfo;  // material id | 0x80000000 when the mesh has vertex normals
+    std::vector<uint32_t> triInfo;  // material id | kTriHasNormals | kTriMorphedNormals
     std::vector<float> normals;     // 3 per vertex (zero for meshes without normals)
     bool attribsDirty = true;
     ag::DeviceBuffer dTriInfo, dNormals;
@@ -120,6 +124,25 @@ struct alpine_gpu_ctx {
     ag::DeviceBuffer dWave;
     uint32_t waveCapacity = 0;
 
+    // morph-target animation (Mesh::Data::targets, src/shapes/mesh.h:27-33;
+    // Animation channels, src/animation.h). The morphed positions and normals
+    // are written on the device; the host mirrors are refreshed on demand.
+    struct Morph {
+        uint32_t shape = 0, targets = 0;
+        bool normals = false;
+        ag::DeviceBuffer dBase, dDeltas;      // positions [V][3], deltas [T][V][3]
+        ag::DeviceBuffer dBaseN, dDeltasN;    // the same for the vertex normals
+        std::vector<float> weights;           // Mesh::mWeights
+    };
+    struct Channel {
+        uint32_t morph = 0;
+        std::vector<float> times;             // keyframe times
+        std::vector<float> weights;           // [keyframes][targets]
+    };
+    std::vector<std::unique_ptr<Morph>> morphs;
+    std::vector<Channel> channels;
+    bool hostVertsStale = false, hostNormalsStale = false;
+
     // learned path guiding
     ag::guide::Guide guide;
     uint32_t guideSeed = 1;
@@ -141,6 +164,23 @@ struct alpine_gpu_ctx {
             cudaStreamSynchronize(stream);
             return fail(ALPINE_GPU_ERR_LIMIT, "device-side limit reached, status bits " + std::to_string(bits));
         }
+        return ALPINE_GPU_OK;
+    }
+
+    // Copies device-side morph results into the host mirrors (before a host
+    // edit of the geometry or attributes would otherwise upload stale data).
+    int pull_host_geometry()
+    {
+        if (!hostVertsStale && !hostNormalsStale) return ALPINE_GPU_OK;
+        cudaError_t e = cudaSuccess;
+        if (hostVertsStale && !verts.empty())
+            e = cudaMemcpyAsync(verts.data(), dVerts.ptr, verts.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess && hostNormalsStale && !normals.empty())
+            e = cudaMemcpyAsync(normals.data(), dNormals.ptr, normals.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return fail(ALPINE_GPU_ERR_CUDA, std::string("geometry read-back: ") + cudaGetErrorString(e));
+        hostVertsStale = hostNormalsStale = false;
         return ALPINE_GPU_OK;
     }
 

@@ -31,7 +31,7 @@ struct SceneView {
     const float* verts;
     const uint32_t* idx;
     const float* normals;      // per vertex, may be null
-    const uint32_t* triInfo;   // per triangle: material id (bits 0-30), bit 31 = has vertex normals
+    const uint32_t* triInfo;   // per triangle: material id | kTriHasNormals | kTriMorphedNormals
     const Material* materials;
     uint32_t materialCount;
     LightSamplerView lights;
@@ -198,15 +198,17 @@ AG_D void surface_at(const SceneView& sc, const uint4 h, Surface& s)
     const float3 v2 = mk3(sc.verts[3ull * i2], sc.verts[3ull * i2 + 1], sc.verts[3ull * i2 + 2]);
     s.ng = normalize3(cross(v1 - v0, v2 - v0));
     const uint32_t info = sc.triInfo[prim];
-    uint32_t mid = info & 0x7fffffffu;
+    uint32_t mid = info & kTriMaterialMask;
     if (mid >= sc.materialCount) mid = 0;
     s.mat = sc.materials[mid];
-    if (info & 0x80000000u) {
+    if (info & kTriHasNormals) {
         const float b0 = 1.0f - b1 - b2;
         const float3 n0 = mk3(sc.normals[3ull * i0], sc.normals[3ull * i0 + 1], sc.normals[3ull * i0 + 2]);
         const float3 n1 = mk3(sc.normals[3ull * i1], sc.normals[3ull * i1 + 1], sc.normals[3ull * i1 + 2]);
         const float3 n2 = mk3(sc.normals[3ull * i2], sc.normals[3ull * i2 + 1], sc.normals[3ull * i2 + 2]);
         s.ns = n0 * b0 + n1 * b1 + n2 * b2;
+        // a morphed normal is re-normalised (mesh.cpp:86-101)
+        if (info & kTriMorphedNormals) s.ns = normalize3(s.ns);
     } else {
         s.ns = s.ng;
     }

@@ -249,7 +249,7 @@ bool upload(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st)
     return cudaMemcpyAsync(buf.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st) == cudaSuccess;
 }
 
-int upload_render_scene(alpine_gpu_ctx* c)
+int upload_scene_data(alpine_gpu_ctx* c)
 {
     cudaStream_t st = c->stream;
     if (c->materialsDirty) {
@@ -462,13 +462,15 @@ int alpine_gpu_set_triangle_attributes(alpine_gpu_ctx* c, uint32_t shape, const 
     if (shape >= c->shapeVertBase.size()) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "bad shape id");
     const uint32_t vb = c->shapeVertBase[shape], vc = c->shapeVertCount[shape];
     const uint32_t tb = c->shapeTriBase[shape], tc = c->shapeTriCount[shape];
+    if (int rc = c->pull_host_geometry()) return rc;
     if (c->triInfo.size() < c->idx.size() / 3) c->triInfo.resize(c->idx.size() / 3, 0u);
     if (c->normals.size() < c->verts.size()) c->normals.resize(c->verts.size(), 0.0f);
     if (normals) std::memcpy(c->normals.data() + 3ull * vb, normals, 3ull * vc * sizeof(float));
     for (uint32_t t = 0; t < tc; ++t) {
         uint32_t mid = tri_material ? tri_material[t] : 0u;
-        if (mid & 0x80000000u) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "material id too large");
-        c->triInfo[tb + t] = mid | (normals ? 0x80000000u : 0u);
+        if (mid & ~ag::kTriMaterialMask) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "material id too large");
+        const uint32_t morphN = c->triInfo[tb + t] & ag::kTriMorphedNormals;  // kept: set by the morph targets
+        c->triInfo[tb + t] = mid | (normals ? ag::kTriHasNormals : 0u) | morphN;
     }
     c->attribsDirty = true;
     return ALPINE_GPU_OK;
@@ -632,10 +634,11 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
     if (!c->accumValid)
         if (int rc = alpine_gpu_reset_accumulation(c)) return rc;
     if (c->triInfo.size() < c->idx.size() / 3) {
+        if (int rc = c->pull_host_geometry()) return rc;
         c->triInfo.resize(c->idx.size() / 3, 0u);
         c->attribsDirty = true;
     }
-    if (int rc = upload_render_scene(c)) return rc;
+    if (int rc = upload_scene_data(c)) return rc;
     if (spp == 0) return ALPINE_GPU_OK;
 
     const bool stream = c->options.sampler == ALPINE_GPU_SAMPLER_REFERENCE_STREAM;
@@ -846,3 +849,7 @@ int alpine_gpu_post_process(alpine_gpu_ctx* c, int tonemap, float* mean_rgb, uin
 }
 
 }  // extern "C"
+
+namespace ag {
+int upload_render_scene(alpine_gpu_ctx* c) { return upload_scene_data(c); }
+}  // namespace ag

@@ -149,6 +149,11 @@ AG_HD float counter_1d(CounterRng& r)
 // Materials.
 enum MaterialKind : uint32_t { kMatDielectric = 0, kMatConductor = 1 };
 
+// Per-triangle render attributes: material id and flags.
+constexpr uint32_t kTriHasNormals = 0x80000000u;      // interpolate the vertex normals
+constexpr uint32_t kTriMorphedNormals = 0x40000000u;  // the mesh has normal morph targets
+constexpr uint32_t kTriMaterialMask = 0x3fffffffu;
+
 struct Material {
     uint32_t kind;
     float r, g, b;    // base colour (Dielectric: diffuse albedo; Conductor: F0)

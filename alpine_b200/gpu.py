@@ -86,6 +86,10 @@ def lib():
         L.alpine_gpu_add_mesh.argtypes = [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32)]
         L.alpine_gpu_update_vertices.argtypes = [vp, C.c_uint32, vp]
         L.alpine_gpu_build.argtypes = [vp, C.POINTER(BvhStats)]
+        L.alpine_gpu_set_morph_targets.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint32]
+        L.alpine_gpu_add_animation_channel.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint32]
+        L.alpine_gpu_update_scene.argtypes = [vp, C.c_float, C.POINTER(BvhStats)]
+        L.alpine_gpu_get_vertices.argtypes = [vp, C.c_uint32, vp, vp]
         L.alpine_gpu_trace.argtypes = [vp, vp, C.c_uint64, vp]
         L.alpine_gpu_occluded.argtypes = [vp, vp, C.c_uint64, vp]
         L.alpine_gpu_trace_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
@@ -173,6 +177,33 @@ class Context:
     def update_vertices(self, shape, verts):
         v = np.ascontiguousarray(verts, np.float32)
         self._check(self.L.alpine_gpu_update_vertices(self.h, shape, _ptr(v)))
+
+    def set_morph_targets(self, shape, vertex_deltas, normal_deltas=None):
+        """vertex_deltas (and normal_deltas): float[T, V, 3] morph targets."""
+        vd = np.ascontiguousarray(vertex_deltas, np.float32)
+        nd = None if normal_deltas is None else np.ascontiguousarray(normal_deltas, np.float32)
+        t = vd.shape[0] if vd.ndim == 3 else 1
+        self._check(self.L.alpine_gpu_set_morph_targets(self.h, shape, _ptr(vd), None if nd is None else _ptr(nd), t))
+
+    def add_animation_channel(self, shape, times, weights):
+        """times: float[K]; weights: float[K, T]."""
+        tt = np.ascontiguousarray(times, np.float32)
+        ww = np.ascontiguousarray(weights, np.float32)
+        self._check(self.L.alpine_gpu_add_animation_channel(self.h, shape, _ptr(tt), _ptr(ww), tt.size))
+
+    def update_scene(self, time) -> dict:
+        """Alpine::updateScene: morph on the GPU, then rebuild the BVH."""
+        s = BvhStats()
+        self._check(self.L.alpine_gpu_update_scene(self.h, float(time), C.byref(s)))
+        self.stats = s.as_dict()
+        return self.stats
+
+    def get_vertices(self, shape, count):
+        """(positions float[count, 3], vertex normals float[count, 3]) of one mesh."""
+        v = np.empty((count, 3), np.float32)
+        n = np.empty((count, 3), np.float32)
+        self._check(self.L.alpine_gpu_get_vertices(self.h, shape, _ptr(v), _ptr(n)))
+        return v, n
 
     def build(self) -> dict:
         s = BvhStats()

@@ -314,6 +314,28 @@ def glossy_interior_scene(seed=1, target_tris=2_000_000, n_boxes=80, n_spheres=2
             "background": (sky, sky, sky)}
 
 
+def sinusoid_morph(verts, normals, amplitude=0.02, phase=0.0, frames=60, period=60.0, with_normals=False):
+    """One morph target moving every vertex by `amplitude` along its normal
+    (the radial direction when there are no normals), driven by the weight
+    sin(2 pi t / period + phase) sampled at `frames` keyframes t = 0, 1, ...
+    (glTF-style keyframed morph weights)."""
+    v = np.asarray(verts, np.float32)
+    if normals is not None:
+        d = np.asarray(normals, np.float32)
+    else:
+        c = v.mean(0)
+        d = v - c
+        d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-12)
+    deltas = (amplitude * d)[None].astype(np.float32)
+    times = np.arange(frames, dtype=np.float32)
+    weights = np.sin(2 * np.pi * times / period + phase).astype(np.float32)[:, None]
+    out = {"deltas": deltas, "times": times, "weights": weights}
+    if with_normals and normals is not None:
+        # a small tilt of the normals, so that normal morphing is exercised
+        out["normal_deltas"] = (0.3 * np.roll(np.asarray(normals, np.float32), 1, axis=1))[None]
+    return out
+
+
 def add_random_lights(scene, n, seed=5, kinds=("disk", "point")):
     """Adds n seeded disk / point lights spread over the room's ceiling half
     (many-light sampler tests)."""
@@ -338,10 +360,19 @@ def load_scene(target, scene, width, height):
     if is_gpu:
         target.reset_scene()
         target.set_materials(scene["materials"])
+    animated = False
     for m in scene["meshes"]:
+        mo = m.get("morph")
+        animated |= mo is not None
         if is_gpu:
             sid = target.add_mesh(m["verts"], m["idx"])
             target.set_triangle_attributes(sid, m["normals"], m["tri_material"])
+            if mo is not None:
+                target.set_morph_targets(sid, mo["deltas"], mo.get("normal_deltas"))
+                target.add_animation_channel(sid, mo["times"], mo["weights"])
+        elif mo is not None:
+            target.add_morph_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"],
+                                  mo["deltas"], mo.get("normal_deltas"), mo["times"], mo["weights"])
         else:
             target.add_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"])
     for l in scene["lights"]:
@@ -354,4 +385,7 @@ def load_scene(target, scene, width, height):
     eye, tgt, up, fovy = scene["camera"]
     target.set_camera(eye, tgt, up, fovy, width / height)
     target.set_background(*scene["background"])
-    target.build()
+    if animated:
+        target.update_scene(scene.get("time", 0.0))  # Alpine::updateScene: animation, then the rebuild
+    else:
+        target.build()

@@ -103,6 +103,30 @@ ALPINE_GPU_API int alpine_gpu_add_mesh(alpine_gpu_ctx* ctx, const float* vertice
  * updateShape, accelerator.h:27-29). Takes effect at the next build. */
 ALPINE_GPU_API int alpine_gpu_update_vertices(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* vertices);
 
+/* Morph-target animation (glTF morph targets: Mesh::Data::targets,
+ * src/shapes/mesh.h:27-33; Animation, src/animation.h).
+ * alpine_gpu_set_morph_targets: `count` (1-32) targets of one mesh, vertex
+ *   deltas float[count][3 * vertex_count] and optionally normal deltas of the
+ *   same shape (the mesh must then have vertex normals, set by
+ *   alpine_gpu_set_triangle_attributes). The mesh's current positions and
+ *   normals become the base; the weights start at 0 (mesh.cpp:14-20).
+ * alpine_gpu_add_animation_channel: one channel (Animation::Channel) of
+ *   `keyframes` (>= 2) morph keyframes for that mesh: times[k] (not
+ *   decreasing) and weights[k][count].
+ * alpine_gpu_update_scene: Alpine::updateScene(time) (alpine.cpp:204-212):
+ *   per channel, time clamped to the keyframe range, the segment found and
+ *   the weights lerped (Animation::update, animation.cpp:10-39); the vertices
+ *   (and normals) morphed on the GPU as Mesh::update does (mesh.cpp:29-55,
+ *   the normals as mesh.cpp:86-101), then the BVH rebuilt (stats may be NULL).
+ * alpine_gpu_get_vertices: the current positions (and vertex normals, zero
+ *   for a mesh without) of one mesh; either pointer may be NULL. */
+ALPINE_GPU_API int alpine_gpu_set_morph_targets(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* vertex_deltas,
+                                                const float* normal_deltas, uint32_t count);
+ALPINE_GPU_API int alpine_gpu_add_animation_channel(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* times,
+                                                    const float* weights, uint32_t keyframes);
+ALPINE_GPU_API int alpine_gpu_update_scene(alpine_gpu_ctx* ctx, float time, alpine_gpu_bvh_stats* stats);
+ALPINE_GPU_API int alpine_gpu_get_vertices(alpine_gpu_ctx* ctx, uint32_t shape_id, float* vertices, float* normals);
+
 /* Full (re)build of the BVH on the GPU: binned SAH with 32 bins, collapsed to
  * an 8-wide quantised BVH (Accelerator::updateScene, accelerator.h:31;
  * src/accelerators/wide_bvh.cpp:175-197). stats may be NULL. */

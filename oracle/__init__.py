@@ -92,6 +92,11 @@ def ref():
         L.ref_render_add_mesh.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, C.c_void_p, _u32p, _f32p,
                                           C.c_uint32]
         L.ref_render_add_mesh.restype = C.c_int
+        L.ref_render_add_morph_mesh.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, C.c_void_p, _u32p, _f32p,
+                                                C.c_uint32, _f32p, C.c_void_p, C.c_uint32, _f32p, _f32p, C.c_uint32]
+        L.ref_render_add_morph_mesh.restype = C.c_int
+        L.ref_morph_vertices.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, _f32p, C.c_uint32, _f32p, _f32p,
+                                         C.c_uint32, C.c_float, _f32p]
         L.ref_render_load_obj.argtypes = [C.c_char_p]
         L.ref_render_load_obj.restype = C.c_int
         L.ref_render_add_disk_light.argtypes = [C.c_float, _f32p, _f32p, _f32p, C.c_float]
@@ -229,6 +234,32 @@ class RefRenderer:
         if not self.L.ref_render_add_mesh(v, v.size // 3, i, nt, nptr, tm, mats, len(materials)):
             raise RuntimeError("ref_render_add_mesh failed")
 
+    def add_morph_mesh(self, verts, idx, normals, tri_material, materials, deltas, normal_deltas, times, weights):
+        """A mesh with morph targets deltas float[T, V, 3] (and normal deltas)
+        and one animation channel (times float[K], weights float[K, T]);
+        update_scene(time) applies it (Alpine::updateScene)."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        i = np.ascontiguousarray(idx, np.uint32).reshape(-1)
+        nt = i.size // 3
+        tm = np.zeros(nt, np.uint32) if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
+        mats = np.array([[k, *c, r] for k, c, r in materials], np.float32).reshape(-1)
+        keep = []
+        nptr = None
+        if normals is not None:
+            keep.append(np.ascontiguousarray(normals, np.float32).reshape(-1))
+            nptr = keep[-1].ctypes.data
+        d = np.ascontiguousarray(deltas, np.float32)
+        ndptr = None
+        if normal_deltas is not None:
+            keep.append(np.ascontiguousarray(normal_deltas, np.float32).reshape(-1))
+            ndptr = keep[-1].ctypes.data
+        t = np.ascontiguousarray(times, np.float32)
+        w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        if not self.L.ref_render_add_morph_mesh(v, v.size // 3, i, nt, nptr, tm, mats, len(materials), d.reshape(-1),
+                                                ndptr, d.shape[0], t, w, t.size):
+            raise RuntimeError("ref_render_add_morph_mesh failed")
+        self._keep = getattr(self, "_keep", []) + keep
+
     def add_disk_light(self, power, color, position, target, radius):
         self.L.ref_render_add_disk_light(power, np.asarray(color, np.float32), np.asarray(position, np.float32),
                                          np.asarray(target, np.float32), radius)
@@ -243,6 +274,10 @@ class RefRenderer:
 
     def build(self):
         self.L.ref_render_update_scene(0.0)
+
+    def update_scene(self, time):
+        """Alpine::updateScene(time): animations, then the accelerator rebuild."""
+        self.L.ref_render_update_scene(float(time))
 
     def build_light_sampler(self, kind):
         self.L.ref_render_build_light_sampler(kind)
@@ -309,6 +344,22 @@ def ref_material_eval(material, wo, wi):
     pdf = np.empty(n, np.float32)
     ref().ref_material_eval(_material_record(material), wo.reshape(-1), wi.reshape(-1), n, bsdf.reshape(-1), pdf)
     return bsdf, pdf
+
+
+def ref_morph_vertices(verts, idx, deltas, times, weights, time):
+    """The reference's Animation::update + Mesh::update (src/animation.cpp:
+    10-39, src/shapes/mesh.cpp:29-55) of one mesh on its Bvh accelerator:
+    the morphed positions at `time`. deltas float[T, V, 3]; times float[K];
+    weights float[K, T]."""
+    v = np.ascontiguousarray(verts, np.float32)
+    i = np.ascontiguousarray(idx, np.uint32)
+    d = np.ascontiguousarray(deltas, np.float32)
+    t = np.ascontiguousarray(times, np.float32)
+    w = np.ascontiguousarray(weights, np.float32)
+    out = np.empty_like(v)
+    ref().ref_morph_vertices(v.reshape(-1), v.shape[0], i.reshape(-1), i.shape[0], d.reshape(-1), d.shape[0], t,
+                             w.reshape(-1), t.size, float(time), out.reshape(-1))
+    return out
 
 
 class RefAccel:

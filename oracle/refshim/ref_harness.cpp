@@ -406,6 +406,111 @@ ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, u
     return 1;
 }
 
+// Morph targets (Mesh::Data::targets) and one animation channel for a mesh
+// record: T targets of vertex deltas [T][V][3] and optional normal deltas,
+// K keyframes: times[K], weights[K][T].
+static void
+add_targets(Mesh::Data& d, uint32_t nverts, const float* vdeltas, const float* ndeltas, uint32_t T)
+{
+    d.targets.resize(T);
+    for (uint32_t j = 0; j < T; ++j)
+    {
+        auto& tg = d.targets[j];
+        tg.vertices.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i)
+        {
+            const float* v = vdeltas + (3ull * nverts * j) + 3ull * i;
+            tg.vertices[i] = float3(v[0], v[1], v[2]);
+        }
+        if (ndeltas)
+        {
+            tg.normals.resize(nverts);
+            for (uint32_t i = 0; i < nverts; ++i)
+            {
+                const float* v = ndeltas + (3ull * nverts * j) + 3ull * i;
+                tg.normals[i] = float3(v[0], v[1], v[2]);
+            }
+        }
+    }
+}
+
+static std::shared_ptr<Animation>
+make_channel(const std::shared_ptr<Shape>& shape, const float* times, const float* weights, uint32_t K, uint32_t T)
+{
+    Animation::Channel ch;
+    ch.shape = shape;
+    for (uint32_t k = 0; k < K; ++k)
+    {
+        Animation::Channel::MorphKeyframe kf;
+        kf.time = times[k];
+        kf.weights.assign(weights + (size_t)k * T, weights + (size_t)(k + 1) * T);
+        ch.morphKeyframes.push_back(std::move(kf));
+    }
+    std::vector<Animation::Channel> chans;
+    chans.push_back(std::move(ch));
+    return std::make_shared<Animation>(std::move(chans));
+}
+
+// Animation::update + Mesh::update on the reference's own Bvh accelerator:
+// writes the morphed positions of a V-vertex mesh at `time`.
+void
+ref_morph_vertices(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris, const float* vdeltas,
+    uint32_t T, const float* times, const float* weights, uint32_t K, float time, float* out)
+{
+    std::vector<std::byte> arena(std::max<size_t>(1 << 20, (size_t)ntris * 512 + (size_t)nverts * 64));
+    Bvh acc{std::span<std::byte>(arena)};
+    Mesh::Data d;
+    d.vertices.resize(nverts);
+    for (uint32_t i = 0; i < nverts; ++i) { d.vertices[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    d.prims.resize(ntris);
+    for (uint32_t i = 0; i < ntris; ++i) { d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]); }
+    add_targets(d, nverts, vdeltas, nullptr, T);
+    auto mesh = std::make_shared<Mesh>(std::move(d), T);
+    mesh->appendTo(&acc);
+    auto anim = make_channel(mesh, times, weights, K, T);
+    anim->update(&acc, time);
+    const float3* vb = static_cast<const float3*>(acc.getVertexBuffer(0));
+    for (uint32_t i = 0; i < nverts; ++i)
+    {
+        for (int k = 0; k < 3; ++k) { out[3 * i + k] = vb[i][k]; }
+    }
+}
+
+// ref_render_add_mesh with T morph targets and one animation channel, which
+// Alpine::updateScene (ref_render_update_scene) then applies.
+int
+ref_render_add_morph_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
+    const float* normals, const uint32_t* triMaterial, const float* materials, uint32_t nmat, const float* vdeltas,
+    const float* ndeltas, uint32_t T, const float* times, const float* weights, uint32_t K)
+{
+    Mesh::Data d;
+    d.vertices.resize(nverts);
+    for (uint32_t i = 0; i < nverts; ++i) { d.vertices[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    if (normals)
+    {
+        d.normals.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i) { d.normals[i] = float3(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]); }
+    }
+    std::vector<std::shared_ptr<Material>> mats(nmat);
+    for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 5 * m); }
+    d.prims.resize(ntris);
+    d.materials.resize(ntris);
+    for (uint32_t i = 0; i < ntris; ++i)
+    {
+        d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]);
+        uint32_t m = triMaterial[i];
+        if (m >= nmat) { return 0; }
+        d.materials[i] = mats[m];
+    }
+    add_targets(d, nverts, vdeltas, normals ? ndeltas : nullptr, T);
+    auto mesh = std::make_shared<Mesh>(std::move(d), T);
+    auto& a = alpine::alpine();
+    a.mScene.shapes.push_back(mesh);
+    mesh->appendTo(a.mAccelerator.get());
+    a.mScene.animations.push_back(make_channel(mesh, times, weights, K, T));
+    return 1;
+}
+
 int ref_render_load_obj(const char* path) { return loadScene(path, FileType::Obj) ? 1 : 0; }
 
 void
