@@ -169,9 +169,11 @@ int alpine_gpu_create(const alpine_gpu_config* cfg, alpine_gpu_ctx** out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     for (int i = 0; i < ag::kCopyStreams && e == cudaSuccess; ++i)
         e = cudaStreamCreateWithFlags(&c->copyStreams[i], cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&c->dStatus, sizeof(uint32_t));
+    // 16 device words: [0] status bits, [4] the sample base of a replayed render
+    if (e == cudaSuccess) e = cudaMalloc(&c->dStatus, 16 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost(&c->hStatus, 16 * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(c->dStatus, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(c->dStatus, 0, 16 * sizeof(uint32_t));
+    if (e == cudaSuccess) c->dSampleBase = c->dStatus + 4;
     if (e != cudaSuccess) {
         cudaGetLastError();
         alpine_gpu_destroy(c);
@@ -188,6 +190,7 @@ void alpine_gpu_destroy(alpine_gpu_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& s : c->copyStreams)
         if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->dStatus) cudaFree(c->dStatus);
     if (c->hStatus) cudaFreeHost(c->hStatus);

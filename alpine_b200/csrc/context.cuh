@@ -123,6 +123,13 @@ struct alpine_gpu_ctx {
     uint32_t totalSamples = 0;
     ag::DeviceBuffer dWave;
     uint32_t waveCapacity = 0;
+    int traceBlock = 128;             // k_trace_dyn block size (autotuned)
+    // CUDA-graph replay of the render loop: the captured graph and the launch
+    // configuration it was captured for
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<unsigned char> graphKey;
+    uint32_t graphLaunches = 0, graphCaptures = 0;
+    uint32_t* dSampleBase = nullptr;  // first sample index of a replayed render
 
     // morph-target animation (Mesh::Data::targets, src/shapes/mesh.h:27-33;
     // Animation channels, src/animation.h). The morphed positions and normals

@@ -43,7 +43,8 @@ struct SceneView {
 struct WaveView {
     uint32_t numPaths;     // S * numPixels
     uint32_t numPixels;
-    uint32_t sampleBase;   // sample index of slice 0 (counter RNG)
+    uint32_t sampleBase;   // sample index of slice 0 (counter RNG), plus *sampleBaseDev when set
+    const uint32_t* sampleBaseDev;
     uint32_t samplesInWave;
     uint32_t seed;
     uint32_t rrStart;      // Russian roulette from this depth; 0 = off (reference behaviour)
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(SceneView sc, WaveView w,
     PathRng r;
     r.stream = streamRng;
     if (streamRng) r.load(w.pixelRng[pixel]);
-    else counter_init(r.cr, w.seed, pixel, w.sampleBase + slice);
+    else counter_init(r.cr, w.seed, pixel, w.sampleBase + (w.sampleBaseDev ? *w.sampleBaseDev : 0u) + slice);
     uint32_t x = pixel % sc.width, y = pixel / sc.width;
     // Sampler::get2D draws x then y (src/sampler.cpp:24-27)
     float jx = r.next();

@@ -411,6 +411,8 @@ __global__ void k_post(const float* a32, const double* a64, uint32_t pixels, uin
     }
 }
 
+__global__ void k_set_word(uint32_t* p, uint32_t v) { *p = v; }
+
 // Turns the wave's recorded vertices into training samples and takes up to
 // `maxSteps` Adam steps; step i uses samples i, i + steps, i + 2 steps, ...
 // so that every batch spans the whole image.
@@ -624,7 +626,7 @@ int alpine_gpu_reset_accumulation(alpine_gpu_ctx* c)
     return ALPINE_GPU_OK;
 }
 
-int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
+static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (c->cfg.width == 0 || c->cfg.height == 0) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "no framebuffer");
@@ -699,13 +701,51 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
     ag::BvhView bvh;
     bvh.nodes = c->dNodes.as<ag::WideNode>();
     bvh.tris = c->dTris.as<ag::TriRecord>();
-    bvh.nodeCount = c->nodeCount;
-    bvh.triCount = c->triCount;
+    // bounds checks against the allocations, so that a rebuilt BVH of the
+    // same scene replays the same captured graph
+    bvh.nodeCount = (uint32_t)(c->dNodes.bytes / sizeof(ag::WideNode));
+    bvh.triCount = (uint32_t)(c->dTris.bytes / sizeof(ag::TriRecord));
 
     const bool fp64 = c->options.accumulate_fp64 != 0;
     float* acc32 = fp64 ? nullptr : c->dAccum.as<float>();
     double* acc64 = fp64 ? c->dAccum.as<double>() : nullptr;
     cudaStream_t st = c->stream;
+
+    // CUDA graph: the whole wave loop of an unguided render, captured once per
+    // launch configuration and replayed; the first sample index is read from
+    // device memory so that successive renders replay the same graph
+    const bool useGraph = o.cuda_graph != 0 && !guiding;
+    std::vector<unsigned char> key;
+    if (useGraph) {
+        auto put = [&](const void* p, size_t n) {
+            const unsigned char* b = static_cast<const unsigned char*>(p);
+            key.insert(key.end(), b, b + n);
+        };
+        const uint32_t cfgWords[] = {spp, S, pixelChunk, pixels, (uint32_t)stream, (uint32_t)fp64,
+                                     (uint32_t)c->traceBlock, c->options.seed, c->options.russian_roulette_depth,
+                                     c->waveCapacity};
+        const void* ptrs[] = {c->dWave.ptr, c->dAccum.ptr, c->dPixelRng.ptr, c->dStatus};
+        put(cfgWords, sizeof cfgWords);
+        put(ptrs, sizeof ptrs);
+        put(&sc, sizeof sc);
+        put(&bvh, sizeof bvh);
+        if (c->graphExec && key == c->graphKey) {
+            k_set_word<<<1, 1, 0, st>>>(c->dSampleBase, c->totalSamples);
+            cudaError_t e = cudaGraphLaunch(c->graphExec, st);
+            if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+            c->totalSamples += spp;
+            ++c->graphLaunches;
+            return ALPINE_GPU_OK;
+        }
+        if (c->graphExec) {
+            cudaGraphExecDestroy(c->graphExec);
+            c->graphExec = nullptr;
+        }
+        k_set_word<<<1, 1, 0, st>>>(c->dSampleBase, c->totalSamples);
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return c->fail(ALPINE_GPU_ERR_CUDA, "render: stream capture could not begin");
+    }
+    const uint32_t sampleOrigin = useGraph ? 0u : c->totalSamples;
     for (uint32_t done = 0; done < spp;) {
         const bool trainNow = trainEnabled && (o.guide_train_steps == 0 || c->guide.steps() < o.guide_train_steps);
         const uint32_t s = std::min(trainNow ? sTrain : S, spp - done);
@@ -715,7 +755,8 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
             w.numPaths = s * w.numPixels;
             w.pixelBase = px;
             w.samplesInWave = s;
-            w.sampleBase = c->totalSamples + done;
+            w.sampleBase = sampleOrigin + done;
+            w.sampleBaseDev = useGraph ? c->dSampleBase : nullptr;
             w.seed = c->options.seed;
             w.rrStart = stream ? 0u : c->options.russian_roulette_depth;
             w.pixelRng = c->dPixelRng.as<uint4>();
@@ -744,7 +785,8 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
             K.generate(sc, w, stream, st);
             for (uint32_t depth = 0; depth < sc.maxDepth; ++depth) {
                 w.depth = depth;
-                ag::launch_trace_dyn(bvh, w.rays, w.queueCount, w.numPaths, false, w.hits, c->dStatus, st);
+                ag::launch_trace_dyn(bvh, w.rays, w.queueCount, w.numPaths, false, w.hits, c->dStatus, st,
+                                     c->traceBlock);
                 cudaMemsetAsync(w.queueCountNext, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(w.shadowCount, 0, sizeof(uint32_t), st);
                 if (guiding) {
@@ -754,7 +796,7 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
                 }
                 K.shade(sc, w, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,
-                                     c->dStatus, st);
+                                     c->dStatus, st, c->traceBlock);
                 K.resolve(w, w.numPaths, st);
                 std::swap(w.rays, w.raysNext);
                 std::swap(w.queuePath, w.queuePathNext);
@@ -770,17 +812,126 @@ int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
         }
         done += s;
     }
+    if (useGraph) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&c->graphExec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            c->graphExec = nullptr;
+            return c->fail(ALPINE_GPU_ERR_CUDA, std::string("render: graph capture: ") + cudaGetErrorString(e));
+        }
+        c->graphKey = key;
+        ++c->graphCaptures;
+        e = cudaGraphLaunch(c->graphExec, st);
+        if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+        ++c->graphLaunches;
+    }
     c->totalSamples += spp;
-    cudaError_t e = cudaStreamSynchronize(st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("render: ") + cudaGetErrorString(e));
+    return ALPINE_GPU_OK;
+}
+
+// Waits for the context's stream and reads the device status word.
+static int render_wait(alpine_gpu_ctx* c)
+{
+    cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("render: ") + cudaGetErrorString(e));
     return c->check_device_status();
 }
 
+int alpine_gpu_render(alpine_gpu_ctx* c, uint32_t spp)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (int rc = render_enqueue(c, spp)) {
+        cudaStreamSynchronize(c->stream);
+        return rc;
+    }
+    return render_wait(c);
+}
+
+int alpine_gpu_render_async(alpine_gpu_ctx* c, uint32_t spp)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    return render_enqueue(c, spp);
+}
+
+int alpine_gpu_render_wait(alpine_gpu_ctx* c)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    return render_wait(c);
+}
+
+int alpine_gpu_render_graph_stats(alpine_gpu_ctx* c, uint32_t* captures, uint32_t* launches)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (captures) *captures = c->graphCaptures;
+    if (launches) *launches = c->graphLaunches;
+    return ALPINE_GPU_OK;
+}
+
+// Times probe renders over wave sizes and traversal block sizes and keeps the
+// fastest pair (samples per second). The probes add to the accumulation,
+// which is reset afterwards.
+int alpine_gpu_autotune(alpine_gpu_ctx* c, uint32_t probe_spp, alpine_gpu_tuning* out)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (probe_spp == 0) probe_spp = 4;
+    const uint32_t waves[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
+    const int blocks[] = {64, 128, 256};
+    const alpine_gpu_render_options saved = c->options;
+    const int savedBlock = c->traceBlock;
+    alpine_gpu_tuning best{};
+    best.samples_per_second = -1.0f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = ALPINE_GPU_OK;
+    // warm-up: allocations, module loading
+    c->options.max_paths_per_wave = waves[0];
+    rc = alpine_gpu_render(c, 1);
+    const uint32_t pixels = c->cfg.width * c->cfg.height;
+    for (uint32_t wi = 0; rc == ALPINE_GPU_OK && wi < sizeof(waves) / sizeof(waves[0]); ++wi) {
+        // more paths than one wave of all samples cannot help
+        if (wi > 0 && waves[wi - 1] >= (uint64_t)pixels * probe_spp) break;
+        for (int b : blocks) {
+            c->options.max_paths_per_wave = waves[wi];
+            c->traceBlock = b;
+            if ((rc = alpine_gpu_render(c, 1))) break;  // buffers for this wave size
+            cudaEventRecord(e0, c->stream);
+            if ((rc = render_enqueue(c, probe_spp))) break;
+            cudaEventRecord(e1, c->stream);
+            if ((rc = render_wait(c))) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const float rate = ms > 0.0f ? (float)pixels * probe_spp / (ms * 1e-3f) : 0.0f;
+            if (rate > best.samples_per_second) {
+                best.samples_per_second = rate;
+                best.max_paths_per_wave = waves[wi];
+                best.trace_block = (uint32_t)b;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->options = saved;
+    c->traceBlock = savedBlock;
+    if (rc) return rc;
+    c->options.max_paths_per_wave = best.max_paths_per_wave;
+    c->traceBlock = (int)best.trace_block;
+    if (out) *out = best;
+    return alpine_gpu_reset_accumulation(c);
+}
+
+
+
 int alpine_gpu_read_accumulation(alpine_gpu_ctx* c, float* sums, uint32_t* total_samples)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (!c->accumValid) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "nothing rendered");
+    cudaStreamSynchronize(c->stream);  // a render_async may be in flight
     size_t pixels = (size_t)c->cfg.width * c->cfg.height;
     if (sums) {
         if (c->options.accumulate_fp64) {
@@ -800,6 +951,7 @@ int alpine_gpu_read_accumulation_f64(alpine_gpu_ctx* c, double* sums, uint32_t* 
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (!c->accumValid) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "nothing rendered");
+    cudaStreamSynchronize(c->stream);  // a render_async may be in flight
     size_t pixels = (size_t)c->cfg.width * c->cfg.height;
     if (sums) {
         if (c->options.accumulate_fp64) {
@@ -820,6 +972,7 @@ int alpine_gpu_read_sampler_state(alpine_gpu_ctx* c, uint32_t* state)
 {
     if (!c || !state) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     if (!c->accumValid) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "nothing rendered");
+    cudaStreamSynchronize(c->stream);
     size_t pixels = (size_t)c->cfg.width * c->cfg.height;
     if (cudaMemcpy(state, c->dPixelRng.ptr, pixels * sizeof(uint4), cudaMemcpyDeviceToHost) != cudaSuccess)
         return c->fail(ALPINE_GPU_ERR_CUDA, "read_sampler_state");

@@ -56,21 +56,23 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const 
     if (err) atomicOr(status, err);
 }
 
-// Variant whose ray count is read from device memory (wavefront queues).
-template <bool kAny>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_dyn(BvhView bvh, const float4* __restrict__ rays,
-                                                           const uint32_t* __restrict__ count, void* __restrict__ out,
-                                                           uint32_t* __restrict__ status)
+// Variant whose ray count is read from device memory (wavefront queues),
+// with the block size as a parameter (chosen by the autotuner).
+template <bool kAny, int kBlock>
+__global__ void __launch_bounds__(kBlock) k_trace_dyn(BvhView bvh, const float4* __restrict__ rays,
+                                                      const uint32_t* __restrict__ count, void* __restrict__ out,
+                                                      uint32_t* __restrict__ status)
 {
-    __shared__ uint2 stack[kTraversalStack * kTraceBlock];
+    static_assert(kTraversalStack * kBlock * sizeof(uint2) <= 48 * 1024, "static shared memory");
+    __shared__ uint2 stack[kTraversalStack * kBlock];
     const uint32_t n = *count;
-    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
         float4 a = rays[2ull * i];
         float4 b = rays[2ull * i + 1];
         TraceResult r;
         uint32_t err = 0, nv = 0, tv = 0;
         bool hit = trace<kAny>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
-                               kTraceBlock, err, nv, tv);
+                               kBlock, err, nv, tv);
         if (kAny) static_cast<uint8_t*>(out)[i] = hit ? 1 : 0;
         else static_cast<uint4*>(out)[i] = make_uint4(r.prim, __float_as_uint(r.t), __float_as_uint(r.b1), __float_as_uint(r.b2));
         if (err) atomicOr(status, err);
@@ -92,14 +94,25 @@ void launch(const BvhView& bvh, const void* rays, uint64_t n, void* out, uint32_
 }
 }  // namespace
 
+namespace {
+template <int kBlock>
+void launch_dyn(const BvhView& bvh, const float4* r, const uint32_t* count, uint32_t maxCount, bool any, void* out,
+                uint32_t* status, cudaStream_t st)
+{
+    const unsigned blocks = (maxCount + kBlock - 1) / kBlock;
+    if (any) k_trace_dyn<true, kBlock><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    else k_trace_dyn<false, kBlock><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+}
+}  // namespace
+
 void launch_trace_dyn(const BvhView& bvh, const void* rays, const uint32_t* count, uint32_t maxCount, bool any,
-                      void* out, uint32_t* status, cudaStream_t st)
+                      void* out, uint32_t* status, cudaStream_t st, int block)
 {
     if (maxCount == 0) return;
-    unsigned blocks = (maxCount + kTraceBlock - 1) / kTraceBlock;
     const float4* r = static_cast<const float4*>(rays);
-    if (any) k_trace_dyn<true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, count, out, status);
-    else k_trace_dyn<false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, count, out, status);
+    if (block == 64) launch_dyn<64>(bvh, r, count, maxCount, any, out, status, st);
+    else if (block == 256) launch_dyn<256>(bvh, r, count, maxCount, any, out, status, st);
+    else launch_dyn<128>(bvh, r, count, maxCount, any, out, status, st);
 }
 
 void launch_trace_count(const BvhView& bvh, const void* rays, uint64_t n, bool any, unsigned long long* counts,

@@ -18,8 +18,9 @@ void launch_occluded(const BvhView& bvh, const void* rays, uint64_t n, uint8_t* 
 
 // Queue variant: the number of rays is *count (device memory, read by the
 // kernel), at most maxCount. any selects any-hit (uint8 results) or closest.
+// block: threads per block, 64, 128 or 256.
 void launch_trace_dyn(const BvhView& bvh, const void* rays, const uint32_t* count, uint32_t maxCount, bool any,
-                      void* out, uint32_t* status, cudaStream_t st);
+                      void* out, uint32_t* status, cudaStream_t st, int block = kTraceBlock);
 
 // Instrumented traversal: counts[0] += wide nodes fetched, counts[1] += triangles tested.
 void launch_trace_count(const BvhView& bvh, const void* rays, uint64_t n, bool any, unsigned long long* counts,

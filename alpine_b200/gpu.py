@@ -53,7 +53,11 @@ class RenderOptions(C.Structure):
                 ("guide_fraction", C.c_float), ("guide_train", C.c_uint32), ("guide_batch", C.c_uint32),
                 ("guide_lr", C.c_float), ("guide_warmup_steps", C.c_uint32), ("guide_spp_per_wave", C.c_uint32),
                 ("guide_steps_per_wave", C.c_uint32), ("guide_min_roughness", C.c_float),
-                ("guide_train_steps", C.c_uint32)]
+                ("guide_train_steps", C.c_uint32), ("cuda_graph", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("max_paths_per_wave", C.c_uint32), ("trace_block", C.c_uint32), ("samples_per_second", C.c_float)]
 
 
 MATERIAL_DTYPE = np.dtype([("kind", np.uint32), ("base_color", np.float32, 3), ("roughness", np.float32)])
@@ -112,6 +116,10 @@ def lib():
         L.alpine_gpu_set_render_options.argtypes = [vp, C.POINTER(RenderOptions)]
         L.alpine_gpu_reset_accumulation.argtypes = [vp]
         L.alpine_gpu_render.argtypes = [vp, C.c_uint32]
+        L.alpine_gpu_render_async.argtypes = [vp, C.c_uint32]
+        L.alpine_gpu_render_wait.argtypes = [vp]
+        L.alpine_gpu_render_graph_stats.argtypes = [vp, u32p, u32p]
+        L.alpine_gpu_autotune.argtypes = [vp, C.c_uint32, C.POINTER(Tuning)]
         L.alpine_gpu_read_accumulation.argtypes = [vp, vp, u32p]
         L.alpine_gpu_read_accumulation_f64.argtypes = [vp, vp, u32p]
         L.alpine_gpu_post_process.argtypes = [vp, C.c_int, vp, vp]
@@ -335,12 +343,13 @@ class Context:
     def set_render_options(self, sampler=RNG_COUNTER, max_paths_per_wave=0, russian_roulette_depth=0, seed=0,
                            accumulate_fp64=False, guide=False, guide_fraction=0.5, guide_train=True,
                            guide_batch=16384, guide_lr=1e-2, guide_warmup_steps=0, guide_spp_per_wave=1,
-                           guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0):
+                           guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0, cuda_graph=False):
         """Options of alpine_gpu_render_options; the guide_* fields apply when
         guide is set (learned path guiding, counter sampler only)."""
         o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64),
                           int(guide), guide_fraction, int(guide_train), guide_batch, guide_lr, guide_warmup_steps,
-                          guide_spp_per_wave, guide_steps_per_wave, guide_min_roughness, guide_train_steps)
+                          guide_spp_per_wave, guide_steps_per_wave, guide_min_roughness, guide_train_steps,
+                          int(cuda_graph))
         self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
 
     def reset_accumulation(self):
@@ -348,6 +357,26 @@ class Context:
 
     def render(self, spp):
         self._check(self.L.alpine_gpu_render(self.h, spp))
+
+    def render_async(self, spp):
+        """Enqueues a render on the context's stream (see alpine_gpu_render_async)."""
+        self._check(self.L.alpine_gpu_render_async(self.h, spp))
+
+    def render_wait(self):
+        self._check(self.L.alpine_gpu_render_wait(self.h))
+
+    def graph_stats(self):
+        """(render graphs captured, render graphs launched)."""
+        a, b = C.c_uint32(), C.c_uint32()
+        self._check(self.L.alpine_gpu_render_graph_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, probe_spp=4):
+        """Picks the wave size and traversal block size for this scene; resets the accumulation."""
+        t = Tuning()
+        self._check(self.L.alpine_gpu_autotune(self.h, probe_spp, C.byref(t)))
+        return {"max_paths_per_wave": t.max_paths_per_wave, "trace_block": t.trace_block,
+                "samples_per_second": t.samples_per_second}
 
     def read_accumulation(self, width, height, fp64=False):
         """(sums float[H, W, 9] = colour, albedo, normal sums; total samples)."""

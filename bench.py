@@ -13,6 +13,9 @@ shadow rays with tmax uniform in (0, 1]. A step traces all 8,388,608 queries.
 the C ABI with pinned host buffers (host->device copy of the rays and
 device->host copy of the results inside the timed region).
 
+`batch` (rank 0, one GPU): frames/s and samples/s of 48 animated scenes
+rendered together (morph + BVH rebuild + render per scene per frame).
+
 `guiding` (rank 0, one GPU): time to relMSE 0.01, guided vs plain MIS, on the
 glossy interior (20 x 4 x 12 m room, 2.0M triangles, 70% GGX with roughness
 in [0.02, 0.4], sky of radiance 5 through two 1 x 2 m window openings, depth
@@ -59,6 +62,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided vs plain time-to-relMSE measurement")
     p.add_argument("--guiding-ref-spp", type=int, default=65536)
+    p.add_argument("--batch-frames", type=int, default=2,
+                   help="frames of the 48-scene animated batch to time (0 = skip)")
     p.add_argument("--profile", action="store_true",
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     return p.parse_args()
@@ -288,6 +293,27 @@ def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
             "projected_time_to_target_s": (plain_spp * W * H / rate) if plain_spp else None}
 
 
+def batch_benchmark(device, frames):
+    """48 independent animated scenes (BASELINE cfg4 shapes; alpine_b200.batch):
+    every frame morphs and rebuilds every BVH and renders every scene at its
+    resolution and spp, the renders of all scenes in flight together, each a
+    replayed CUDA graph. One warm-up frame (graph capture) is not timed."""
+    from alpine_b200 import batch
+
+    cfgs = batch.batch_configs()
+    t0 = time.perf_counter()
+    br = batch.BatchRenderer(cfgs, device=device, cuda_graph=True)
+    setup = time.perf_counter() - t0
+    br.run(1, start=0)
+    r = br.run(frames, start=1)
+    r.update({"scenes": len(cfgs), "triangles": br.triangles, "setup_s": setup,
+              "samples_per_frame": sum(c["width"] * c["height"] * c["spp"] for c in cfgs),
+              "workload": "48 scenes, tris log-uniform 1k-500k, res 128^2-1024^2, spp 4/16/64, 1-64 quad lights, "
+                          "0.02-amplitude sinusoid morph, BVH rebuilt per frame, depth 8, light-BVH sampler"})
+    br.close()
+    return r
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU WideBvh on the host cores, same
     metric; each step is a 131,072-query sample of the workload."""
@@ -454,11 +480,14 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
-    guiding = None
-    if rank == 0 and world == 1 and not args.no_guiding:
+    guiding = batched = None
+    if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames):
         ctx.close()
         ctx = None
+    if rank == 0 and world == 1 and not args.no_guiding:
         guiding = guiding_benchmark(local, args.guiding_ref_spp)
+    if rank == 0 and world == 1 and args.batch_frames:
+        batched = batch_benchmark(local, args.batch_frames)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -479,6 +508,7 @@ def run_ours(args):
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),
             "guiding": guiding,
+            "batch": batched,
         }
         print(json.dumps(line), flush=True)
     if ctx is not None:

@@ -291,7 +291,11 @@ ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3]
  *   near-specular lobe is already sampled well and is narrower than the
  *   guide's lobes); 0 = guide every vertex.
  * guide_train_steps: stop training after this many Adam steps since the
- *   guide's last reset (the guide is then used as it is); 0 = no limit. */
+ *   guide's last reset (the guide is then used as it is); 0 = no limit.
+ * cuda_graph: 1 = capture the whole wave loop of an unguided render as a CUDA
+ *   graph and replay it while the launch configuration (spp, sizes, device
+ *   buffers, camera, lights, options) stays the same; a rebuilt BVH of the
+ *   same scene replays the same graph. Results are identical either way. */
 #define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
 #define ALPINE_GPU_SAMPLER_COUNTER 1u
 typedef struct alpine_gpu_render_options {
@@ -310,6 +314,7 @@ typedef struct alpine_gpu_render_options {
     uint32_t guide_steps_per_wave;
     float guide_min_roughness;
     uint32_t guide_train_steps;
+    uint32_t cuda_graph;
 } alpine_gpu_render_options;
 ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
 
@@ -320,6 +325,28 @@ ALPINE_GPU_API int alpine_gpu_reset_accumulation(alpine_gpu_ctx* ctx);
 /* alpine::render(spp) (alpine.h:61, alpine.cpp:271-288): adds spp samples
  * per pixel to the accumulation. Synchronous. */
 ALPINE_GPU_API int alpine_gpu_render(alpine_gpu_ctx* ctx, uint32_t spp);
+
+/* The same without waiting: the render is enqueued on the context's stream
+ * (an unguided render never waits for the GPU; a training guided render
+ * waits between waves). alpine_gpu_render_wait waits for it and reports
+ * device-side errors. Contexts are independent, so renders of several
+ * contexts enqueued from one thread run concurrently on the GPU. Reading the
+ * accumulation waits as well. */
+ALPINE_GPU_API int alpine_gpu_render_async(alpine_gpu_ctx* ctx, uint32_t spp);
+ALPINE_GPU_API int alpine_gpu_render_wait(alpine_gpu_ctx* ctx);
+/* Number of render graphs captured and launched on this context. */
+ALPINE_GPU_API int alpine_gpu_render_graph_stats(alpine_gpu_ctx* ctx, uint32_t* captures, uint32_t* launches);
+
+/* Autotuner (no counterpart in the reference): renders probe_spp samples per
+ * pixel (0 = 4) for each wave size (2^18 ... 2^22 paths) and traversal block
+ * size (64, 128, 256 threads), keeps the fastest pair for this context and
+ * writes it; then resets the accumulation. */
+typedef struct alpine_gpu_tuning {
+    uint32_t max_paths_per_wave;
+    uint32_t trace_block;
+    float samples_per_second;
+} alpine_gpu_tuning;
+ALPINE_GPU_API int alpine_gpu_autotune(alpine_gpu_ctx* ctx, uint32_t probe_spp, alpine_gpu_tuning* result);
 
 /* Per-pixel sums of colour, albedo and normal (9 floats per pixel, the
  * reference's RenderTarget layout, src/denoisers/denoiser.h:7-12) and the
