@@ -336,6 +336,102 @@ def sinusoid_morph(verts, normals, amplitude=0.02, phase=0.0, frames=60, period=
     return out
 
 
+def blackbody_rgb(kelvin):
+    """Relative linear RGB of a blackbody: Planck's law sampled at 610, 550
+    and 465 nm, normalised to a maximum of 1."""
+    h, c, k = 6.62607015e-34, 2.99792458e8, 1.380649e-23
+    lam = np.array([610e-9, 550e-9, 465e-9])
+    b = 1.0 / (lam ** 5 * (np.exp(h * c / (lam * k * kelvin)) - 1.0))
+    return b / b.max()
+
+
+def city_scene(seed=1, buildings=2000, lights=131072, extent=1000.0, panel=2.5, window=(1.2, 1.5)):
+    """Many-light city: `buildings` extruded boxes (footprints uniform in
+    [5, 40] m, heights log-normal(ln 20, 0.6)) on a ground plane of
+    `extent` m, facades tessellated into `panel`-metre panels, and `lights`
+    emissive window quads on the facades, facing outwards (power log-normal
+    with sigma 1.5, colour temperature uniform in [2700, 6500] K). Materials:
+    GGX with roughness uniform in [0.05, 1], metallic (conductor) with
+    probability 0.2, else a dielectric (F0 0.04 coat over a diffuse base)."""
+    rng = np.random.default_rng(seed)
+    half = extent / 2
+    verts, idx, tmat, materials = [], [], [], []
+    nv = 0
+
+    def add_quads(corners):  # corners [n, 4, 3] counter-clockwise seen from the front
+        nonlocal nv
+        n = corners.shape[0]
+        verts.append(corners.reshape(-1, 3))
+        b = nv + 4 * np.arange(n, dtype=np.int64)[:, None]
+        idx.append(np.concatenate([b + [0, 1, 2], b + [0, 2, 3]]).reshape(2, n, 3).transpose(1, 0, 2).reshape(-1, 3))
+        nv += 4 * n
+        return 2 * n
+
+    materials.append((0, (0.35, 0.35, 0.35), 1.0))  # ground
+    g = np.array([[[-half, 0, -half], [-half, 0, half], [half, 0, half], [half, 0, -half]]], np.float64)
+    tmat.append(np.zeros(add_quads(g), np.uint32))
+    facades = []  # (origin, u axis, v axis, width, height) per facade
+    for b in range(buildings):
+        w, d = rng.uniform(5.0, 40.0, 2)
+        hgt = float(np.exp(rng.normal(math.log(20.0), 0.6)))
+        cx, cz = rng.uniform(-half + 40, half - 40, 2)
+        ang = rng.uniform(0, math.pi / 2)
+        ca, sa = math.cos(ang), math.sin(ang)
+        ex, ez = np.array([ca, 0, -sa]), np.array([sa, 0, ca])
+        c0 = np.array([cx, 0.0, cz]) - ex * w / 2 - ez * d / 2
+        base = [c0, c0 + ex * w, c0 + ex * w + ez * d, c0 + ez * d]
+        kind = 1 if rng.random() < 0.2 else 0
+        materials.append((kind, tuple(float(x) for x in rng.uniform(0.3, 0.9, 3)), float(rng.uniform(0.05, 1.0))))
+        mid = len(materials) - 1
+        quads = []
+        for k in range(4):
+            p0, p1 = base[k], base[(k + 1) % 4]
+            length = float(np.linalg.norm(p1 - p0))
+            u = (p1 - p0) / length
+            nu, nh = max(1, int(length / panel)), max(1, int(hgt / panel))
+            us = np.linspace(0, length, nu + 1)
+            hs = np.linspace(0, hgt, nh + 1)
+            U0, H0 = np.meshgrid(us[:-1], hs[:-1], indexing="ij")
+            U1, H1 = np.meshgrid(us[1:], hs[1:], indexing="ij")
+            a = p0 + U0.reshape(-1, 1) * u + H0.reshape(-1, 1) * np.array([0, 1, 0])
+            bb = p0 + U1.reshape(-1, 1) * u + H0.reshape(-1, 1) * np.array([0, 1, 0])
+            cc = p0 + U1.reshape(-1, 1) * u + H1.reshape(-1, 1) * np.array([0, 1, 0])
+            dd = p0 + U0.reshape(-1, 1) * u + H1.reshape(-1, 1) * np.array([0, 1, 0])
+            # walls go counter-clockwise around the footprint seen from above,
+            # so (a, d, c, b) faces outwards
+            quads.append(np.stack([a, dd, cc, bb], 1))
+            facades.append((p0, u, length, hgt))
+        top = np.array([[base[0] + [0, hgt, 0], base[3] + [0, hgt, 0], base[2] + [0, hgt, 0], base[1] + [0, hgt, 0]]])
+        quads.append(top)
+        q = np.concatenate(quads)
+        tmat.append(np.full(add_quads(q), mid, np.uint32))
+    v = np.concatenate(verts).astype(np.float32)
+    t = np.concatenate(idx).astype(np.uint32)
+    # orient every triangle so that its normal points away from its building's centre line or up
+    meshes = [{"verts": v, "idx": t, "normals": None, "tri_material": np.concatenate(tmat)}]
+    light_list = []
+    fa = rng.integers(0, len(facades), lights)
+    temps = rng.uniform(2700.0, 6500.0, lights)
+    powers = np.exp(rng.normal(0.0, 1.5, lights)) * 20.0
+    ww, wh = window
+    for i in range(lights):
+        p0, u, length, hgt = facades[fa[i]]
+        if length < ww + 0.2 or hgt < wh + 1.0:
+            continue
+        s_ = rng.uniform(0.1, length - ww - 0.1)
+        y = rng.uniform(0.5, hgt - wh - 0.2)
+        outward = np.cross(np.array([0.0, 1.0, 0.0]), u)  # facing away from the footprint
+        corner = p0 + u * s_ + np.array([0.0, y, 0.0]) + outward * 0.05
+        area = ww * wh
+        L = powers[i] / (area * math.pi) * blackbody_rgb(temps[i])
+        # edges (0, wh, 0) x (ww u): cross points along `outward`
+        light_list.append(("quad", tuple(float(x) for x in L), tuple(float(x) for x in corner),
+                           (0.0, float(wh), 0.0), tuple(float(x) for x in u * ww)))
+    camera = ((0.0, 180.0, -half * 0.9), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), math.radians(50.0))
+    return {"meshes": meshes, "materials": materials, "lights": light_list, "camera": camera,
+            "background": (0.01, 0.01, 0.02)}
+
+
 def add_random_lights(scene, n, seed=5, kinds=("disk", "point")):
     """Adds n seeded disk / point lights spread over the room's ceiling half
     (many-light sampler tests)."""

@@ -13,6 +13,9 @@ shadow rays with tmax uniform in (0, 1]. A step traces all 8,388,608 queries.
 the C ABI with pinned host buffers (host->device copy of the rays and
 device->host copy of the results inside the timed region).
 
+`many_lights` (rank 0, one GPU): the many-light city, samples/s and relMSE
+per light sampler (uniform, power, light BVH).
+
 `batch` (rank 0, one GPU): frames/s and samples/s of 48 animated scenes
 rendered together (morph + BVH rebuild + render per scene per frame).
 
@@ -64,6 +67,7 @@ def parse_args():
     p.add_argument("--guiding-ref-spp", type=int, default=65536)
     p.add_argument("--batch-frames", type=int, default=2,
                    help="frames of the 48-scene animated batch to time (0 = skip)")
+    p.add_argument("--no-many-lights", action="store_true", help="skip the many-light city measurement")
     p.add_argument("--profile", action="store_true",
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     return p.parse_args()
@@ -314,6 +318,61 @@ def batch_benchmark(device, frames):
     return r
 
 
+def many_lights_benchmark(device, spp=4, cmp_res=(480, 270), cmp_spp=64, ref_spp=4096):
+    """Many-light city (BASELINE cfg3 shapes; alpine_b200.scenes.city_scene:
+    2,000 buildings, ~1.2M triangles, 131,072 window quad lights): samples/s
+    of each light sampler at 1920x1080, depth 8 (`spp` samples per pixel after
+    a warm-up); and at cmp_res the relMSE of each sampler at cmp_spp against a
+    ref_spp light-BVH image, with the equal-time efficiency 1 / (relMSE x
+    time)."""
+    from alpine_b200 import gpu, scenes
+
+    t0 = time.perf_counter()
+    scene = scenes.city_scene()
+    gen_s = time.perf_counter() - t0
+    names = {gpu.SAMPLER_UNIFORM: "uniform", gpu.SAMPLER_POWER: "power", gpu.SAMPLER_BVH: "light_bvh"}
+    out = {"triangles": int(sum(m["idx"].shape[0] for m in scene["meshes"])), "lights": len(scene["lights"]),
+           "scene_generation_s": gen_s, "resolution": [1920, 1080], "depth": 8, "spp": spp, "samplers": {}}
+
+    def context(w, h, kind, seed):
+        c = gpu.Context(device, w, h, 8)
+        scenes.load_scene(c, scene, w, h)
+        t1 = time.perf_counter()
+        c.build_light_sampler(kind)
+        build = time.perf_counter() - t1
+        c.set_render_options(sampler=gpu.RNG_COUNTER, seed=seed)
+        c.reset_accumulation()
+        return c, build
+
+    for kind, name in names.items():
+        c, build = context(1920, 1080, kind, 1)
+        c.render(1)
+        t1 = time.perf_counter()
+        c.render(spp)
+        dt = time.perf_counter() - t1
+        c.close()
+        out["samplers"][name] = {"samples_per_s": 1920 * 1080 * spp / dt, "sampler_build_s": build}
+    W, H = cmp_res
+    c, _ = context(W, H, gpu.SAMPLER_BVH, 99)
+    c.render(ref_spp)
+    a, n = c.read_accumulation(W, H, fp64=True)
+    ref = a[..., :3].astype(np.float64) / n
+    c.close()
+    for kind, name in names.items():
+        c, _ = context(W, H, kind, 3)
+        c.render(1)
+        c.reset_accumulation()
+        t1 = time.perf_counter()
+        c.render(cmp_spp)
+        dt = time.perf_counter() - t1
+        a, n = c.read_accumulation(W, H, fp64=True)
+        c.close()
+        e = relmse(a[..., :3].astype(np.float64) / n, ref)
+        out["samplers"][name].update({"relmse_at_cmp_spp": e, "cmp_seconds": dt, "efficiency": 1.0 / (e * dt)})
+    out["comparison"] = f"{W}x{H}, {cmp_spp} spp vs a {ref_spp}-spp light-BVH image"
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU WideBvh on the host cores, same
     metric; each step is a 131,072-query sample of the workload."""
@@ -480,10 +539,12 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
-    guiding = batched = None
-    if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames):
+    guiding = batched = many = None
+    if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames or not args.no_many_lights):
         ctx.close()
         ctx = None
+    if rank == 0 and world == 1 and not args.no_many_lights:
+        many = many_lights_benchmark(local)
     if rank == 0 and world == 1 and not args.no_guiding:
         guiding = guiding_benchmark(local, args.guiding_ref_spp)
     if rank == 0 and world == 1 and args.batch_frames:
@@ -509,6 +570,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "guiding": guiding,
             "batch": batched,
+            "many_lights": many,
         }
         print(json.dumps(line), flush=True)
     if ctx is not None:
