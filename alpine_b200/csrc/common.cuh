@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #define AG_HD __host__ __device__ __forceinline__
 #define AG_D __device__ __forceinline__

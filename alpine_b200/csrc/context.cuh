@@ -108,7 +108,7 @@ struct alpine_gpu_ctx {
     // lights and the light sampler
     std::vector<ag::Light> lights;
     bool lightsDirty = true;
-    ag::DeviceBuffer dLights, dAlias, dLightNodes;
+    ag::DeviceBuffer dLights, dAlias, dLightNodes, dLightPairs;
     uint32_t samplerKind = ag::kSamplerNone;
     uint32_t samplerLightCount = 0;
     uint32_t lightNodeCount = 0;

@@ -565,7 +565,27 @@ int alpine_gpu_build_light_sampler(alpine_gpu_ctx* c, int type)
         std::vector<ag::LightNode> nodes;
         nodes.reserve(2 * all.size());
         create_light_node(c->lights, all, nodes);
-        if (!upload(c->dLightNodes, nodes, c->stream)) return c->fail(ALPINE_GPU_ERR_CUDA, "light BVH upload failed");
+        // the descent's packed records: both children of every interior node
+        std::vector<ag::LightPair> pairs(nodes.size());
+        auto ref = [&](int32_t i) {
+            const ag::LightNode& n = nodes[i];
+            const int32_t r = (n.left >= 0 && n.right >= 0) ? i : -(n.light + 1);
+            float f;
+            std::memcpy(&f, &r, sizeof f);
+            return f;
+        };
+        for (size_t i = 0; i < nodes.size(); ++i) {
+            const ag::LightNode& n = nodes[i];
+            if (n.left < 0 || n.right < 0) continue;
+            const ag::LightNode& a = nodes[n.left];
+            const ag::LightNode& b = nodes[n.right];
+            pairs[i].lo0 = make_float4(a.bmin.x, a.bmin.y, a.bmin.z, a.power);
+            pairs[i].hi0 = make_float4(a.bmax.x, a.bmax.y, a.bmax.z, ref(n.left));
+            pairs[i].lo1 = make_float4(b.bmin.x, b.bmin.y, b.bmin.z, b.power);
+            pairs[i].hi1 = make_float4(b.bmax.x, b.bmax.y, b.bmax.z, ref(n.right));
+        }
+        if (!upload(c->dLightNodes, nodes, c->stream) || !upload(c->dLightPairs, pairs, c->stream))
+            return c->fail(ALPINE_GPU_ERR_CUDA, "light BVH upload failed");
         c->lightNodeCount = (uint32_t)nodes.size();
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess)
@@ -693,6 +713,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
     sc.lights.lights = c->dLights.as<ag::Light>();
     sc.lights.alias = c->dAlias.as<ag::AliasBin>();
     sc.lights.nodes = c->dLightNodes.as<ag::LightNode>();
+    sc.lights.pairs = c->dLightPairs.as<ag::LightPair>();
     sc.background = c->background;
     sc.cam = c->camera;
     sc.width = c->cfg.width;

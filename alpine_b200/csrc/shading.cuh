@@ -531,13 +531,47 @@ AG_HD float light_node_importance(const LightNode& n, float3 p, float3 nrm)
     return imp;
 }
 
+// The light BVH as the sampler descends it: per interior node, both
+// children's bounds and power in one 64-byte record (one aligned load per
+// level). ref: the child's interior node index, or -(light + 1) for a leaf.
+struct LightPair {
+    float4 lo0;  // child 0: bmin.xyz, power
+    float4 hi0;  // child 0: bmax.xyz, ref (int bits)
+    float4 lo1;  // child 1
+    float4 hi1;
+};
+static_assert(sizeof(LightPair) == 64, "LightPair layout");
+
 struct LightSamplerView {
     uint32_t kind;
     uint32_t count;
     const Light* lights;
     const AliasBin* alias;
-    const LightNode* nodes;
+    const LightNode* nodes;   // the tree (the root is read when it is a single leaf)
+    const LightPair* pairs;   // the same tree packed for the descent
 };
+
+AG_HD int32_t float_bits(float f)
+{
+#ifdef __CUDA_ARCH__
+    return __float_as_int(f);
+#else
+    int32_t i;
+    memcpy(&i, &f, sizeof i);
+    return i;
+#endif
+}
+
+AG_HD LightNode light_child(float4 lo, float4 hi)
+{
+    LightNode n;
+    n.power = lo.w;
+    n.bmin = mk3(lo.x, lo.y, lo.z);
+    n.bmax = mk3(hi.x, hi.y, hi.z);
+    n.left = n.right = -1;
+    n.light = -1;
+    return n;
+}
 
 // LightSampler::sample: uniform (uniform_light_sampler.cpp:15-27), power
 // (power_light_sampler.cpp:25-35 + alias_table.cpp:71-81), BVH
@@ -560,26 +594,37 @@ AG_HD int sample_light(const LightSamplerView& ls, float u, float3 hit, float3 n
         return (int)idx;
     }
     // BVH: stochastic descent by importance with u remapping
+    const LightNode& root = ls.nodes[0];
+    if (root.left < 0 || root.right < 0) {  // a single light
+        if (root.light >= 0 && light_node_importance(root, hit, ns) > 0.0f) {
+            pdf = 1.0f;
+            return root.light;
+        }
+        return -1;
+    }
     int node = 0;
     float p = 1.0f;
     for (int guard = 0; guard < 128; ++guard) {
-        const LightNode& n = ls.nodes[node];
-        if (n.left >= 0 && n.right >= 0) {
-            float w0 = light_node_importance(ls.nodes[n.left], hit, ns);
-            float w1 = light_node_importance(ls.nodes[n.right], hit, ns);
-            if (w0 == 0.0f && w1 == 0.0f) return -1;
-            float up = (w0 + w1) * u;
-            int idx = up < w0 ? 0 : 1;
-            node = idx == 0 ? n.left : n.right;
-            p *= (idx == 0 ? w0 : w1) / (w0 + w1);
-            u = idx == 0 ? fminf(up / w0, kOneMinusEpsilon) : fminf((up - w0) / w1, kOneMinusEpsilon);
-        } else {
-            if (n.light >= 0 && light_node_importance(n, hit, ns) > 0.0f) {
+        const float4* q = reinterpret_cast<const float4*>(ls.pairs + node);
+        const float4 lo0 = q[0], hi0 = q[1], lo1 = q[2], hi1 = q[3];
+        const float w0 = light_node_importance(light_child(lo0, hi0), hit, ns);
+        const float w1 = light_node_importance(light_child(lo1, hi1), hit, ns);
+        if (w0 == 0.0f && w1 == 0.0f) return -1;
+        float up = (w0 + w1) * u;
+        int idx = up < w0 ? 0 : 1;
+        const float wc = idx == 0 ? w0 : w1;
+        p *= wc / (w0 + w1);
+        u = idx == 0 ? fminf(up / w0, kOneMinusEpsilon) : fminf((up - w0) / w1, kOneMinusEpsilon);
+        const int ref = float_bits(idx == 0 ? hi0.w : hi1.w);
+        if (ref < 0) {
+            // a leaf: its importance is wc (the same function of the same node)
+            if (wc > 0.0f) {
                 pdf = p;
-                return n.light;
+                return -ref - 1;
             }
             return -1;
         }
+        node = ref;
     }
     return -1;
 }
