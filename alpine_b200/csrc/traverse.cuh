@@ -80,19 +80,20 @@ AG_D float safe_rcp(float d)
 
 AG_D uint4 ldg4(const void* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
 
-// Exact float value of byte k of w: either by the conversion unit (I2F,
-// measured faster on B200) or by placing the byte under the exponent of 2^23
-// (PRMT) and subtracting 2^23 (FADD).
-#ifndef AG_BYTE_CVT_I2F
-#define AG_BYTE_CVT_I2F 1
+// Exact float value of byte k of w, by the conversion unit (I2F, XU pipe) or
+// by placing the byte under the exponent of 2^23 (PRMT) and subtracting 2^23
+// (FADD), which runs on the ALU and FMA pipes. Bit i of AG_CVT_PRMT_MASK
+// selects the second form for plane group i (near x, y, z, far x, y, z), so
+// the 48 conversions of a node can be split between the pipes.
+#ifndef AG_CVT_PRMT_MASK
+#define AG_CVT_PRMT_MASK 0x12  // measured best on B200: y planes on ALU + FMA, the rest on XU
 #endif
+template <int kGroup>
 AG_D float byte_to_float(uint32_t w, uint32_t k)
 {
-#if AG_BYTE_CVT_I2F
+    if ((AG_CVT_PRMT_MASK >> kGroup) & 1)
+        return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7440u | k)) - 8388608.0f;
     return float((w >> (8 * k)) & 0xffu);
-#else
-    return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7440u | k)) - 8388608.0f;
-#endif
 }
 
 AG_D float max3f(float a, float b, float c)
@@ -135,12 +136,12 @@ AG_D uint32_t intersect_children(const uint4& w0, const uint4& w1, const uint4& 
     for (int h = 0; h < 2; ++h) {
 #pragma unroll
         for (uint32_t k = 0; k < 4; ++k) {
-            float tnx = fmaf(byte_to_float(nearX[h], k), sx, ox);
-            float tny = fmaf(byte_to_float(nearY[h], k), sy, oy);
-            float tnz = fmaf(byte_to_float(nearZ[h], k), sz, oz);
-            float tfx = fmaf(byte_to_float(farX[h], k), sx, ox);
-            float tfy = fmaf(byte_to_float(farY[h], k), sy, oy);
-            float tfz = fmaf(byte_to_float(farZ[h], k), sz, oz);
+            float tnx = fmaf(byte_to_float<0>(nearX[h], k), sx, ox);
+            float tny = fmaf(byte_to_float<1>(nearY[h], k), sy, oy);
+            float tnz = fmaf(byte_to_float<2>(nearZ[h], k), sz, oz);
+            float tfx = fmaf(byte_to_float<3>(farX[h], k), sx, ox);
+            float tfy = fmaf(byte_to_float<4>(farY[h], k), sy, oy);
+            float tfz = fmaf(byte_to_float<5>(farZ[h], k), sz, oz);
             float tn = max3f(tnx, tny, fmaxf(tnz, tmin));
             float tf = min3f(tfx, tfy, tfz) * kBoxExitScale;
             if (tn <= tf && tn <= tmax) {
