@@ -576,16 +576,20 @@ AG_HD LightNode light_child(float4 lo, float4 hi)
 // LightSampler::sample: uniform (uniform_light_sampler.cpp:15-27), power
 // (power_light_sampler.cpp:25-35 + alias_table.cpp:71-81), BVH
 // (bvh_light_sampler.cpp:267-319). Returns the light index or -1.
+// kKind: the sampler kind when it is known at compile time (-1: read ls.kind),
+// so that a kernel specialised for one sampler holds only its code.
+template <int kKind = -1>
 AG_HD int sample_light(const LightSamplerView& ls, float u, float3 hit, float3 ns, float& pdf)
 {
-    if (ls.count == 0 || ls.kind == kSamplerNone) return -1;
-    if (ls.kind == kSamplerUniform) {
+    const uint32_t kind = kKind >= 0 ? (uint32_t)kKind : ls.kind;
+    if (ls.count == 0 || kind == kSamplerNone) return -1;
+    if (kind == kSamplerUniform) {
         uint32_t i = (uint32_t)(u * (float)ls.count);
         if (i > ls.count - 1) i = ls.count - 1;
         pdf = 1.0f / (float)ls.count;
         return (int)i;
     }
-    if (ls.kind == kSamplerPower) {
+    if (kind == kSamplerPower) {
         uint32_t b = (uint32_t)(u * (float)ls.count);
         if (b > ls.count - 1) b = ls.count - 1;
         float up = fminf(u * (float)ls.count - (float)b, kOneMinusEpsilon);
