@@ -1,0 +1,50 @@
+"""Small fixed rendering workloads for profiling (ncu launch lists and
+captures) and quick timing. Each renders twice, so a capture can skip the
+first render's launches.
+
+    python -m alpine_b200.workloads room     # 256x256, 2 x 16 spp, depth 8, RR from depth 3,
+                                             # power sampler, quad ceiling light (the small room)
+    python -m alpine_b200.workloads guided   # glossy interior 320x180, depth 12, guided:
+                                             # 16 Adam steps, then 2 x 32 spp
+    python -m alpine_b200.workloads city     # many-light city 960x540, 1 + 2 spp, depth 8, light BVH
+"""
+from __future__ import annotations
+
+import sys
+import time
+
+from . import gpu, scenes
+
+
+def run(mode: str, device: int = 0) -> float:
+    """Runs one workload; returns the wall time of its second render (s)."""
+    if mode == "room":
+        sc, (W, H), depth = scenes.room_scene(light="quad"), (256, 256), 8
+        opts, sampler, spp = dict(russian_roulette_depth=3), gpu.SAMPLER_POWER, (16, 16)
+    elif mode == "guided":
+        sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
+        opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
+                    guide_min_roughness=0.2, guide_train_steps=16)
+        sampler, spp = None, (32, 32)
+    elif mode == "city":
+        sc, (W, H), depth = scenes.city_scene(), (960, 540), 8
+        opts, sampler, spp = {}, gpu.SAMPLER_BVH, (1, 2)
+    else:
+        raise ValueError(f"unknown workload {mode!r}")
+    c = gpu.Context(device, W, H, depth)
+    scenes.load_scene(c, sc, W, H)
+    if sampler is not None:
+        c.build_light_sampler(sampler)
+    c.set_render_options(sampler=gpu.RNG_COUNTER, **opts)
+    c.reset_accumulation()
+    c.render(spp[0])
+    t0 = time.perf_counter()
+    c.render(spp[1])
+    dt = time.perf_counter() - t0
+    c.close()
+    return dt
+
+
+if __name__ == "__main__":
+    for m in sys.argv[1:] or ["room"]:
+        print(f"{m}: second render {run(m) * 1e3:.1f} ms", flush=True)
