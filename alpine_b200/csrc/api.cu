@@ -26,6 +26,7 @@ std::string status_msg(uint32_t bits)
     if (bits & ag::kErrIterations) m += " traversal visit cap reached;";
     if (bits & ag::kErrBuildDepth) m += " BVH build level cap reached;";
     if (bits & ag::kErrQueueOverflow) m += " wavefront queue overflow;";
+    if (bits & ag::kErrTensorWait) m += " tensor-core completion wait timed out;";
     return m;
 }
 

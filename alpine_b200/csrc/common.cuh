@@ -20,6 +20,7 @@ enum DeviceError : uint32_t {
     kErrIterations = 1u << 2,      // traversal visit cap reached
     kErrBuildDepth = 1u << 3,      // BVH build exceeded its level cap
     kErrQueueOverflow = 1u << 4,   // wavefront queue full
+    kErrTensorWait = 1u << 5,      // a tensor-core (tcgen05) completion wait ran out
 };
 
 // ---------------------------------------------------------------------------

@@ -178,6 +178,233 @@ __global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Quer
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// One CTA of 128 threads (one warpgroup) runs tiles of 128 queries: thread r
+// encodes query r of the tile into row r of the activation tile A[128 x 64]
+// (bf16, shared memory); per layer one elected thread issues four
+// tcgen05.mma (M 128, N 64 or 48, K 16, bf16 x bf16 -> fp32) from A and the
+// layer's weights W_l[N x 64] (shared memory) into a 64-column accumulator in
+// tensor memory, and commits them to an mbarrier; then warp w reads rows
+// 32w..32w+31 back from tensor memory (tcgen05.ld 32x32b), applies ReLU and
+// writes the bf16 row into A for the next layer.
+//
+// Operands use the no-swizzle K-major layout of 8 x 16-byte core matrices:
+// element (row, k) at (row / 8) * 1024 + (k / 8) * 128 + (row % 8) * 16 +
+// (k % 8) * 2 bytes, i.e. leading-dimension (K) core-matrix stride 128 B and
+// stride-dimension (M/N) core-matrix stride 1024 B. Every completion wait
+// is bounded: when it runs out the CTA records kErrTensorWait, stops, and
+// still frees its tensor memory.
+constexpr int kTcRows = 128;                       // queries per tile (MMA M)
+constexpr uint32_t kTcCols = 64;                   // tensor-memory columns (fp32 accumulator)
+constexpr uint32_t kTcLbo = 128, kTcSbo = 1024;    // core-matrix strides (bytes)
+constexpr int kTcATile = kTcRows * kIn * 2;        // 16 KiB
+__host__ __device__ constexpr int tc_w_offset(int l)  // bytes of W_0 .. W_{l-1}
+{
+    int o = 0;
+    for (int i = 0; i < l; ++i) o += layer_out(i) * kIn * 2;
+    return o;
+}
+constexpr int kTcWBytes = tc_w_offset(kLayers);   // 38,912
+constexpr int kTcSmem = kTcWBytes + kTcATile + 16;  // + mbarrier + tensor-memory address
+constexpr uint32_t kTcWaitLimit = 1u << 24;
+
+AG_D uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of tcgen05 (no swizzle): start address,
+// leading- and stride-dimension byte offsets (all >> 4), version 1 at bit 46.
+AG_D uint64_t tc_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(kTcLbo >> 4) << 16) | ((uint64_t)(kTcSbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16: fp32 accumulator (bits
+// 4-5 = 1), bf16 A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t tc_idesc(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+AG_D void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+AG_D void tc_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+AG_D bool mbar_try_wait(uint32_t mbar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+AG_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+AG_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive fp32 columns of this thread's tensor-memory lane, waited for.
+AG_D void tc_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];\n\ttcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of (row, k) in a no-swizzle K-major operand tile.
+AG_HD uint32_t tc_offset(uint32_t row, uint32_t k)
+{
+    return (row >> 3) * kTcSbo + (k >> 3) * kTcLbo + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// Threads of the CTA barrier around tensor-core work (the fences order
+// tcgen05 operations against the thread barrier).
+AG_D void tc_sync()
+{
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+__global__ void __launch_bounds__(kTcRows) k_infer_tc(Params g, const Query* __restrict__ q, uint32_t n,
+                                                      const uint32_t* __restrict__ nDev, float* __restrict__ raw,
+                                                      uint32_t* __restrict__ status)
+{
+    if (nDev) n = min(n, *nDev);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* wt = smem;                                 // W_0..W_4, core-matrix layout
+    unsigned char* at = smem + kTcWBytes;                     // activation tile A
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(at + kTcATile);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(at + kTcATile + 8);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+
+    // weights: packed [out][in] bf16 -> core-matrix layout, 16 bytes at a time
+    for (int l = 0; l < kLayers; ++l) {
+        const uint4* src = reinterpret_cast<const uint4*>(g.W + layer_offset(l));
+        const int chunks = layer_out(l) * (kIn / 8);
+        for (int i = tid; i < chunks; i += kTcRows) {
+            const uint32_t row = (uint32_t)(i / (kIn / 8)), c = (uint32_t)(i % (kIn / 8));
+            *reinterpret_cast<uint4*>(wt + tc_w_offset(l) + tc_offset(row, 8 * c)) = src[i];
+        }
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t mb = smem_addr(mbar);
+    const uint32_t aBase = smem_addr(at), wBase = smem_addr(wt);
+    const uint32_t myLane = tmem + ((warp * 32u) << 16);      // this warp's 32 lanes
+    uint32_t phase = 0;
+    bool failed = false;
+    const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
+    for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
+        const uint32_t i = tile * kTcRows + tid;
+        {
+            __align__(16) __nv_bfloat16 row[kIn];
+            if (i < n) {
+                encode_row(g, q[i], row);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kIn; ++k) row[k] = bf(0.0f);
+            }
+#pragma unroll
+            for (int c = 0; c < kIn / 8; ++c)
+                *reinterpret_cast<uint4*>(at + tc_offset(tid, 8 * c)) = *reinterpret_cast<const uint4*>(row + 8 * c);
+        }
+        for (int l = 0; l < kLayers && !failed; ++l) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A visible to the tensor cores
+            tc_sync();
+            const int nOut = layer_out(l);
+            if (tid == 0) {
+                const uint32_t idesc = tc_idesc(kTcRows, nOut);
+#pragma unroll
+                for (int ks = 0; ks < kIn / 16; ++ks)
+                    tc_mma(tmem, tc_desc(aBase + ks * 2 * kTcLbo), tc_desc(wBase + tc_w_offset(l) + ks * 2 * kTcLbo),
+                           idesc, ks > 0 ? 1u : 0u);
+                tc_commit(mb);
+            }
+            uint32_t tries = 0;
+            bool late = false;
+            while (!mbar_try_wait(mb, phase))
+                if (++tries >= kTcWaitLimit) {
+                    late = true;
+                    break;
+                }
+            phase ^= 1u;
+            // one decision for the whole CTA: the loads below are warp-collective
+            failed = __syncthreads_or(late) != 0;
+            if (failed) break;
+            tc_fence_after();
+            if (l < kLayers - 1) {
+#pragma unroll
+                for (int c16 = 0; c16 < kHidden / 16; ++c16) {
+                    float v[16];
+                    tc_ld16(myLane + 16u * c16, v);
+                    uint4 lo, hi;
+                    lo.x = pack_bf2(fmaxf(v[0], 0.0f), fmaxf(v[1], 0.0f));
+                    lo.y = pack_bf2(fmaxf(v[2], 0.0f), fmaxf(v[3], 0.0f));
+                    lo.z = pack_bf2(fmaxf(v[4], 0.0f), fmaxf(v[5], 0.0f));
+                    lo.w = pack_bf2(fmaxf(v[6], 0.0f), fmaxf(v[7], 0.0f));
+                    hi.x = pack_bf2(fmaxf(v[8], 0.0f), fmaxf(v[9], 0.0f));
+                    hi.y = pack_bf2(fmaxf(v[10], 0.0f), fmaxf(v[11], 0.0f));
+                    hi.z = pack_bf2(fmaxf(v[12], 0.0f), fmaxf(v[13], 0.0f));
+                    hi.w = pack_bf2(fmaxf(v[14], 0.0f), fmaxf(v[15], 0.0f));
+                    // the MMAs reading A have completed (mbarrier), so A is rewritten in place
+                    *reinterpret_cast<uint4*>(at + tc_offset(tid, 16 * c16)) = lo;
+                    *reinterpret_cast<uint4*>(at + tc_offset(tid, 16 * c16 + 8)) = hi;
+                }
+            } else {
+#pragma unroll
+                for (int c16 = 0; c16 < 3; ++c16) {  // columns 0..47; 0..39 are the mixture
+                    float v[16];
+                    tc_ld16(myLane + 16u * c16, v);
+                    if (i < n)
+#pragma unroll
+                        for (int k = 0; k < 16; k += 4)
+                            if (16 * c16 + k < 40)
+                                *reinterpret_cast<float4*>(raw + (uint64_t)i * 40 + 16 * c16 + k) =
+                                    make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+                }
+            }
+        }
+        tc_sync();  // tensor memory read by every warp before the next tile's MMAs
+    }
+    if (failed && status) atomicOr(status, kErrTensorWait);
+    tc_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+}
+
 // Training: forward with saved activations, mixture gradient, backward with
 // tensor cores. dW is accumulated per block in shared memory and written to
 // the block's slice of `partial` (reduced by k_reduce_dw); grid gradients
@@ -512,11 +739,26 @@ Params Guide::params() const
     return p;
 }
 
-void Guide::infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const { infer_queue(q, nullptr, n, raw, st); }
+void Guide::infer(const Query* q, uint32_t n, float* raw, cudaStream_t st, uint32_t* status) const
+{
+    infer_queue(q, nullptr, n, raw, st, status);
+}
 
-void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st) const
+void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st,
+                        uint32_t* status) const
 {
     if (maxN == 0) return;
+    if (kernel_ == kKernelTensorMemory) {
+        cudaFuncSetAttribute(k_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        uint32_t tiles = (maxN + kTcRows - 1) / kTcRows;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // four CTAs per SM: 4 x 55 KB of shared memory, 4 x 64 of the 512 tensor-memory columns
+        const uint32_t blocks = std::min<uint32_t>(tiles, 4u * (uint32_t)sms);
+        k_infer_tc<<<blocks, kTcRows, kTcSmem, st>>>(params(), q, maxN, count, raw, status);
+        return;
+    }
     // per call: the attribute belongs to the current device
     cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
     uint32_t chunks = (maxN + 31) / 32;

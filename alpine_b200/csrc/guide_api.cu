@@ -99,12 +99,22 @@ int alpine_gpu_guide_infer(alpine_gpu_ctx* c, const float* queries, uint32_t n, 
         return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide_infer buffers");
     cudaError_t e = cudaMemcpyAsync(dq.ptr, queries, (size_t)n * sizeof(G::Query), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
-        c->guide.infer(dq.as<G::Query>(), n, dr.as<float>(), c->stream);
+        c->guide.infer(dq.as<G::Query>(), n, dr.as<float>(), c->stream, c->dStatus);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(raw, dr.ptr, (size_t)n * 40 * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("guide_infer: ") + cudaGetErrorString(e));
+    return c->check_device_status();
+}
+
+int alpine_gpu_guide_set_kernel(alpine_gpu_ctx* c, int kernel)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (kernel != ALPINE_GPU_GUIDE_KERNEL_WARP_MMA && kernel != ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "guide_set_kernel: unknown kernel");
+    c->guide.set_kernel(kernel == ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY ? G::Guide::kKernelTensorMemory
+                                                                       : G::Guide::kKernelWarpMma);
     return ALPINE_GPU_OK;
 }
 

@@ -19,9 +19,16 @@ public:
     void set_scene_box(float3 lo, float3 hi);
     Params params() const;
     // raw: n x 40 fp32 mixture parameters.
-    void infer(const Query* q, uint32_t n, float* raw, cudaStream_t st) const;
+    // status (optional): device word that receives kErrTensorWait bits.
+    void infer(const Query* q, uint32_t n, float* raw, cudaStream_t st, uint32_t* status = nullptr) const;
     // The same for a queue whose length (at most maxN) is in device memory.
-    void infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st) const;
+    void infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st,
+                     uint32_t* status = nullptr) const;
+    // Inference kernel: warp-level mma.sync tiles of 32 queries, or tcgen05
+    // MMAs with tensor-memory accumulators on tiles of 128 queries.
+    static constexpr int kKernelWarpMma = 0, kKernelTensorMemory = 1;
+    void set_kernel(int k) { kernel_ = k; }
+    int kernel() const { return kernel_; }
     // Adds the gradient of the batch s[offset + i * stride], i < n (mean
     // loss, scaled by invBatch) to the gradient buffers, without an update.
     void accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset = 0,
@@ -50,6 +57,7 @@ private:
 
     void* mem_ = nullptr;
     bool ready_ = false;
+    int kernel_ = kKernelWarpMma;
     uint32_t step_ = 0;
     float* gridP_ = nullptr;
     float* gridM_ = nullptr;

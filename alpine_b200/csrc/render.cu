@@ -813,7 +813,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
                 if (guiding) {
                     cudaMemsetAsync(w.guideCount, 0, sizeof(uint32_t), st);
                     K.guide_query(sc, w, w.numPaths, st);
-                    if (sampleGuide) c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.raw, st);
+                    if (sampleGuide) c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.raw, st, c->dStatus);
                 }
                 K.shade(sc, w, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,

@@ -26,6 +26,8 @@ RAY_DTYPE = np.dtype([("org", np.float32, 3), ("tmin", np.float32), ("dir", np.f
 HIT_DTYPE = np.dtype([("prim", np.uint32), ("t", np.float32), ("b1", np.float32), ("b2", np.float32)])
 MISS = 0xFFFFFFFF
 NOALLOC_MAX_RAYS = 65536
+GUIDE_KERNEL_WARP_MMA = 0
+GUIDE_KERNEL_TENSOR_MEMORY = 1
 
 
 class GpuError(RuntimeError):
@@ -128,6 +130,7 @@ def lib():
         L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
         L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p, C.POINTER(C.c_float)]
+        L.alpine_gpu_guide_set_kernel.argtypes = [vp, C.c_int]
         L.alpine_gpu_guide_gradients.argtypes = [vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_guide_train.argtypes = [vp, vp, C.c_uint32, C.c_float, f3]
         L.alpine_gpu_guide_get_weights.argtypes = [vp, vp]
@@ -413,6 +416,10 @@ class Context:
         a, b, l = C.c_uint32(), C.c_uint32(), C.c_float()
         self._check(self.L.alpine_gpu_guide_steps(self.h, C.byref(a), C.byref(b), C.byref(l)))
         return (a.value, b.value, l.value) if with_loss else (a.value, b.value)
+
+    def guide_set_kernel(self, kernel):
+        """GUIDE_KERNEL_WARP_MMA (mma.sync) or GUIDE_KERNEL_TENSOR_MEMORY (tcgen05)."""
+        self._check(self.L.alpine_gpu_guide_set_kernel(self.h, kernel))
 
     def guide_infer(self, queries):
         q = np.ascontiguousarray(queries, np.float32).reshape(-1, 12)

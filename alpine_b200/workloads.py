@@ -6,6 +6,7 @@ first render's launches.
                                              # power sampler, quad ceiling light (the small room)
     python -m alpine_b200.workloads guided   # glossy interior 320x180, depth 12, guided:
                                              # 16 Adam steps, then 2 x 32 spp
+    python -m alpine_b200.workloads guided_tc  # the same with the tcgen05 inference kernel
     python -m alpine_b200.workloads city     # many-light city 960x540, 1 + 2 spp, depth 8, light BVH
 """
 from __future__ import annotations
@@ -21,7 +22,7 @@ def run(mode: str, device: int = 0) -> float:
     if mode == "room":
         sc, (W, H), depth = scenes.room_scene(light="quad"), (256, 256), 8
         opts, sampler, spp = dict(russian_roulette_depth=3), gpu.SAMPLER_POWER, (16, 16)
-    elif mode == "guided":
+    elif mode in ("guided", "guided_tc"):
         sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
         opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
                     guide_min_roughness=0.2, guide_train_steps=16)
@@ -32,6 +33,8 @@ def run(mode: str, device: int = 0) -> float:
     else:
         raise ValueError(f"unknown workload {mode!r}")
     c = gpu.Context(device, W, H, depth)
+    if mode == "guided_tc":
+        c.guide_set_kernel(gpu.GUIDE_KERNEL_TENSOR_MEMORY)
     scenes.load_scene(c, sc, W, H)
     if sampler is not None:
         c.build_light_sampler(sampler)

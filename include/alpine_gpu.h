@@ -373,6 +373,15 @@ ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_
 ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],
                                           const float scene_hi[3]);
 ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw);
+/* Inference kernel of the guide (rendering and alpine_gpu_guide_infer):
+ * WARP_MMA (default): each warp runs 32 queries through the MLP with
+ *   warp-level mma.sync tiles; TENSOR_MEMORY: tiles of 128 queries run
+ *   through tcgen05 MMAs with the accumulators in tensor memory (sm_100a).
+ * Both compute the same BF16 x BF16 -> FP32 products; sums may differ in the
+ * last bits (accumulation order). */
+#define ALPINE_GPU_GUIDE_KERNEL_WARP_MMA 0
+#define ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY 1
+ALPINE_GPU_API int alpine_gpu_guide_set_kernel(alpine_gpu_ctx* ctx, int kernel);
 /* Adam steps taken since the last reset, waves rendered with guiding, and the
  * mean training loss (KL divergence up to a constant) of the last trained
  * wave's steps (0 before any). Any pointer may be NULL. */

@@ -65,6 +65,32 @@ def test_inference_matches_oracle(ctx):
     assert err < 2e-2
 
 
+@pytest.mark.parametrize("n", [1000, 128, 1, 70000])
+def test_tensor_memory_inference_matches(ctx, n):
+    """The tcgen05 kernel (tiles of 128 queries, accumulators in tensor
+    memory) against the BF16-emulating FP64 oracle and against the warp-MMA
+    kernel, for partial, single and many-tile batches."""
+    q = _queries(n, 11)
+    w, res, lookup = _randomise(ctx, q, 12)
+    ctx.guide_set_kernel(gpu.GUIDE_KERNEL_WARP_MMA)
+    warp = ctx.guide_infer(q)
+    ctx.guide_set_kernel(gpu.GUIDE_KERNEL_TENSOR_MEMORY)
+    try:
+        tc = ctx.guide_infer(q)
+        tc2 = ctx.guide_infer(q)
+    finally:
+        ctx.guide_set_kernel(gpu.GUIDE_KERNEL_WARP_MMA)
+    assert np.array_equal(tc, tc2)  # deterministic
+    m = min(n, 1000)
+    X = G.encode(q[:m], LO, HI, res, lookup, half=True)
+    ref, _ = G.forward(X, G.unpack(w), emulate_bf16=True)
+    err = np.linalg.norm(tc[:m] - ref[:, :40]) / np.linalg.norm(ref[:, :40])
+    diff = np.linalg.norm(tc - warp) / np.linalg.norm(warp)
+    print(f"n={n}: tcgen05 vs oracle {err:.2e}, vs warp MMA {diff:.2e}")
+    assert err < 2e-2
+    assert diff < 1e-2
+
+
 def test_gradients_match_oracle(ctx):
     q = _queries(2048, 3)
     w, res, lookup = _randomise(ctx, q, 4)
