@@ -111,10 +111,9 @@ int alpine_gpu_guide_infer(alpine_gpu_ctx* c, const float* queries, uint32_t n, 
 int alpine_gpu_guide_set_kernel(alpine_gpu_ctx* c, int kernel)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
-    if (kernel != ALPINE_GPU_GUIDE_KERNEL_WARP_MMA && kernel != ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY)
-        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "guide_set_kernel: unknown kernel");
-    c->guide.set_kernel(kernel == ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY ? G::Guide::kKernelTensorMemory
-                                                                       : G::Guide::kKernelWarpMma);
+    if (kernel == ALPINE_GPU_GUIDE_KERNEL_WARP_MMA) c->guide.set_kernel(G::Guide::kKernelWarpMma);
+    else if (kernel == ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY) c->guide.set_kernel(G::Guide::kKernelTensorMemory);
+    else return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "guide_set_kernel: unknown kernel");
     return ALPINE_GPU_OK;
 }
 

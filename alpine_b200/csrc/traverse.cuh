@@ -196,6 +196,8 @@ template <bool kAny>
 AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, uint32_t& err, uint32_t& nodeVisits,
                    uint32_t& triVisits)
 {
+    // all pending triangles before the next node (measured on B200: testing
+    // at most 1, 2 or 4 per step is 25-30 % slower)
     while (s.tgroup.y != 0u) {
         uint32_t k = __ffs(s.tgroup.y) - 1u;
         s.tgroup.y &= s.tgroup.y - 1u;
