@@ -26,6 +26,7 @@ in [0.02, 0.4], sky of radiance 5 through two 1 x 2 m window openings, depth
 relMSE = mean over pixels and channels of (x - r)^2 / (r^2 + 0.01 mean(r)^2).
 Time is the wall time of the render calls (synchronous), guided training
 included; both curves are sampled at doubling spp and interpolated in log-log.
+Each arm runs twice and keeps its faster time (both are reported).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one process per GPU under torchrun; each rank is an independent
@@ -254,8 +255,18 @@ def guiding_benchmark(device, ref_spp, target=0.01):
     warm = context(seed=5, **GUIDE_OPTIONS)  # module loading, allocations
     warm.render(4)
     warm.close()
-    plain_at, plain_pts, _ = curve(dict(seed=1))
-    guided_at, guided_pts, steps = curve(dict(seed=2, **GUIDE_OPTIONS))
+
+    def best_of(opts, repeats):
+        """Each curve twice (same seed): a host or device stall of the shared
+        machine inside one measurement does not decide the result; the
+        faster time to the target is kept and every repeat is reported."""
+        runs = [curve(opts) for _ in range(repeats)]
+        timed = [r for r in runs if r[0] is not None]
+        best = min(timed, key=lambda r: r[0][0]) if timed else runs[0]
+        return best, [r[0][0] if r[0] else None for r in runs]
+
+    (plain_at, plain_pts, _), plain_all = best_of(dict(seed=1), 2)
+    (guided_at, guided_pts, steps), guided_all = best_of(dict(seed=2, **GUIDE_OPTIONS), 2)
     out = {
         "metric": "time to relMSE 0.01, guided vs plain MIS", "unit": "s", "target_relmse": target,
         "scene": "glossy interior, 2.0M triangles, sky 5 through two 1x2 m windows, depth 12, no lights",
@@ -265,6 +276,7 @@ def guiding_benchmark(device, ref_spp, target=0.01):
         "plain_s": plain_at[0] if plain_at else None, "plain_spp": plain_at[1] if plain_at else None,
         "guided_s": guided_at[0] if guided_at else None, "guided_spp": guided_at[1] if guided_at else None,
         "speedup": (plain_at[0] / guided_at[0]) if plain_at and guided_at else None,
+        "repeats_s": {"plain": plain_all, "guided": guided_all},
         "guide": {k: v for k, v in GUIDE_OPTIONS.items() if k != "guide"} | {"adam_steps": steps},
         "plain_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in plain_pts],
         "guided_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in guided_pts],
