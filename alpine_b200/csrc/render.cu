@@ -810,12 +810,18 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
                                      c->traceBlock);
                 cudaMemsetAsync(w.queueCountNext, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(w.shadowCount, 0, sizeof(uint32_t), st);
-                if (guiding) {
+                const bool guideHere = guiding && (o.guide_max_depth == 0 || depth < o.guide_max_depth);
+                if (guideHere) {
                     cudaMemsetAsync(w.guideCount, 0, sizeof(uint32_t), st);
                     K.guide_query(sc, w, w.numPaths, st);
                     if (sampleGuide) c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.raw, st, c->dStatus);
+                    K.shade(sc, w, stream, w.numPaths, st);
+                } else {
+                    ag::WaveView plain = w;  // unguided shading (pending training records still resolve)
+                    plain.guideQuery = nullptr;
+                    plain.guideRaw = nullptr;
+                    K.shade(sc, plain, stream, w.numPaths, st);
                 }
-                K.shade(sc, w, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,
                                      c->dStatus, st, c->traceBlock);
                 K.resolve(w, w.numPaths, st);

@@ -55,7 +55,8 @@ class RenderOptions(C.Structure):
                 ("guide_fraction", C.c_float), ("guide_train", C.c_uint32), ("guide_batch", C.c_uint32),
                 ("guide_lr", C.c_float), ("guide_warmup_steps", C.c_uint32), ("guide_spp_per_wave", C.c_uint32),
                 ("guide_steps_per_wave", C.c_uint32), ("guide_min_roughness", C.c_float),
-                ("guide_train_steps", C.c_uint32), ("cuda_graph", C.c_uint32)]
+                ("guide_train_steps", C.c_uint32), ("cuda_graph", C.c_uint32),
+                ("guide_max_depth", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -346,13 +347,14 @@ class Context:
     def set_render_options(self, sampler=RNG_COUNTER, max_paths_per_wave=0, russian_roulette_depth=0, seed=0,
                            accumulate_fp64=False, guide=False, guide_fraction=0.5, guide_train=True,
                            guide_batch=16384, guide_lr=1e-2, guide_warmup_steps=0, guide_spp_per_wave=1,
-                           guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0, cuda_graph=False):
+                           guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0, cuda_graph=False,
+                           guide_max_depth=0):
         """Options of alpine_gpu_render_options; the guide_* fields apply when
         guide is set (learned path guiding, counter sampler only)."""
         o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64),
                           int(guide), guide_fraction, int(guide_train), guide_batch, guide_lr, guide_warmup_steps,
                           guide_spp_per_wave, guide_steps_per_wave, guide_min_roughness, guide_train_steps,
-                          int(cuda_graph))
+                          int(cuda_graph), guide_max_depth)
         self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
 
     def reset_accumulation(self):

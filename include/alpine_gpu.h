@@ -295,7 +295,10 @@ ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3]
  * cuda_graph: 1 = capture the whole wave loop of an unguided render as a CUDA
  *   graph and replay it while the launch configuration (spp, sizes, device
  *   buffers, camera, lights, options) stays the same; a rebuilt BVH of the
- *   same scene replays the same graph. Results are identical either way. */
+ *   same scene replays the same graph. Results are identical either way.
+ * guide_max_depth: vertices at this depth and deeper use the material's
+ *   procedure only and are not recorded (their throughput is small, their
+ *   inference costs the same); 0 = guide every depth. */
 #define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
 #define ALPINE_GPU_SAMPLER_COUNTER 1u
 typedef struct alpine_gpu_render_options {
@@ -315,6 +318,7 @@ typedef struct alpine_gpu_render_options {
     float guide_min_roughness;
     uint32_t guide_train_steps;
     uint32_t cuda_graph;
+    uint32_t guide_max_depth;
 } alpine_gpu_render_options;
 ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
 
