@@ -432,9 +432,9 @@ def run_ours(args):
 
     from alpine_b200 import gpu, scenes
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from alpine_b200 import replicas
+
+    world, rank, local = replicas.world_info()
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -451,11 +451,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, "cuda")
 
     verts, idx, closest, shadow = scenes.traversal_workload()
     n = closest.shape[0]
@@ -510,10 +506,10 @@ def run_ours(args):
     ctx.synchronize()
     barrier()
     total_ms = start.elapsed_time(end)
-    ms_step = max_over_ranks(total_ms / args.steps)
+    value, ms_step = replicas.job_rate(2 * n, total_ms / args.steps, world, dist, "cuda")
     closest_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
     any_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
-    value = world * 2 * n / (ms_step / 1e3) / 1e6
+    value /= 1e6  # Mrays/s
 
     if args.profile:
         if rank == 0:
@@ -533,9 +529,9 @@ def run_ours(args):
     for _ in range(args.steps):
         ctx.trace(h_closest, h_hits)
         ctx.occluded(h_shadow, h_occ)
-    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - t0) / args.steps)
+    e2e_value, e2e_ms = replicas.job_rate(2 * n, 1e3 * (time.perf_counter() - t0) / args.steps, world, dist, "cuda")
     barrier()
-    e2e_value = world * 2 * n / (e2e_ms / 1e3) / 1e6
+    e2e_value /= 1e6
 
     peak, peak_kind = peaks()
     bytes_closest = n * (RAY_BYTES + HIT_BYTES) + nv_c * NODE_BYTES + tv_c * TRI_BYTES
