@@ -13,6 +13,10 @@ shadow rays with tmax uniform in (0, 1]. A step traces all 8,388,608 queries.
 the C ABI with pinned host buffers (host->device copy of the rays and
 device->host copy of the results inside the timed region).
 
+`room` (rank 0, one GPU): the small procedural room of the reference's own
+CPU-runnable configuration, GPU samples/s next to the reference renderer's
+on the host cores.
+
 `many_lights` (rank 0, one GPU): the many-light city, samples/s and relMSE
 per light sampler (uniform, power, light BVH).
 
@@ -69,6 +73,7 @@ def parse_args():
     p.add_argument("--batch-frames", type=int, default=2,
                    help="frames of the 48-scene animated batch to time (0 = skip)")
     p.add_argument("--no-many-lights", action="store_true", help="skip the many-light city measurement")
+    p.add_argument("--no-room", action="store_true", help="skip the small-room render measurement")
     p.add_argument("--profile", action="store_true",
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     return p.parse_args()
@@ -332,6 +337,58 @@ def batch_benchmark(device, frames):
     return r
 
 
+def room_benchmark(device, W=256, H=256, spp=16, depth=8, repeats=5):
+    """The small procedural room (4,036 triangles, 0.5 x
+    0.5 quad ceiling light of radiance 15, power sampler, depth 8, 256 x 256,
+    16 spp) rendered by the GPU and by the reference's own renderer
+    (oracle/_ref: class Alpine with its binary BVH) on all host cores. Both
+    run the reference's estimator (no Russian roulette); the GPU is also
+    timed with roulette from depth 3 as configs[0] asks. Samples per second;
+    the GPU's best of `repeats` renders; the image means are compared."""
+    from alpine_b200 import gpu, scenes
+    import oracle
+
+    scene = scenes.room_scene(light="quad")
+    out = {"workload": f"room, {W}x{H}, {spp} spp, depth {depth}, power sampler, quad light", "gpu": {}}
+
+    def gpu_rate(rr):
+        c = gpu.Context(device, W, H, depth)
+        scenes.load_scene(c, scene, W, H)
+        c.build_light_sampler(gpu.SAMPLER_POWER)
+        c.set_render_options(sampler=gpu.RNG_COUNTER, russian_roulette_depth=rr, seed=3)
+        c.reset_accumulation()
+        c.render(spp)
+        best = float("inf")
+        for _ in range(repeats):
+            c.reset_accumulation()
+            t0 = time.perf_counter()
+            c.render(spp)
+            best = min(best, time.perf_counter() - t0)
+        a, n = c.read_accumulation(W, H)
+        c.close()
+        return W * H * spp / best, float(a[..., :3].mean() / n)
+
+    rate, gmean = gpu_rate(0)
+    out["gpu"]["samples_per_s"] = rate
+    out["gpu"]["samples_per_s_rr3"] = gpu_rate(3)[0]
+    if oracle.ref_available():
+        r = oracle.RefRenderer(W, H, depth, accelerator=oracle.RefRenderer.ACC_BVH)
+        scenes.load_scene(r, scene, W, H)
+        r.build_light_sampler(gpu.SAMPLER_POWER)
+        r.reset_accumulation()
+        t0 = time.perf_counter()
+        r.render(spp)
+        dt = time.perf_counter() - t0
+        a, n = r.read_accumulation()
+        r.close()
+        rmean = float(a[..., :3].mean() / n)
+        out["cpu_reference"] = {"samples_per_s": W * H * spp / dt, "cores": os.cpu_count() or 1, "kind": "reference",
+                                "sample": f"one render of {spp} spp (binary BVH, quad light as a harness Light)"}
+        out["speedup_vs_cpu_reference"] = rate / out["cpu_reference"]["samples_per_s"]
+        out["image_mean"] = {"gpu": gmean, "reference": rmean, "rel_diff": abs(gmean - rmean) / rmean}
+    return out
+
+
 def many_lights_benchmark(device, spp=4, cmp_res=(480, 270), cmp_spp=64, ref_spp=4096):
     """Many-light city (BASELINE cfg3 shapes; alpine_b200.scenes.city_scene:
     2,000 buildings, ~1.2M triangles, 131,072 window quad lights): samples/s
@@ -549,10 +606,13 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
-    guiding = batched = many = None
-    if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames or not args.no_many_lights):
+    guiding = batched = many = room = None
+    if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames or not args.no_many_lights
+                                     or not args.no_room):
         ctx.close()
         ctx = None
+    if rank == 0 and world == 1 and not args.no_room:
+        room = room_benchmark(local)
     if rank == 0 and world == 1 and not args.no_many_lights:
         many = many_lights_benchmark(local)
     if rank == 0 and world == 1 and not args.no_guiding:
@@ -581,6 +641,7 @@ def run_ours(args):
             "guiding": guiding,
             "batch": batched,
             "many_lights": many,
+            "room": room,
         }
         print(json.dumps(line), flush=True)
     if ctx is not None:
