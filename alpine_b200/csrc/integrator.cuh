@@ -362,8 +362,19 @@ __global__ void __launch_bounds__(kThreads) k_guide_query(SceneView sc, WaveView
 }
 
 // kSampler: the light sampler kind, or -1 to read it from the scene.
+// Resident blocks per SM: the shading kernel waits on instruction fetch and
+// memory, so more warps beat fewer spills (measured on B200: 14 blocks of
+// 128, 32 registers with spills to L1, +28-41 % samples/s over 6 blocks for
+// unguided shading; the guided kernel, with more live state, is best at 10).
+#ifndef AG_SHADE_MIN_BLOCKS
+#define AG_SHADE_MIN_BLOCKS 14
+#endif
+#ifndef AG_SHADE_MIN_BLOCKS_GUIDED
+#define AG_SHADE_MIN_BLOCKS_GUIDED 10
+#endif
 template <bool kGuided, int kSampler>
-__global__ void __launch_bounds__(kThreads) k_shade(SceneView sc, WaveView w, bool streamRng)
+__global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED : AG_SHADE_MIN_BLOCKS)
+    k_shade(SceneView sc, WaveView w, bool streamRng)
 {
     const uint32_t n = *w.queueCount;
     uint32_t q = blockIdx.x * kThreads + threadIdx.x;
