@@ -41,7 +41,7 @@ struct DeviceBuffer {
     T* as() const { return static_cast<T*>(ptr); }
 };
 
-constexpr int kCopyStreams = 4;
+constexpr int kCopyStreams = 8;  // host-query pipeline streams
 
 int upload_render_scene(alpine_gpu_ctx* c);  // render.cu: materials, attributes, lights to the device
 int upload_geometry(alpine_gpu_ctx* c);      // api.cu: vertices and indices to the device
