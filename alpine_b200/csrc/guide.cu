@@ -142,10 +142,54 @@ AG_D void hidden_layers(const __nv_bfloat16* W, __nv_bfloat16* X, __nv_bfloat16*
     }
 }
 
-// n queries, or *nDev when nDev is not null (a queue length written on the device).
-__global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Query* __restrict__ q, uint32_t n,
-                                                          const uint32_t* __restrict__ nDev, float* __restrict__ raw)
+// Packs the output tile of one warp's 32 queries (acc, the mma fragments of
+// the output layer) into decoded mixtures, 16 rows at a time: the rows are
+// staged as fp32 in the warp's activation tile (free after the output
+// layer), then two lanes per row decode 4 lobes each.
+AG_D void pack_tile(const float (&acc)[2][kOut / 8][4], __nv_bfloat16* X, uint32_t row0, uint32_t n, float* out,
+                   uint32_t stride)
 {
+    const int lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+    float* S = reinterpret_cast<float*>(X);  // 16 x 40 floats: 2,560 of the tile's 4,608 bytes
+    static_assert(16 * 40 * 4 <= 32 * kLd * 2, "staging fits the activation tile");
+    const int row = lane >> 1, part = lane & 1;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        __syncwarp();  // every lane is done with X (output layer, or the previous half)
+#pragma unroll
+        for (int nt = 0; nt < 5; ++nt) {
+            const int col = nt * 8 + 2 * t4;
+            *reinterpret_cast<float2*>(S + g4 * 40 + col) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
+            *reinterpret_cast<float2*>(S + (g4 + 8) * 40 + col) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
+        }
+        __syncwarp();
+        const float* r = S + row * 40 + part * 4 * kRawPerLobe;
+        float mx = -3.4e38f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mx = fmaxf(mx, r[k * kRawPerLobe + 4]);
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sum += expf(r[k * kRawPerLobe + 4] - mx);
+        sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+        const float invSum = 1.0f / sum;
+        const uint32_t gr = row0 + mt * 16 + row;
+        if (gr < n)
+#pragma unroll 1
+            for (int k = 0; k < 4; ++k) pack_lobe(r + k * kRawPerLobe, mx, invSum, part * 4 + k, out + gr, stride);
+    }
+    __syncwarp();
+}
+
+// n queries, or *nDev when nDev is not null (a queue length written on the
+// device). Writes the 40 raw outputs per query, or with `packed` the decoded
+// mixtures as kPacked field arrays of n floats each (field f of query i at
+// raw[f * n + i]).
+__global__ void __launch_bounds__(32 * kInferWarps, 2) k_infer(Params g, const Query* __restrict__ q, uint32_t n,
+                                                          const uint32_t* __restrict__ nDev, float* __restrict__ raw,
+                                                          bool packed)
+{
+    const uint32_t nMax = n;
     if (nDev) n = min(n, *nDev);
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -165,6 +209,10 @@ __global__ void __launch_bounds__(32 * kInferWarps) k_infer(Params g, const Quer
         hidden_layers(W, X, nullptr);
         float acc[2][kOut / 8][4];
         warp_layer<kOut, kHidden>(X, W + wsm_offset(kLayers - 1), wld(kLayers - 1), acc);
+        if (packed) {
+            pack_tile(acc, X, ch * 32, n, raw, nMax);
+            continue;
+        }
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -287,10 +335,11 @@ AG_D void tc_sync()
     tc_fence_after();
 }
 
-__global__ void __launch_bounds__(kTcRows) k_infer_tc(Params g, const Query* __restrict__ q, uint32_t n,
+__global__ void __launch_bounds__(kTcRows, 4) k_infer_tc(Params g, const Query* __restrict__ q, uint32_t n,
                                                       const uint32_t* __restrict__ nDev, float* __restrict__ raw,
-                                                      uint32_t* __restrict__ status)
+                                                      uint32_t* __restrict__ status, bool packed)
 {
+    const uint32_t nMax = n;
     if (nDev) n = min(n, *nDev);
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* wt = smem;                                 // W_0..W_4, core-matrix layout
@@ -384,16 +433,23 @@ __global__ void __launch_bounds__(kTcRows) k_infer_tc(Params g, const Query* __r
                     *reinterpret_cast<uint4*>(at + tc_offset(tid, 16 * c16 + 8)) = hi;
                 }
             } else {
+                float r[48];  // columns 0..47; 0..39 are the mixture
 #pragma unroll
-                for (int c16 = 0; c16 < 3; ++c16) {  // columns 0..47; 0..39 are the mixture
+                for (int c16 = 0; c16 < 3; ++c16) {
                     float v[16];
                     tc_ld16(myLane + 16u * c16, v);
-                    if (i < n)
 #pragma unroll
-                        for (int k = 0; k < 16; k += 4)
-                            if (16 * c16 + k < 40)
-                                *reinterpret_cast<float4*>(raw + (uint64_t)i * 40 + 16 * c16 + k) =
-                                    make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+                    for (int k = 0; k < 16; ++k) r[16 * c16 + k] = v[k];
+                }
+                if (i < n) {
+                    if (packed) {
+                        pack_mixture(r, raw + i, nMax);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 40; k += 4)
+                            *reinterpret_cast<float4*>(raw + (uint64_t)i * 40 + k) =
+                                make_float4(r[k], r[k + 1], r[k + 2], r[k + 3]);
+                    }
                 }
             }
         }
@@ -744,8 +800,8 @@ void Guide::infer(const Query* q, uint32_t n, float* raw, cudaStream_t st, uint3
     infer_queue(q, nullptr, n, raw, st, status);
 }
 
-void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st,
-                        uint32_t* status) const
+void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* out, cudaStream_t st,
+                        uint32_t* status, bool packed) const
 {
     if (maxN == 0) return;
     if (kernel_ == kKernelTensorMemory) {
@@ -756,7 +812,7 @@ void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, fl
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         // four CTAs per SM: 4 x 55 KB of shared memory, 4 x 64 of the 512 tensor-memory columns
         const uint32_t blocks = std::min<uint32_t>(tiles, 4u * (uint32_t)sms);
-        k_infer_tc<<<blocks, kTcRows, kTcSmem, st>>>(params(), q, maxN, count, raw, status);
+        k_infer_tc<<<blocks, kTcRows, kTcSmem, st>>>(params(), q, maxN, count, out, status, packed);
         return;
     }
     // per call: the attribute belongs to the current device
@@ -764,7 +820,7 @@ void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, fl
     uint32_t chunks = (maxN + 31) / 32;
     uint32_t blocks = (chunks + kInferWarps - 1) / kInferWarps;
     if (blocks > 148 * 2) blocks = 148 * 2;  // two resident blocks per SM; each loads the weights once
-    k_infer<<<blocks, 32 * kInferWarps, infer_smem(), st>>>(params(), q, maxN, count, raw);
+    k_infer<<<blocks, 32 * kInferWarps, infer_smem(), st>>>(params(), q, maxN, count, out, packed);
 }
 
 void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset,

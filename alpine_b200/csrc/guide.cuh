@@ -161,37 +161,83 @@ AG_HD float mixture_pdf(const Mixture& m, float3 w)
     return p;
 }
 
-AG_HD float3 mixture_sample(const Mixture& m, float u0, float u1, float u2)
+// The decoded mixture as the shading kernel reads it: 48 fields per vertex,
+// lambda[8] (selection probabilities), c[8] (density constants lambda kappa /
+// (2 pi (1 - exp(-2 kappa)))), kappa[8], mu.x[8], mu.y[8], mu.z[8] (unit
+// mean directions, world space). Field f of a vertex is at L[f * stride]:
+// the render keeps the fields of a wave's vertices in separate arrays
+// (stride = the wave's capacity), so the loads of a warp's consecutive
+// vertices coalesce. Sampling and the density read the mixture lobe by
+// lobe; a thread never holds all of it. Offsets are 32-bit: a wave holds
+// fewer than 2^32 / kPacked vertices.
+constexpr int kPacked = 48;
+constexpr int kPackLambda = 0, kPackC = 8, kPackKappa = 16, kPackMu = 24;
+
+// Lobe k from its 5 raw outputs r, given the largest logit mx and 1 / the
+// sum of exp(logit - mx) over the lobes (the softmax of decode_mixture).
+AG_HD void pack_lobe(const float* r, float mx, float invSum, int k, float* out, uint32_t stride)
 {
-    // lobe: the first k with u0 < lambda_0 + ... + lambda_k (the last one if
-    // rounding leaves u0 above the total), selected without dynamic indexing
+    const float3 d = mk3(r[0], r[1], r[2]);
+    const float l = sqrtf(dot(d, d));
+    const float3 mu = l > 1e-12f ? d / l : mk3(0.0f, 0.0f, 1.0f);
+    const float kappa = expf(fminf(fmaxf(r[3], kLogKappaMin), kLogKappaMax));
+    const float lambda = expf(r[4] - mx) * invSum;
+    out[(kPackLambda + k) * stride] = lambda;
+    out[(kPackC + k) * stride] = lambda * kappa / (2.0f * kPi * (-expm1f(-2.0f * kappa)));
+    out[(kPackKappa + k) * stride] = kappa;
+    out[(kPackMu + k) * stride] = mu.x;
+    out[(kPackMu + 8 + k) * stride] = mu.y;
+    out[(kPackMu + 16 + k) * stride] = mu.z;
+}
+
+// All 8 lobes of one vertex's 40 raw outputs.
+AG_HD void pack_mixture(const float raw[40], float* out, uint32_t stride)
+{
+    float mx = -3.4e38f;
+    for (int k = 0; k < kLobes; ++k) mx = fmaxf(mx, raw[k * kRawPerLobe + 4]);
+    float sum = 0.0f;
+    for (int k = 0; k < kLobes; ++k) sum += expf(raw[k * kRawPerLobe + 4] - mx);
+    const float invSum = 1.0f / sum;
+    for (int k = 0; k < kLobes; ++k) pack_lobe(raw + k * kRawPerLobe, mx, invSum, k, out, stride);
+}
+
+// A direction from a packed mixture: the first lobe k with u0 < lambda_0 +
+// ... + lambda_k (the last one if rounding leaves u0 above the total), then
+// cos(theta) about its mean by inverting the vMF CDF (Jakob 2012).
+AG_HD float3 lobes_sample(const float* L, uint32_t stride, float u0, float u1, float u2)
+{
     int k = kLobes - 1;
     float c = 0.0f;
-    bool found = false;
-#pragma unroll
-    for (int j = 0; j < kLobes; ++j) {
-        c += m.lambda[j];
-        if (!found && u0 < c) {
+    for (int j = 0; j < kLobes - 1; ++j) {
+        c += L[(kPackLambda + j) * stride];
+        if (u0 < c) {
             k = j;
-            found = true;
+            break;
         }
     }
-    float kappa = m.kappa[0];
-    float3 mu = m.mu[0];
-#pragma unroll
-    for (int j = 1; j < kLobes; ++j)
-        if (k == j) {
-            kappa = m.kappa[j];
-            mu = m.mu[j];
-        }
-    // cos(theta) by inverting the CDF (Jakob 2012)
+    const float kappa = L[(kPackKappa + k) * stride];
+    const float3 mu = mk3(L[(kPackMu + k) * stride], L[(kPackMu + 8 + k) * stride], L[(kPackMu + 16 + k) * stride]);
     float wc = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
     wc = fminf(fmaxf(wc, -1.0f), 1.0f);
-    float st = sqrtf(fmaxf(0.0f, 1.0f - wc * wc));
-    float phi = 2.0f * kPi * u2;
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - wc * wc));
+    const float phi = 2.0f * kPi * u2;
     float3 t1, t2;
     get_basis(mu, t1, t2);
     return t1 * (st * cosf(phi)) + t2 * (st * sinf(phi)) + mu * wc;
+}
+
+// Density of a packed mixture at the unit direction w:
+// sum_k c_k exp(kappa_k (mu_k . w - 1)).
+AG_HD float lobes_pdf(const float* L, uint32_t stride, float3 w)
+{
+    float p = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k) {
+        const float cosMu = L[(kPackMu + k) * stride] * w.x + L[(kPackMu + 8 + k) * stride] * w.y +
+                            L[(kPackMu + 16 + k) * stride] * w.z;
+        p += L[(kPackC + k) * stride] * expf(L[(kPackKappa + k) * stride] * (cosMu - 1.0f));
+    }
+    return p;
 }
 
 // d(-w log q)/d raw for one sample direction w (q = mixture pdf).

@@ -23,15 +23,15 @@ __global__ void k_sample_mixture(const float* raw, const float* u, uint32_t n, f
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float r[40];
+    // the packed form the shading kernel samples
+    float r[40], lobes[G::kPacked];
     for (int k = 0; k < 40; ++k) r[k] = raw[k];
-    G::Mixture m;
-    G::decode_mixture(r, m);
-    float3 d = G::mixture_sample(m, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+    G::pack_mixture(r, lobes, 1);
+    float3 d = G::lobes_sample(lobes, 1, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
     dirs[3 * i] = d.x;
     dirs[3 * i + 1] = d.y;
     dirs[3 * i + 2] = d.z;
-    pdfs[i] = G::mixture_pdf(m, d);
+    pdfs[i] = G::lobes_pdf(lobes, 1, d);
 }
 
 __global__ void k_gather(const float* src, const uint64_t* idx, uint32_t n, float* dst)

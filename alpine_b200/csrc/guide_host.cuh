@@ -21,9 +21,12 @@ public:
     // raw: n x 40 fp32 mixture parameters.
     // status (optional): device word that receives kErrTensorWait bits.
     void infer(const Query* q, uint32_t n, float* raw, cudaStream_t st, uint32_t* status = nullptr) const;
-    // The same for a queue whose length (at most maxN) is in device memory.
-    void infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* raw, cudaStream_t st,
-                     uint32_t* status = nullptr) const;
+    // The same for a queue whose length (at most maxN) is in device memory;
+    // with `packed`, out receives the decoded mixtures that the shading
+    // kernel samples instead of the raw parameters: kPacked field arrays of
+    // maxN floats (field f of query i at out[f * maxN + i]).
+    void infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, float* out, cudaStream_t st,
+                     uint32_t* status = nullptr, bool packed = false) const;
     // Inference kernel: warp-level mma.sync tiles of 32 queries, or tcgen05
     // MMAs with tensor-memory accumulators on tiles of 128 queries.
     static constexpr int kKernelWarpMma = 0, kKernelTensorMemory = 1;

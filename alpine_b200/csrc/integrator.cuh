@@ -75,9 +75,10 @@ struct WaveView {
     uint4* pixelRng;
     // learned guiding (counter RNG only)
     guide::Query* guideQuery;  // compacted queries of the guided vertices; null = guiding off
-    int* guideSlot;            // per queue entry: index into guideQuery / guideRaw, -1 = not guided
+    int* guideSlot;            // per queue entry: index into guideQuery / guideLobes, -1 = not guided
     uint32_t* guideCount;      // number of guided vertices of the current queue
-    const float* guideRaw;     // per guided vertex: 40 mixture parameters; null = material sampling only
+    const float* guideLobes;   // decoded mixtures of the guided vertices: guide::kPacked field arrays of numPaths
+                               // floats (field f of slot s at [f * numPaths + s]); null = material sampling only
     float guideFraction;       // probability of sampling the guide at an eligible vertex
     float guideMinRough;       // eligible vertices: material alpha >= this
     guide::Sample* trainRec;   // recorded vertices: query, direction (weight filled by finalize)
@@ -282,34 +283,21 @@ AG_D alpine_gpu_ray make_ray(float3 o, float3 d, float tmax)
 }
 
 // One-sample MIS continuation: the direction comes from the guide's mixture
-// (moved into the local shading frame) with probability alpha, else from the
-// material's procedure; either way the weight is f / (alpha p_guide +
-// (1 - alpha) p_mat) with f and p_mat the material procedure's effective
-// integrand and true density (plain_eval), an unbiased estimate of what the
-// material's own sampling estimates.
-AG_D bool guided_continuation(const Material& mat, float3 wo, const float* raw, float alpha, float3 ss, float3 ts,
-                              float3 ns, PathRng& rng, float3& wi, float3& est)
+// with probability alpha, else from the material's procedure; either way the
+// weight is f / (alpha p_guide + (1 - alpha) p_mat) with f and p_mat the
+// material procedure's effective integrand and true density (plain_eval),
+// an unbiased estimate of what the material's own sampling estimates. The
+// mixture (guide::kPacked fields `stride` apart, world space) is read lobe
+// by lobe; its density is evaluated at the world-space direction.
+AG_D bool guided_continuation(const Material& mat, float3 wo, const float* lobes, uint32_t stride, float alpha,
+                              float3 ss, float3 ts, float3 ns, PathRng& rng, float3& wi, float3& est)
 {
-    float r[40];
-#pragma unroll
-    for (int k = 0; k < 40; k += 4) {
-        const float4 v = __ldcs(reinterpret_cast<const float4*>(raw + k));
-        r[k] = v.x; r[k + 1] = v.y; r[k + 2] = v.z; r[k + 3] = v.w;
-    }
-    guide::Mixture m;
-    guide::decode_mixture(r, m);
-#pragma unroll
-    for (int k = 0; k < guide::kLobes; ++k) {
-        const float3 mu = to_local(m.mu[k], ss, ts, ns);
-        const float l = len3(mu);
-        m.mu[k] = l > 0.0f ? mu / l : mk3(0.0f, 0.0f, 1.0f);
-    }
     const float us = rng.next();
     const float u0 = rng.next();
     const float u1 = rng.next();
     const float u2 = rng.next();
     if (us < alpha) {
-        wi = guide::mixture_sample(m, u0, u1, u2);
+        wi = normalize3(to_local(guide::lobes_sample(lobes, stride, u0, u1, u2), ss, ts, ns));
     } else {
         BsdfSample ms;
         if (!sample_material(mat, wo, u0, u1, ms)) return false;
@@ -318,7 +306,7 @@ AG_D bool guided_continuation(const Material& mat, float3 wo, const float* raw, 
     float pm;
     float3 fcos;
     if (!plain_eval(mat, wo, wi, pm, fcos)) return false;  // outside the procedure's support: f = 0
-    float pg = guide::mixture_pdf(m, wi);
+    float pg = guide::lobes_pdf(lobes, stride, normalize3(to_world(wi, ss, ts, ns)));
     if (!(pg >= 0.0f && pg < 3.0e38f)) pg = 0.0f;
     const float qm = alpha * pg + (1.0f - alpha) * pm;
     if (!(qm > 0.0f)) return false;
@@ -473,8 +461,9 @@ __global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED
         // as well, should contraction round the two tests differently)
         const int gslot = kGuided ? w.guideSlot[q] : -1;
         const bool guidable = gslot >= 0 && wo.z > 0.0f;
-        if (guidable && w.guideRaw) {
-            ok = guided_continuation(mat, wo, w.guideRaw + 40ull * gslot, w.guideFraction, ss, ts, ns, rng, wiL, est);
+        if (guidable && w.guideLobes) {
+            ok = guided_continuation(mat, wo, w.guideLobes + gslot, w.numPaths, w.guideFraction, ss, ts, ns, rng, wiL,
+                                     est);
         } else {
             BsdfSample ms;
             float cu0 = rng.next();

@@ -337,7 +337,7 @@ ag::WaveView carve_wave(alpine_gpu_ctx* c)
 struct GuideWave {
     ag::guide::Query* query;
     int* querySlot;      // per queue entry
-    float* raw;
+    float* lobes;        // per guided vertex: the decoded mixture (kPacked floats)
     int* slot;
     ag::guide::Sample* rec;
     float4* aux;
@@ -348,7 +348,7 @@ struct GuideWave {
 bool reserve_guide_wave(alpine_gpu_ctx* c, uint32_t paths, uint32_t cap, GuideWave& g)
 {
     size_t P = paths, R = cap;
-    size_t bytes = round256(P * sizeof(ag::guide::Query)) + round256(P * sizeof(int)) + round256(P * 40 * sizeof(float)) +
+    size_t bytes = round256(P * sizeof(ag::guide::Query)) + round256(P * sizeof(int)) + round256(P * ag::guide::kPacked * sizeof(float)) +
                    round256(P * sizeof(int)) + round256(R * sizeof(ag::guide::Sample)) +
                    round256(2 * R * sizeof(float4)) + round256(R * sizeof(ag::guide::Sample)) + 256;
     if (!c->dGuideWave.reserve(bytes)) return false;
@@ -360,7 +360,7 @@ bool reserve_guide_wave(alpine_gpu_ctx* c, uint32_t paths, uint32_t cap, GuideWa
     };
     g.query = (ag::guide::Query*)take(P * sizeof(ag::guide::Query));
     g.querySlot = (int*)take(P * sizeof(int));
-    g.raw = (float*)take(P * 40 * sizeof(float));
+    g.lobes = (float*)take(P * ag::guide::kPacked * sizeof(float));
     g.slot = (int*)take(P * sizeof(int));
     g.rec = (ag::guide::Sample*)take(R * sizeof(ag::guide::Sample));
     g.aux = (float4*)take(2 * R * sizeof(float4));
@@ -787,7 +787,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
                 w.guideQuery = gw.query;
                 w.guideSlot = gw.querySlot;
                 w.guideCount = gw.counters + 2;
-                w.guideRaw = sampleGuide ? gw.raw : nullptr;
+                w.guideLobes = sampleGuide ? gw.lobes : nullptr;
                 w.guideFraction = gFrac;
                 w.guideMinRough = o.guide_min_roughness;
             }
@@ -814,12 +814,13 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
                 if (guideHere) {
                     cudaMemsetAsync(w.guideCount, 0, sizeof(uint32_t), st);
                     K.guide_query(sc, w, w.numPaths, st);
-                    if (sampleGuide) c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.raw, st, c->dStatus);
+                    if (sampleGuide)
+                        c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.lobes, st, c->dStatus, true);
                     K.shade(sc, w, stream, w.numPaths, st);
                 } else {
                     ag::WaveView plain = w;  // unguided shading (pending training records still resolve)
                     plain.guideQuery = nullptr;
-                    plain.guideRaw = nullptr;
+                    plain.guideLobes = nullptr;
                     K.shade(sc, plain, stream, w.numPaths, st);
                 }
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,

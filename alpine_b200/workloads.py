@@ -8,6 +8,10 @@ first render's launches.
                                              # 16 Adam steps, then 2 x 32 spp
     python -m alpine_b200.workloads guided_tc  # the same with the tcgen05 inference kernel
     python -m alpine_b200.workloads city     # many-light city 960x540, 1 + 2 spp, depth 8, light BVH
+    python -m alpine_b200.workloads interior        # glossy interior 320x180, depth 12, plain MIS, 2 x 64 spp
+    python -m alpine_b200.workloads interior_guided # the same guided with the time-to-relMSE schedule
+                                                    # (8 spp waves, 16 Adam steps per wave, 512 steps):
+                                                    # 256 spp while training, then 64 spp
 """
 from __future__ import annotations
 
@@ -27,6 +31,13 @@ def run(mode: str, device: int = 0) -> float:
         opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
                     guide_min_roughness=0.2, guide_train_steps=16)
         sampler, spp = None, (32, 32)
+    elif mode in ("interior", "interior_guided"):
+        sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
+        opts, sampler, spp = dict(accumulate_fp64=True), None, (64, 64)
+        if mode == "interior_guided":
+            opts.update(guide=True, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=16, guide_lr=1e-2,
+                        guide_min_roughness=0.2, guide_train_steps=512)
+            spp = (256, 64)
     elif mode == "city":
         sc, (W, H), depth = scenes.city_scene(), (960, 540), 8
         opts, sampler, spp = {}, gpu.SAMPLER_BVH, (1, 2)
