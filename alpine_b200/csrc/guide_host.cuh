@@ -73,7 +73,9 @@ private:
     float* wG_ = nullptr;
     __nv_bfloat16* wB_ = nullptr;
     __nv_bfloat16* wT_ = nullptr;
-    float* partial_ = nullptr;
+    float* partial_ = nullptr;   // per-split weight gradients
+    __nv_bfloat16* xt_ = nullptr;  // layer inputs of a training slice, transposed
+    __nv_bfloat16* dt_ = nullptr;  // layer output gradients of a training slice, transposed
     float* loss_ = nullptr;
     float3 bmin_ = make_float3(0.0f, 0.0f, 0.0f);
     float3 invExtent_ = make_float3(1.0f, 1.0f, 1.0f);
