@@ -47,43 +47,46 @@ AG_D void load_weights(const __nv_bfloat16* __restrict__ g, __nv_bfloat16* s)
     }
 }
 
-// Encodes the 64 inputs of one query into a bf16 row. Levels are processed
-// two at a time with their 16 corner loads issued together: the encoding is
-// bound by the latency of these gathers.
+// Encodes the 64 inputs of one query into a bf16 row. The corner loads of
+// kEncodeLevels levels are issued together, the trilinear weights formed
+// after them (2, 4 and 8 levels per round measured the same).
+constexpr int kEncodeLevels = 4;
+static_assert(kLevels % kEncodeLevels == 0, "levels per round");
 AG_D void encode_row(const Params& g, const Query& q, __nv_bfloat16* row)
 {
     const float3 p = normalise_position(g, mk3(q.pos[0], q.pos[1], q.pos[2]));
 #pragma unroll
-    for (int l0 = 0; l0 < kLevels; l0 += 2) {
-        uint32_t idx[2][8];
-        float w[2][8];
-        __half2 v[2][8];
+    for (int l0 = 0; l0 < kLevels; l0 += kEncodeLevels) {
+        __half2 v[kEncodeLevels][8];
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < kEncodeLevels; ++j)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) grid_corner(g.res[l0 + j], p, c, idx[j][c], w[j][c]);
+            for (int c = 0; c < 8; ++c) {
+                uint32_t idx;
+                float w;
+                grid_corner(g.res[l0 + j], p, c, idx, w);
+                v[j][c] = *reinterpret_cast<const __half2*>(g.grid + ((uint64_t)(l0 + j) * kTableSize + idx) * kFeatures);
+            }
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                v[j][c] = *reinterpret_cast<const __half2*>(g.grid + ((uint64_t)(l0 + j) * kTableSize + idx[j][c]) * kFeatures);
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < kEncodeLevels; ++j) {
             float f0 = 0.0f, f1 = 0.0f;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
-                f0 += w[j][c] * __low2float(v[j][c]);
-                f1 += w[j][c] * __high2float(v[j][c]);
+                uint32_t idx;
+                float w;
+                grid_corner(g.res[l0 + j], p, c, idx, w);
+                f0 += w * __low2float(v[j][c]);
+                f1 += w * __high2float(v[j][c]);
             }
-            row[2 * (l0 + j)] = bf(f0);
-            row[2 * (l0 + j) + 1] = bf(f1);
+            *reinterpret_cast<uint32_t*>(row + 2 * (l0 + j)) = pack_bf2(f0, f1);
         }
     }
     float ex[8];
     extra_inputs(mk3(q.wo[0], q.wo[1], q.wo[2]), mk3(q.n[0], q.n[1], q.n[2]), q.rough, ex);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) row[kGridDims + k] = bf(ex[k]);
-    for (int k = kGridDims + 8; k < kIn; ++k) row[k] = bf(0.0f);
+    for (int k = 0; k < 8; k += 2) *reinterpret_cast<uint32_t*>(row + kGridDims + k) = pack_bf2(ex[k], ex[k + 1]);
+#pragma unroll
+    for (int k = kGridDims + 8; k < kIn; k += 2) *reinterpret_cast<uint32_t*>(row + k) = 0u;
 }
 
 // acc = X[32 x K] * Wl^T for one warp's 32 rows: X row-major (stride kLd),
@@ -141,43 +144,73 @@ AG_D void hidden_layers(const __nv_bfloat16* W, __nv_bfloat16* X, __nv_bfloat16*
     }
 }
 
-// Packs the output tile of one warp's 32 queries (acc, the mma fragments of
-// the output layer) into decoded mixtures, 16 rows at a time: the rows are
-// staged as fp32 in the warp's activation tile (free after the output
-// layer), then two lanes per row decode 4 lobes each.
-AG_D void pack_tile(const float (&acc)[2][kOut / 8][4], __nv_bfloat16* X, uint32_t row0, uint32_t n, float* out,
-                   uint32_t stride)
+// The inference kernel's shared copy of the output layer has its rows (the
+// output units) permuted so that each lane's mma fragments hold whole lobes:
+// fragment column c = 8 nt + 2 t + e (lane t of a quad, nt < 5, e < 2) is
+// raw output (2 t + s / 5) * 5 + s % 5 with s = 2 nt + e, i.e. lane t holds
+// the 5 values of lobes 2t and 2t+1 of its two rows; columns 40..47 (nt = 5)
+// stay the unused outputs 40..47.
+__host__ __device__ constexpr int out_column_raw(int c)
+{
+    return c >= 40 ? c : (2 * ((c % 8) / 2) + (2 * (c / 8) + c % 2) / 5) * 5 + (2 * (c / 8) + c % 2) % 5;
+}
+
+AG_D void load_weights_infer(const __nv_bfloat16* __restrict__ g, __nv_bfloat16* s)
+{
+    for (int l = 0; l < kLayers; ++l) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(g + layer_offset(l));
+        uint32_t* dst = reinterpret_cast<uint32_t*>(s + wsm_offset(l));
+        const int words = layer_in(l) / 2, rows = layer_out(l);
+        for (int i = threadIdx.x; i < rows * words; i += blockDim.x) {
+            const int r = i / words, k = i % words;
+            const int from = l == kLayers - 1 ? out_column_raw(r) : r;
+            dst[r * (wld(l) / 2) + k] = src[from * words + k];
+        }
+    }
+}
+
+// Writes the output tile of one warp's 32 queries (acc: the mma fragments of
+// the permuted output layer) as raw parameters (raw[query * 40 + i]) or, with
+// `packed`, as decoded mixtures in field arrays `stride` long: each lane
+// decodes lobes 2t and 2t+1 of its rows from registers, the softmax over a
+// row's 8 lobes reduced across the quad.
+AG_D void write_outputs(const float (&acc)[2][kOut / 8][4], uint32_t row0, uint32_t n, float* out, bool packed,
+                        uint32_t stride)
 {
     const int lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
-    float* S = reinterpret_cast<float*>(X);  // 16 x 40 floats: 2,560 of the tile's 4,608 bytes
-    static_assert(16 * 40 * 4 <= 32 * kLd * 2, "staging fits the activation tile");
-    const int row = lane >> 1, part = lane & 1;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-        __syncwarp();  // every lane is done with X (output layer, or the previous half)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 5; ++nt) {
-            const int col = nt * 8 + 2 * t4;
-            *reinterpret_cast<float2*>(S + g4 * 40 + col) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
-            *reinterpret_cast<float2*>(S + (g4 + 8) * 40 + col) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
+        for (int h = 0; h < 2; ++h) {  // rows g4 and g4 + 8 of the m tile
+            const uint32_t gr = row0 + mt * 16 + g4 + 8 * h;
+            float r[2][kRawPerLobe];
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int v = 0; v < kRawPerLobe; ++v) {
+                    const int sIdx = kRawPerLobe * j + v;
+                    r[j][v] = acc[mt][sIdx / 2][2 * h + sIdx % 2];
+                }
+            if (!packed) {
+                if (gr < n)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+#pragma unroll
+                        for (int v = 0; v < kRawPerLobe; ++v)
+                            out[(uint64_t)gr * 40 + (2 * t4 + j) * kRawPerLobe + v] = r[j][v];
+                continue;
+            }
+            float mx = fmaxf(r[0][4], r[1][4]);
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            float sum = expf(r[0][4] - mx) + expf(r[1][4] - mx);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+            const float invSum = 1.0f / sum;
+            if (gr < n)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) pack_lobe(r[j], mx, invSum, 2 * t4 + j, out + gr, stride);
         }
-        __syncwarp();
-        const float* r = S + row * 40 + part * 4 * kRawPerLobe;
-        float mx = -3.4e38f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) mx = fmaxf(mx, r[k * kRawPerLobe + 4]);
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-        float sum = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) sum += expf(r[k * kRawPerLobe + 4] - mx);
-        sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-        const float invSum = 1.0f / sum;
-        const uint32_t gr = row0 + mt * 16 + row;
-        if (gr < n)
-#pragma unroll 1
-            for (int k = 0; k < 4; ++k) pack_lobe(r + k * kRawPerLobe, mx, invSum, part * 4 + k, out + gr, stride);
-    }
-    __syncwarp();
 }
 
 // n queries, or *nDev when nDev is not null (a queue length written on the
@@ -192,9 +225,9 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_infer(Params g, const Q
     if (nDev) n = min(n, *nDev);
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __nv_bfloat16* X = W + kWsm + warp * 32 * kLd;
-    load_weights(g.W, W);
+    load_weights_infer(g.W, W);
     __syncthreads();
     const uint32_t chunks = (n + 31) / 32;
     for (uint32_t ch = blockIdx.x * kInferWarps + warp; ch < chunks; ch += gridDim.x * kInferWarps) {
@@ -208,19 +241,7 @@ __global__ void __launch_bounds__(32 * kInferWarps, 2) k_infer(Params g, const Q
         hidden_layers(W, X, nullptr);
         float acc[2][kOut / 8][4];
         warp_layer<kOut, kHidden>(X, W + wsm_offset(kLayers - 1), wld(kLayers - 1), acc);
-        if (packed) {
-            pack_tile(acc, X, ch * 32, n, raw, nMax);
-            continue;
-        }
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 5; ++nt) {  // columns 0..39
-                const int col = nt * 8 + 2 * t4;
-                const uint32_t r0 = ch * 32 + mt * 16 + g4, r1 = r0 + 8;
-                if (r0 < n) *reinterpret_cast<float2*>(raw + (uint64_t)r0 * 40 + col) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
-                if (r1 < n) *reinterpret_cast<float2*>(raw + (uint64_t)r1 * 40 + col) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
-            }
+        write_outputs(acc, ch * 32, n, raw, packed, nMax);
         __syncwarp();
     }
 }
