@@ -683,7 +683,11 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
     uint32_t pixelChunk = std::min(pixels, maxPaths / S);
     if (!reserve_wave(c, S * pixelChunk)) return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "wave buffers");
     GuideWave gw{};
-    const uint32_t trainCap = trainEnabled ? std::min<uint32_t>(1u << 21, 2u * gSteps * gBatch) : 0u;
+    // Recorded vertices per wave: only those that later receive radiance
+    // become samples (about 12% in a dim interior), so 8 x steps x batch
+    // records keep every step of the wave at about a full batch (2 x, 4 x and
+    // 8 x measured 2.45, 2.76 and 2.78 x plain's speed to a relMSE of 0.01).
+    const uint32_t trainCap = trainEnabled ? std::min<uint32_t>(1u << 22, 8u * gSteps * gBatch) : 0u;
     if (guiding) {
         if (!c->guide.ready() && c->guide.reset(c->guideSeed, c->stream) != 0)
             return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "guide: parameter allocation failed");

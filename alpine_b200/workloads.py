@@ -10,7 +10,7 @@ first render's launches.
     python -m alpine_b200.workloads city     # many-light city 960x540, 1 + 2 spp, depth 8, light BVH
     python -m alpine_b200.workloads interior        # glossy interior 320x180, depth 12, plain MIS, 2 x 64 spp
     python -m alpine_b200.workloads interior_guided # the same guided with the time-to-relMSE schedule
-                                                    # (8 spp waves, 16 Adam steps per wave, 512 steps):
+                                                    # (8 spp waves, 32 Adam steps per wave, 512 steps):
                                                     # 256 spp while training, then 64 spp
 """
 from __future__ import annotations
@@ -35,7 +35,7 @@ def run(mode: str, device: int = 0) -> float:
         sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
         opts, sampler, spp = dict(accumulate_fp64=True), None, (64, 64)
         if mode == "interior_guided":
-            opts.update(guide=True, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=16, guide_lr=1e-2,
+            opts.update(guide=True, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=32, guide_lr=1e-2,
                         guide_min_roughness=0.2, guide_train_steps=512)
             spp = (256, 64)
     elif mode == "city":
