@@ -414,8 +414,12 @@ __global__ void k_post(const float* a32, const double* a64, uint32_t pixels, uin
 __global__ void k_set_word(uint32_t* p, uint32_t v) { *p = v; }
 
 // Turns the wave's recorded vertices into training samples and takes up to
-// `maxSteps` Adam steps; step i uses samples i, i + steps, i + 2 steps, ...
-// so that every batch spans the whole image.
+// `maxSteps` Adam steps; step i uses samples i, i + stride, i + 2 stride, ...
+// so that every batch spans the whole image. The stride is the number of
+// steps, or larger when the wave kept more than steps x batch samples: a
+// step then takes `batch` samples (the surplus is not used), which keeps it
+// one k_train_rows launch (a second slice would cost a whole latency-bound
+// launch for a few samples).
 int train_guide(alpine_gpu_ctx* c, const ag::IntegratorKernels& K, const ag::WaveView& w, const GuideWave& gw,
                 uint32_t batch, uint32_t maxSteps, float lr)
 {
@@ -429,9 +433,13 @@ int train_guide(alpine_gpu_ctx* c, const ag::IntegratorKernels& K, const ag::Wav
     if (kept == 0) return ALPINE_GPU_OK;
     const uint32_t steps = std::min(maxSteps, (kept + batch - 1) / batch);
     c->guide.reset_loss(st);
+    // with a surplus, stride = kept / batch >= steps: the steps' residues are
+    // disjoint and i + (batch - 1) stride < kept
+    const bool surplus = (uint64_t)kept > (uint64_t)steps * batch;
+    const uint32_t stride = surplus ? kept / batch : steps;
     for (uint32_t i = 0; i < steps; ++i) {
-        const uint32_t n = (kept - i + steps - 1) / steps;
-        c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, steps);
+        const uint32_t n = surplus ? batch : (kept - i + steps - 1) / steps;
+        c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, stride);
         c->guide.apply_adam(lr, st);
     }
     c->guideLastLossSteps = steps;
