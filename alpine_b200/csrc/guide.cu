@@ -213,10 +213,10 @@ AG_D void write_outputs(const float (&acc)[2][kOut / 8][4], uint32_t row0, uint3
         }
 }
 
-// n queries, or *nDev when nDev is not null (a queue length written on the
-// device). Writes the 40 raw outputs per query, or with `packed` the decoded
-// mixtures as kPacked field arrays of n floats each (field f of query i at
-// raw[f * n + i]).
+// n queries, or min(n, *nDev) when nDev is not null (a queue length written
+// on the device). Writes the 40 raw outputs per query, or with `packed` the
+// decoded mixtures as kPacked field arrays of n floats each, n as passed in
+// (field f of query i at raw[f * n + i]).
 __global__ void __launch_bounds__(32 * kInferWarps, 2) k_infer(Params g, const Query* __restrict__ q, uint32_t n,
                                                           const uint32_t* __restrict__ nDev, float* __restrict__ raw,
                                                           bool packed)
