@@ -18,18 +18,6 @@ std::string cuda_msg(const char* what, cudaError_t e)
     return std::string(what) + ": " + cudaGetErrorString(e);
 }
 
-std::string status_msg(uint32_t bits)
-{
-    std::string m = "device-side limit:";
-    if (bits & ag::kErrStackOverflow) m += " traversal stack overflow;";
-    if (bits & ag::kErrBadIndex) m += " node/triangle index out of range;";
-    if (bits & ag::kErrIterations) m += " traversal visit cap reached;";
-    if (bits & ag::kErrBuildDepth) m += " BVH build level cap reached;";
-    if (bits & ag::kErrQueueOverflow) m += " wavefront queue overflow;";
-    if (bits & ag::kErrTensorWait) m += " tensor-core completion wait timed out;";
-    return m;
-}
-
 // Reads and clears the device status word (stream must be idle).
 int check_status(alpine_gpu_ctx* c)
 {
@@ -40,7 +28,7 @@ int check_status(alpine_gpu_ctx* c)
         uint32_t bits = *c->hStatus;
         cudaMemsetAsync(c->dStatus, 0, sizeof(uint32_t), c->stream);
         cudaStreamSynchronize(c->stream);
-        return c->fail(ALPINE_GPU_ERR_LIMIT, status_msg(bits));
+        return c->fail(ALPINE_GPU_ERR_LIMIT, ag::status_msg(bits));
     }
     return ALPINE_GPU_OK;
 }
@@ -59,15 +47,7 @@ int upload_geometry_now(alpine_gpu_ctx* c)
     return ALPINE_GPU_OK;
 }
 
-ag::BvhView view(const alpine_gpu_ctx* c)
-{
-    ag::BvhView v;
-    v.nodes = c->dNodes.as<ag::WideNode>();
-    v.tris = c->dTris.as<ag::TriRecord>();
-    v.nodeCount = c->nodeCount;
-    v.triCount = c->triCount;
-    return v;
-}
+ag::BvhView view(const alpine_gpu_ctx* c) { return c->bvh_view(); }
 
 int require_bvh(alpine_gpu_ctx* c)
 {
@@ -345,6 +325,19 @@ int alpine_gpu_traversal_stats(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, ui
     *nodeVisits = h[0];
     *triVisits = h[1];
     return check_status(c);
+}
+
+int alpine_gpu_set_traversal_options(alpine_gpu_ctx* c, const alpine_gpu_traversal_options* o)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!o) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_traversal_options: null options");
+    if (o->triangle_test != ALPINE_GPU_TRIANGLE_TEST_WIDE_BVH && o->triangle_test != ALPINE_GPU_TRIANGLE_TEST_BINARY_BVH)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_traversal_options: unknown triangle_test");
+    if (o->stack_limit > (uint32_t)ag::kTraversalStack)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT,
+                       "set_traversal_options: stack_limit above " + std::to_string(ag::kTraversalStack));
+    c->traversal = *o;
+    return ALPINE_GPU_OK;
 }
 
 int alpine_gpu_synchronize(alpine_gpu_ctx* c)

@@ -66,13 +66,22 @@ constexpr int kSahBins = 32;             // binned SAH resolution
 #define AG_TRAVERSAL_STACK 24
 #endif
 constexpr int kTraversalStack = AG_TRAVERSAL_STACK;  // node-group stack entries per ray
-constexpr uint32_t kMaxVisits = 1u << 16;  // per-ray wide-node visit cap
+constexpr uint32_t kMaxVisits = 1u << 16;  // default per-ray wide-node visit cap
+
+// Triangle acceptance rule of a traversal: the reference's 8-wide BVH
+// (src/ispc/triangle.ispc:46-87) or its binary BVH
+// (src/accelerators/bvh_common.cpp:66-103).
+constexpr uint32_t kTriTestWide = 0;
+constexpr uint32_t kTriTestBinary = 1;
 
 struct BvhView {
-    const WideNode* nodes;
-    const TriRecord* tris;
-    uint32_t nodeCount;
-    uint32_t triCount;
+    const WideNode* nodes = nullptr;
+    const TriRecord* tris = nullptr;
+    uint32_t nodeCount = 0;
+    uint32_t triCount = 0;
+    uint32_t maxVisits = kMaxVisits;                 // a ray fetching more nodes ends with kErrIterations
+    uint32_t stackLimit = (uint32_t)kTraversalStack;  // stack entries a ray may use (<= kTraversalStack)
+    uint32_t triTest = kTriTestWide;                 // selects the kernel instantiation at launch
 };
 
 }  // namespace ag

@@ -43,6 +43,19 @@ struct DeviceBuffer {
 
 constexpr int kCopyStreams = 8;  // host-query pipeline streams
 
+// Human-readable description of DeviceError bits.
+inline std::string status_msg(uint32_t bits)
+{
+    std::string m = "device-side limit:";
+    if (bits & kErrStackOverflow) m += " traversal stack overflow;";
+    if (bits & kErrBadIndex) m += " node/triangle index out of range;";
+    if (bits & kErrIterations) m += " traversal visit cap reached;";
+    if (bits & kErrBuildDepth) m += " BVH build level cap reached;";
+    if (bits & kErrQueueOverflow) m += " wavefront queue overflow;";
+    if (bits & kErrTensorWait) m += " tensor-core completion wait timed out;";
+    return m;
+}
+
 int upload_render_scene(alpine_gpu_ctx* c);  // render.cu: materials, attributes, lights to the device
 int upload_geometry(alpine_gpu_ctx* c);      // api.cu: vertices and indices to the device
 
@@ -131,6 +144,9 @@ struct alpine_gpu_ctx {
     uint32_t graphLaunches = 0, graphCaptures = 0;
     uint32_t* dSampleBase = nullptr;  // first sample index of a replayed render
 
+    // traversal options (triangle rule, device-side limits)
+    alpine_gpu_traversal_options traversal{};
+
     // morph-target animation (Mesh::Data::targets, src/shapes/mesh.h:27-33;
     // Animation channels, src/animation.h). The morphed positions and normals
     // are written on the device; the host mirrors are refreshed on demand.
@@ -169,9 +185,25 @@ struct alpine_gpu_ctx {
             uint32_t bits = *hStatus;
             cudaMemsetAsync(dStatus, 0, sizeof(uint32_t), stream);
             cudaStreamSynchronize(stream);
-            return fail(ALPINE_GPU_ERR_LIMIT, "device-side limit reached, status bits " + std::to_string(bits));
+            return fail(ALPINE_GPU_ERR_LIMIT, ag::status_msg(bits));
         }
         return ALPINE_GPU_OK;
+    }
+
+    // The BVH as the traversal kernels see it, with this context's options.
+    // nodeCount / triCount are the built counts (the render passes its
+    // allocation sizes instead, see render.cu).
+    ag::BvhView bvh_view() const
+    {
+        ag::BvhView v;
+        v.nodes = dNodes.as<ag::WideNode>();
+        v.tris = dTris.as<ag::TriRecord>();
+        v.nodeCount = nodeCount;
+        v.triCount = triCount;
+        v.triTest = traversal.triangle_test;
+        v.maxVisits = traversal.max_visits ? traversal.max_visits : ag::kMaxVisits;
+        v.stackLimit = traversal.stack_limit ? traversal.stack_limit : (uint32_t)ag::kTraversalStack;
+        return v;
     }
 
     // Copies device-side morph results into the host mirrors (before a host

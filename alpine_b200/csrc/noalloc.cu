@@ -18,7 +18,10 @@
 // Host code must not use the array's name as a device address (on the host it
 // is only a stand-in). The device address is obtained once per device with
 // cudaGetSymbolAddress, with that device current, on the first call for that
-// device. Make that first call before any stream capture begins.
+// device; under CUDA's lazy module loading that first call may also load the
+// module holding the array. Every call is synchronous and copies through host
+// memory, so none may be made while the context's stream (or a stream it
+// depends on) is being captured.
 //
 // All calls in a process share the one array, which keeps the contents of the
 // last call; the status word is cleared at the start of every call. Calls that
@@ -77,11 +80,7 @@ extern "C" int alpine_gpu_trace_noalloc(alpine_gpu_ctx* c, const alpine_gpu_ray*
     void* dHits = base + kRayBytes;
     uint32_t* dStatus = reinterpret_cast<uint32_t*>(base + kRayBytes + kHitBytes);
 
-    ag::BvhView v;
-    v.nodes = c->dNodes.as<ag::WideNode>();
-    v.tris = c->dTris.as<ag::TriRecord>();
-    v.nodeCount = c->nodeCount;
-    v.triCount = c->triCount;
+    const ag::BvhView v = c->bvh_view();
 
     uint32_t status = 0;
     e = cudaMemsetAsync(dStatus, 0, sizeof(uint32_t), c->stream);
@@ -97,6 +96,6 @@ extern "C" int alpine_gpu_trace_noalloc(alpine_gpu_ctx* c, const alpine_gpu_ray*
         cudaGetLastError();
         return c->fail(ALPINE_GPU_ERR_CUDA, std::string("trace_noalloc: ") + cudaGetErrorString(e));
     }
-    if (status) return c->fail(ALPINE_GPU_ERR_LIMIT, "trace_noalloc: device-side limit reached (status bits set)");
+    if (status) return c->fail(ALPINE_GPU_ERR_LIMIT, "trace_noalloc: " + ag::status_msg(status));
     return ALPINE_GPU_OK;
 }

@@ -731,9 +731,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
     sc.width = c->cfg.width;
     sc.height = c->cfg.height;
     sc.maxDepth = c->cfg.max_depth;
-    ag::BvhView bvh;
-    bvh.nodes = c->dNodes.as<ag::WideNode>();
-    bvh.tris = c->dTris.as<ag::TriRecord>();
+    ag::BvhView bvh = c->bvh_view();
     // bounds checks against the allocations, so that a rebuilt BVH of the
     // same scene replays the same captured graph
     bvh.nodeCount = (uint32_t)(c->dNodes.bytes / sizeof(ag::WideNode));
@@ -756,7 +754,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
         };
         const uint32_t cfgWords[] = {spp, S, pixelChunk, pixels, (uint32_t)stream, (uint32_t)fp64,
                                      (uint32_t)c->traceBlock, c->options.seed, c->options.russian_roulette_depth,
-                                     c->waveCapacity};
+                                     c->waveCapacity, bvh.triTest, bvh.maxVisits, bvh.stackLimit};
         const void* ptrs[] = {c->dWave.ptr, c->dAccum.ptr, c->dPixelRng.ptr, c->dStatus};
         put(cfgWords, sizeof cfgWords);
         put(ptrs, sizeof ptrs);

@@ -5,7 +5,7 @@
 namespace ag {
 namespace {
 
-template <bool kAny>
+template <bool kAny, bool kBinary>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(BvhView bvh, const float4* __restrict__ rays, uint32_t n,
                                                        void* __restrict__ out, uint32_t* __restrict__ status)
 {
@@ -17,8 +17,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(BvhView bvh, const float4
     float4 b = __ldcs(rays + 2ull * i + 1);
     TraceResult r;
     uint32_t err = 0, nv = 0, tv = 0;
-    bool hit = trace<kAny>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
-                           kTraceBlock, err, nv, tv);
+    bool hit = trace<kAny, kBinary>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
+                                    kTraceBlock, err, nv, tv);
     if (kAny) {
         __stcs(static_cast<uint8_t*>(out) + i, (uint8_t)(hit ? 1 : 0));
     } else {
@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(BvhView bvh, const float4
 }
 
 // Instrumented variant: same traversal, accumulates node / triangle visits.
-template <bool kAny>
+template <bool kAny, bool kBinary>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const float4* __restrict__ rays, uint32_t n,
                                                              unsigned long long* __restrict__ counts,
                                                              uint32_t* __restrict__ status)
@@ -40,8 +40,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const 
     if (i < n) {
         float4 a = rays[2ull * i], b = rays[2ull * i + 1];
         TraceResult r;
-        trace<kAny>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x, kTraceBlock,
-                    err, nv, tv);
+        trace<kAny, kBinary>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
+                             kTraceBlock, err, nv, tv);
     }
     unsigned long long snv = nv, stv = tv;
 #pragma unroll
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const 
 
 // Variant whose ray count is read from device memory (wavefront queues),
 // with the block size as a parameter (chosen by the autotuner).
-template <bool kAny, int kBlock>
+template <bool kAny, int kBlock, bool kBinary>
 __global__ void __launch_bounds__(kBlock) k_trace_dyn(BvhView bvh, const float4* __restrict__ rays,
                                                       const uint32_t* __restrict__ count, void* __restrict__ out,
                                                       uint32_t* __restrict__ status)
@@ -71,8 +71,8 @@ __global__ void __launch_bounds__(kBlock) k_trace_dyn(BvhView bvh, const float4*
         float4 b = rays[2ull * i + 1];
         TraceResult r;
         uint32_t err = 0, nv = 0, tv = 0;
-        bool hit = trace<kAny>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
-                               kBlock, err, nv, tv);
+        bool hit = trace<kAny, kBinary>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r,
+                                        stack + threadIdx.x, kBlock, err, nv, tv);
         if (kAny) static_cast<uint8_t*>(out)[i] = hit ? 1 : 0;
         else static_cast<uint4*>(out)[i] = make_uint4(r.prim, __float_as_uint(r.t), __float_as_uint(r.b1), __float_as_uint(r.b2));
         if (err) atomicOr(status, err);
@@ -89,7 +89,8 @@ void launch(const BvhView& bvh, const void* rays, uint64_t n, void* out, uint32_
         void* o = kAny ? static_cast<void*>(static_cast<uint8_t*>(out) + s)
                        : static_cast<void*>(static_cast<uint4*>(out) + s);
         unsigned blocks = (m + kTraceBlock - 1) / kTraceBlock;
-        k_trace<kAny><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, o, status);
+        if (bvh.triTest == kTriTestBinary) k_trace<kAny, true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, o, status);
+        else k_trace<kAny, false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, o, status);
     }
 }
 }  // namespace
@@ -100,8 +101,11 @@ void launch_dyn(const BvhView& bvh, const float4* r, const uint32_t* count, uint
                 uint32_t* status, cudaStream_t st)
 {
     const unsigned blocks = (maxCount + kBlock - 1) / kBlock;
-    if (any) k_trace_dyn<true, kBlock><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
-    else k_trace_dyn<false, kBlock><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    const bool bin = bvh.triTest == kTriTestBinary;
+    if (any && bin) k_trace_dyn<true, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    else if (any) k_trace_dyn<true, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    else if (bin) k_trace_dyn<false, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    else k_trace_dyn<false, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
 }
 }  // namespace
 
@@ -123,8 +127,11 @@ void launch_trace_count(const BvhView& bvh, const void* rays, uint64_t n, bool a
         uint32_t m = (uint32_t)(n - s < kMaxPerLaunch ? n - s : kMaxPerLaunch);
         const float4* r = static_cast<const float4*>(rays) + 2 * s;
         unsigned blocks = (m + kTraceBlock - 1) / kTraceBlock;
-        if (any) k_trace_count<true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
-        else k_trace_count<false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
+        const bool bin = bvh.triTest == kTriTestBinary;
+        if (any && bin) k_trace_count<true, true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
+        else if (any) k_trace_count<true, false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
+        else if (bin) k_trace_count<false, true><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
+        else k_trace_count<false, false><<<blocks, kTraceBlock, 0, st>>>(bvh, r, m, counts, status);
     }
 }
 

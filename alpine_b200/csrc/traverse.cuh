@@ -7,7 +7,10 @@
 // t < current tmax (the reference's `t >= tNear -> reject`). The triangle
 // arithmetic is the reference's, with every product, sum and the reciprocal
 // rounded separately (__fmul_rn / __fadd_rn / __frcp_rn), so t, b1 and b2 are
-// bit-identical to the reference's FP32 values for the same triangle. Child
+// bit-identical to the reference's FP32 values for the same triangle.
+// The binary-BVH rule (kBinary, src/accelerators/bvh_common.cpp:66-103) is
+// selectable per launch: |det| >= FLT_EPSILON, t, b1, b2 by IEEE division,
+// b1 <= 1 and b2 <= 1 - b1, with the reference's order of tests. Child
 // boxes are tested conservatively (quantised boxes are rounded outwards and
 // the exit distance is scaled by 1 + 4e-7 as bounding_box.ispc:29 does).
 //
@@ -61,6 +64,36 @@ AG_D bool tri_test(float3 o, float3 d, float4 v0, float4 e0, float4 e1, float tm
     float v = __fmul_rn(nb2, rcp);
     if (!(tt >= tmin) || !(tt < tmax)) return false;
     if (!(u >= 0.0f) || !(v >= 0.0f) || !(__fadd_rn(u, v) <= 1.0f)) return false;
+    t = tt;
+    b1 = u;
+    b2 = v;
+    return true;
+}
+
+// The reference binary BVH's Primitive::intersect
+// (src/accelerators/bvh_common.cpp:66-103) with explicit rounding: divisions
+// instead of one reciprocal, det rejected below FLT_EPSILON, and the tests in
+// the reference's order. tmin / tmax bound the accepted t as in tri_test
+// (tmin = 0 is the reference's own t >= 0 test); a NaN t is rejected there.
+AG_D bool tri_test_binary(float3 o, float3 d, float4 v0, float4 e0, float4 e1, float tmin, float tmax, float& t,
+                          float& b1, float& b2)
+{
+    float sx = __fsub_rn(o.x, v0.x), sy = __fsub_rn(o.y, v0.y), sz = __fsub_rn(o.z, v0.z);
+    float s1x = __fsub_rn(__fmul_rn(d.y, e1.z), __fmul_rn(d.z, e1.y));
+    float s1y = __fsub_rn(__fmul_rn(d.z, e1.x), __fmul_rn(d.x, e1.z));
+    float s1z = __fsub_rn(__fmul_rn(d.x, e1.y), __fmul_rn(d.y, e1.x));
+    float det = dot_rn(s1x, s1y, s1z, e0.x, e0.y, e0.z);
+    if (fabsf(det) < 1.1920928955078125e-7f) return false;  // FLT_EPSILON
+    float s2x = __fsub_rn(__fmul_rn(sy, e0.z), __fmul_rn(sz, e0.y));
+    float s2y = __fsub_rn(__fmul_rn(sz, e0.x), __fmul_rn(sx, e0.z));
+    float s2z = __fsub_rn(__fmul_rn(sx, e0.y), __fmul_rn(sy, e0.x));
+    float tt = __fdiv_rn(dot_rn(s2x, s2y, s2z, e1.x, e1.y, e1.z), det);
+    if (tt < 0.0f) return false;
+    float u = __fdiv_rn(dot_rn(s1x, s1y, s1z, sx, sy, sz), det);
+    if (u < 0.0f || u > 1.0f) return false;
+    float v = __fdiv_rn(dot_rn(d.x, d.y, d.z, s2x, s2y, s2z), det);
+    if (v < 0.0f || v > __fsub_rn(1.0f, u)) return false;
+    if (!(tt >= tmin) || !(tt < tmax)) return false;
     t = tt;
     b1 = u;
     b2 = v;
@@ -192,7 +225,7 @@ AG_D void ray_init(RayState& s, float3 o, float3 d, float tmin, float tmax)
 // stack: this thread's first entry in shared memory, entries `stride` apart.
 // nodeVisits / triVisits count wide nodes fetched and triangles tested (the
 // reference's BvhStats counters, src/accelerators/bvh_common.h:19-61).
-template <bool kAny>
+template <bool kAny, bool kBinary = false>
 AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, uint32_t& err, uint32_t& nodeVisits,
                    uint32_t& triVisits)
 {
@@ -207,7 +240,9 @@ AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, ui
         const TriRecord* r = bvh.tris + ti;
         float4 v0 = __ldg(&r->v0), e0 = __ldg(&r->e0), e1 = __ldg(&r->e1);
         float t, b1, b2;
-        if (tri_test(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2)) {
+        const bool accepted = kBinary ? tri_test_binary(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2)
+                                      : tri_test(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2);
+        if (accepted) {
             s.res.prim = __float_as_uint(v0.w);
             s.res.t = t;
             s.res.b1 = b1;
@@ -226,11 +261,11 @@ AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, ui
     uint32_t slot = p ^ s.oct;
     uint32_t child = s.ngroup.x + __popc(s.ngroup.y & 0xffu & ((1u << slot) - 1u));
     if (s.ngroup.y & 0xff000000u) {
-        if (s.sp >= kTraversalStack) { err |= kErrStackOverflow; s.found = false; return true; }
+        if (s.sp >= (int)bvh.stackLimit) { err |= kErrStackOverflow; s.found = false; return true; }
         stack[s.sp++ * stride] = s.ngroup;
     }
     if (child >= bvh.nodeCount) { err |= kErrBadIndex; s.found = false; return true; }
-    if (++s.visits > kMaxVisits) { err |= kErrIterations; s.found = false; return true; }
+    if (++s.visits > bvh.maxVisits) { err |= kErrIterations; s.found = false; return true; }
     ++nodeVisits;
     const uint4* np = reinterpret_cast<const uint4*>(bvh.nodes + child);
     uint4 w0 = ldg4(np), w1 = ldg4(np + 1), w2 = ldg4(np + 2), w3 = ldg4(np + 3), w4 = ldg4(np + 4);
@@ -242,14 +277,14 @@ AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, ui
 
 // Traces one ray to completion. Returns true when something was hit
 // (closest: res filled; any: the first hit found).
-template <bool kAny>
+template <bool kAny, bool kBinary = false>
 AG_D bool trace(const BvhView& bvh, float3 o, float3 d, float tmin, float tmax, TraceResult& res, uint2* stack,
                 int stride, uint32_t& err, uint32_t& nodeVisits, uint32_t& triVisits)
 {
     RayState s;
     ray_init(s, o, d, tmin, tmax);
     if (bvh.nodeCount != 0) {
-        while (!ray_step<kAny>(bvh, s, stack, stride, err, nodeVisits, triVisits)) {
+        while (!ray_step<kAny, kBinary>(bvh, s, stack, stride, err, nodeVisits, triVisits)) {
         }
     }
     if (!s.found) {

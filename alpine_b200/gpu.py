@@ -28,6 +28,8 @@ MISS = 0xFFFFFFFF
 NOALLOC_MAX_RAYS = 65536
 GUIDE_KERNEL_WARP_MMA = 0
 GUIDE_KERNEL_TENSOR_MEMORY = 1
+TRIANGLE_TEST_WIDE_BVH = 0
+TRIANGLE_TEST_BINARY_BVH = 1
 
 
 class GpuError(RuntimeError):
@@ -57,6 +59,10 @@ class RenderOptions(C.Structure):
                 ("guide_steps_per_wave", C.c_uint32), ("guide_min_roughness", C.c_float),
                 ("guide_train_steps", C.c_uint32), ("cuda_graph", C.c_uint32),
                 ("guide_max_depth", C.c_uint32)]
+
+
+class TraversalOptions(C.Structure):
+    _fields_ = [("triangle_test", C.c_uint32), ("max_visits", C.c_uint32), ("stack_limit", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -103,6 +109,7 @@ def lib():
         L.alpine_gpu_occluded_device.argtypes = [vp, vp, C.c_uint64, vp, vp]
         L.alpine_gpu_synchronize.argtypes = [vp]
         L.alpine_gpu_trace_noalloc.argtypes = [vp, vp, C.c_uint64, vp]
+        L.alpine_gpu_set_traversal_options.argtypes = [vp, C.POINTER(TraversalOptions)]
         f3 = C.POINTER(C.c_float)
         u32p = C.POINTER(C.c_uint32)
         L.alpine_gpu_set_materials.argtypes = [vp, vp, C.c_uint32]
@@ -250,6 +257,12 @@ class Context:
     def occluded_device(self, rays_ptr: int, n: int, occ_ptr: int, stream: int = 0):
         self._check(self.L.alpine_gpu_occluded_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr),
                                                       C.c_void_p(stream or None)))
+
+    def set_traversal_options(self, triangle_test=TRIANGLE_TEST_WIDE_BVH, max_visits=0, stack_limit=0):
+        """Triangle rule of every traversal (the reference's 8-wide or binary
+        BVH) and the per-ray device-side limits (0 = defaults)."""
+        o = TraversalOptions(triangle_test, max_visits, stack_limit)
+        self._check(self.L.alpine_gpu_set_traversal_options(self.h, C.byref(o)))
 
     def traversal_stats(self, rays_ptr: int, n: int, any_hit: bool):
         """(wide nodes fetched, triangles tested) summed over n device rays."""

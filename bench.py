@@ -159,6 +159,17 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def ref_build_label():
+    """Which build of the reference the timed CPU arms use."""
+    import oracle
+
+    name = os.path.basename(oracle.timing_build())
+    flags = {"libalpine_ref_fast_v4.so": "-O3 -march=x86-64-v4 (AVX-512) -mtune=native, FMA contraction",
+             "libalpine_ref_fast_v3.so": "-O3 -march=x86-64-v3 (AVX2) -mtune=native, FMA contraction",
+             "libalpine_ref.so": "-O3 -march=x86-64-v3 -ffp-contract=off (parity build)"}
+    return f"{name}: {flags.get(name, '?')}"
+
+
 def cpu_baseline(verts, idx, closest, shadow, budget_s):
     """The reference's own WideBvh (oracle/_ref: src/accelerators/wide_bvh.cpp
     with the ISPC kernels restated in C++) on all host cores, on a bounded
@@ -168,7 +179,7 @@ def cpu_baseline(verts, idx, closest, shadow, budget_s):
     if not oracle.ref_available():
         return None
     ncores = os.cpu_count() or 1
-    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx)
+    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx, timing=True)
     rng = np.random.default_rng(7)
     order = rng.permutation(closest.shape[0])
     chunk = 16384
@@ -183,6 +194,7 @@ def cpu_baseline(verts, idx, closest, shadow, budget_s):
         done += 2 * chunk
         k += 1
     return {"value": done / t_total / 1e6, "unit": UNIT, "cores": ncores, "kind": "reference",
+            "build": ref_build_label(),
             "sample": f"{done // 2} random rays of the workload (primary+incoherent mix), closest + any hit each; "
                       f"reference WideBvh build {acc.build_ms:.0f} ms (not in the rate)",
             "seconds": t_total}
@@ -302,7 +314,7 @@ def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
 
     if not oracle.ref_available():
         return None
-    r = oracle.RefRenderer(W, H, GUIDING_DEPTH, accelerator=oracle.RefRenderer.ACC_WIDE_BVH)
+    r = oracle.RefRenderer(W, H, GUIDING_DEPTH, accelerator=oracle.RefRenderer.ACC_WIDE_BVH, timing=True)
     t0 = time.perf_counter()
     scenes.load_scene(r, scene, W, H)
     load_s = time.perf_counter() - t0
@@ -313,7 +325,7 @@ def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
     dt = time.perf_counter() - t0
     r.close()
     rate = spp * W * H / dt
-    return {"samples_per_s": rate, "cores": os.cpu_count() or 1, "kind": "reference",
+    return {"samples_per_s": rate, "cores": os.cpu_count() or 1, "kind": "reference", "build": ref_build_label(),
             "sample": f"{spp} spp at {W}x{H} after 1 warm-up spp; scene load + BVH build {load_s:.1f} s",
             "projected_time_to_target_s": (plain_spp * W * H / rate) if plain_spp else None}
 
@@ -374,7 +386,7 @@ def room_benchmark(device, W=256, H=256, spp=16, depth=8, repeats=5):
     out["gpu"]["samples_per_s"] = rate
     out["gpu"]["samples_per_s_rr3"] = gpu_rate(3)[0]
     if oracle.ref_available():
-        r = oracle.RefRenderer(W, H, depth, accelerator=oracle.RefRenderer.ACC_BVH)
+        r = oracle.RefRenderer(W, H, depth, accelerator=oracle.RefRenderer.ACC_BVH, timing=True)
         scenes.load_scene(r, scene, W, H)
         r.build_light_sampler(gpu.SAMPLER_POWER)
         r.reset_accumulation()
@@ -385,6 +397,7 @@ def room_benchmark(device, W=256, H=256, spp=16, depth=8, repeats=5):
         r.close()
         rmean = float(a[..., :3].mean() / n)
         out["cpu_reference"] = {"samples_per_s": W * H * spp / dt, "cores": os.cpu_count() or 1, "kind": "reference",
+                                "build": ref_build_label(),
                                 "sample": f"one render of {spp} spp (binary BVH, quad light as a harness Light)"}
         out["speedup_vs_cpu_reference"] = rate / out["cpu_reference"]["samples_per_s"]
         out["image_mean"] = {"gpu": gmean, "reference": rmean, "rel_diff": abs(gmean - rmean) / rmean}
@@ -446,6 +459,60 @@ def many_lights_benchmark(device, spp=4, cmp_res=(480, 270), cmp_spp=64, ref_spp
     return out
 
 
+def traversal_split(ctx, d_closest, d_shadow, d_hits, d_occ, stream, half, reps=5):
+    """Device Mrays/s of each half of the workload on its own: the 2,097,152
+    coherent primary rays and the 2,097,152 incoherent rays, closest hit and
+    any hit, each timed with CUDA events on the launching stream (mean of
+    `reps` launches after one warm-up)."""
+    import torch
+
+    sp = stream.cuda_stream
+    out = {}
+    for name, off in (("coherent", 0), ("incoherent", half)):
+        for kind in ("closest", "any"):
+            src = (d_closest if kind == "closest" else d_shadow).data_ptr() + off * 32
+            if kind == "closest":
+                dst = d_hits.data_ptr() + off * 16
+
+                def launch():
+                    ctx.trace_device(src, half, dst, sp)
+            else:
+                dst = d_occ.data_ptr() + off
+
+                def launch():
+                    ctx.occluded_device(src, half, dst, sp)
+            launch()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(stream)
+            for _ in range(reps):
+                launch()
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            out[f"{name}_{kind}"] = half * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e6
+    ctx.synchronize()
+    return out
+
+
+def l2_copy_bandwidth(stream, mib=24, reps=200):
+    """GB/s (read + write bytes) of a device copy whose source and
+    destination stay resident in the 126 MB L2: the denominator for kernels
+    whose working set is served from L2."""
+    import torch
+
+    n = mib * (1 << 20) // 4
+    a = torch.ones(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        b.copy_(a)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    return 2 * a.numel() * 4 * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU WideBvh on the host cores, same
     metric; each step is a 131,072-query sample of the workload."""
@@ -457,7 +524,7 @@ def run_reference(args):
 
     verts, idx, closest, shadow = scenes.traversal_workload()
     ncores = os.cpu_count() or 1
-    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx)
+    acc = oracle.RefAccel(oracle.RefAccel.WIDE_BVH, verts, idx, timing=True)
     rng = np.random.default_rng(11)
     per = 65536
     times = []
@@ -479,6 +546,7 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "sample_per_step": f"{per} closest + {per} any-hit queries",
                    "accelerator": "reference WideBvh (8-wide, ISPC kernels restated in C++), CPU"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "reference",
+                         "build": ref_build_label(),
                          "sample": f"{per} closest + {per} any-hit random rays of the workload per step",
                          "build_ms": acc.build_ms},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -575,6 +643,8 @@ def run_ours(args):
             print(json.dumps({"profile": True, "closest_ms": closest_ms, "any_ms": any_ms}), flush=True)
         ctx.close()
         return
+    split = traversal_split(ctx, d_closest, d_shadow, d_hits, d_occ, stream, n // 2)
+    l2_gbs = l2_copy_bandwidth(stream)
     # end to end through the C ABI with pinned host buffers
     h_closest = torch.from_numpy(closest).pin_memory().numpy()
     h_shadow = torch.from_numpy(shadow).pin_memory().numpy()
@@ -599,6 +669,12 @@ def run_ours(args):
     roofline = {
         "bound": "hbm", "kernel": "k_trace<closest>", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_from_profile(),
+        "traffic_source": "DRAM bytes of one full-size launch from the committed ncu summary of this workload "
+                          "(profiles/trace_closest_soup1M.md); not captured in this run",
+        "limiter": "instruction issue and SIMD divergence: the BVH (about 57 MB) is served from L2, so DRAM "
+                   "traffic is a small fraction of the algorithmic bytes",
+        "l2": {"achieved": achieved, "peak": l2_gbs, "frac": achieved / l2_gbs if l2_gbs else None,
+               "peak_source": "L2-resident device copy (2 x 24 MiB) measured in this run"},
         "algorithmic_bytes_per_launch": bytes_closest,
         "per_ray": {"node_visits": nv_c / n, "tri_tests": tv_c / n, "bytes": bytes_closest / n},
         "any_hit": {"ms": any_ms, "achieved_gbs": bytes_any / (any_ms / 1e3) / 1e9,
@@ -637,6 +713,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * RAY_BYTES,
                     "d2h_bytes_per_step": n * (HIT_BYTES + 1), "ms_per_step": e2e_ms},
             "roofline": roofline,
+            "traversal_split_mrays_s": split,
             "cpu_baseline": base,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),

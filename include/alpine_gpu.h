@@ -158,13 +158,45 @@ ALPINE_GPU_API int alpine_gpu_occluded_device(alpine_gpu_ctx* ctx, const alpine_
  * buffers as needed; this variant stages through one fixed 3 MiB array in
  * device memory that every GPU loading the library holds until exit. Larger
  * batches are rejected with ALPINE_GPU_ERR_INVALID_ARGUMENT. The first call
- * on a device looks up the array's device address; make it before any stream
- * capture. All calls share the array, so calls are serialised inside the
- * library; calls that overlapped on one device would race. Blocks until done.
- * Results are identical to alpine_gpu_trace. */
+ * on a device looks up the array's device address; with CUDA's lazy module
+ * loading that first call may also load the module that holds the array. The
+ * call is synchronous (it waits for its own copies) and copies through host
+ * memory, so it must never be made while the context's stream, or a stream it
+ * depends on, is being captured. All calls share the array, so calls are
+ * serialised inside the library; calls that overlapped on one device would
+ * race. Results are identical to alpine_gpu_trace. */
 #define ALPINE_GPU_NOALLOC_MAX_RAYS 65536
 ALPINE_GPU_API int alpine_gpu_trace_noalloc(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count,
                                             alpine_gpu_hit* hits);
+
+/* Traversal options (no counterpart in the reference's API; default: all 0).
+ * triangle_test selects the hit rule of every traversal of the context
+ *   (queries and rendering), i.e. which reference accelerator's answers the
+ *   GPU reproduces bit for bit:
+ *   WIDE_BVH (0): the reference's 8-wide BVH and its ISPC triangle kernel
+ *     (src/accelerators/wide_bvh.cpp:487-619, src/ispc/triangle.ispc:46-87):
+ *     |det| >= 1e-6, t, b1, b2 by one reciprocal of det, b1 + b2 <= 1;
+ *   BINARY_BVH (1): the reference's binary BVH (AcceleratorType::Bvh,
+ *     Primitive::intersect, src/accelerators/bvh_common.cpp:66-103):
+ *     |det| >= FLT_EPSILON, t, b1, b2 by division, b1 <= 1, b2 <= 1 - b1.
+ *   The two rules disagree on near-degenerate triangles (about 0.2% of
+ *   incoherent rays on a dense soup).
+ * max_visits: per-ray cap on wide nodes fetched; 0 = 65536. A ray that reaches
+ *   it ends as a miss and the call reports ALPINE_GPU_ERR_LIMIT.
+ * stack_limit: traversal stack entries a ray may use, 1-24; 0 = 24. A ray that
+ *   needs more ends as a miss and the call reports ALPINE_GPU_ERR_LIMIT. The
+ *   reference's traversals stop on an assert instead
+ *   (src/accelerators/bvh.cpp:231, wide_bvh.cpp:604).
+ * The two limits exist so that the device-side failure path can be exercised
+ * on purpose; the defaults are never reached by a BVH this library builds. */
+#define ALPINE_GPU_TRIANGLE_TEST_WIDE_BVH 0u
+#define ALPINE_GPU_TRIANGLE_TEST_BINARY_BVH 1u
+typedef struct alpine_gpu_traversal_options {
+    uint32_t triangle_test;
+    uint32_t max_visits;
+    uint32_t stack_limit;
+} alpine_gpu_traversal_options;
+ALPINE_GPU_API int alpine_gpu_set_traversal_options(alpine_gpu_ctx* ctx, const alpine_gpu_traversal_options* options);
 
 /* Traversal statistics for `count` rays in DEVICE memory: runs the same
  * traversal as alpine_gpu_trace_device / alpine_gpu_occluded_device (any_hit

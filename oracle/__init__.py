@@ -8,7 +8,11 @@ ctypes bindings to two CPU libraries built by ``oracle/Makefile``:
   src/utils/bounding_box.h:23-56), canonical brute-force / BVH-accelerated
   closest and any-hit queries and an FP64 Moller-Trumbore.
 * ``_ref/libalpine_ref.so`` -- the unmodified reference sources (Bvh, WideBvh,
-  integrator) behind a C-ABI harness (``refshim/ref_harness.cpp``).
+  integrator) behind a C-ABI harness (``refshim/ref_harness.cpp``), built for
+  parity (IEEE FP32, no FMA contraction).
+* ``_ref/libalpine_ref_fast_v3.so`` / ``_v4.so`` -- the same sources built for
+  speed (FMA contraction, AVX2 / AVX-512); used only by the timed CPU arms
+  (``timing=True``), never for parity.
 
 Only the tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline and
 reference arms use this package. The product (``alpine_b200``) never imports it.
@@ -23,6 +27,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 REF_SO = os.path.join(_HERE, "_ref", "libalpine_ref.so")
+REF_FAST_SO = {3: os.path.join(_HERE, "_ref", "libalpine_ref_fast_v3.so"),
+               4: os.path.join(_HERE, "_ref", "libalpine_ref_fast_v4.so")}
 
 TRI_ISPC = 0
 TRI_PRIM = 1
@@ -33,7 +39,7 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 
 _lib = None
-_ref = None
+_ref = {}
 
 
 def lib():
@@ -70,13 +76,35 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
-def ref():
-    """The compiled reference (``oracle/_ref/libalpine_ref.so``)."""
-    global _ref
-    if _ref is None:
-        if not os.path.exists(REF_SO):
-            raise RuntimeError(f"{REF_SO} missing: run `make -C oracle ref` where the reference tree exists")
-        L = C.CDLL(REF_SO)
+def _host_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = line.split()
+                    return all(x in flags for x in ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"))
+    except OSError:
+        pass
+    return False
+
+
+def timing_build() -> str:
+    """Path of the speed build of the reference for this host (AVX-512 when
+    the host has it), else the parity build."""
+    for level in ((4, 3) if _host_has_avx512() else (3,)):
+        if os.path.exists(REF_FAST_SO[level]):
+            return REF_FAST_SO[level]
+    return REF_SO
+
+
+def ref(timing: bool = False):
+    """The compiled reference: the parity build (``oracle/_ref/libalpine_ref.so``)
+    or, with timing=True, the speed build for this host."""
+    path = timing_build() if timing else REF_SO
+    if path not in _ref:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        L = C.CDLL(path)
         L.ref_accel_create.argtypes = [C.c_int, C.c_uint64]
         L.ref_accel_create.restype = C.c_void_p
         L.ref_accel_add_mesh.argtypes = [C.c_void_p, _f32p, C.c_uint32, _u32p, C.c_uint32]
@@ -114,8 +142,8 @@ def ref():
         L.ref_render_read_sampler_state.argtypes = [_u32p]
         L.ref_material_sample.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, _f32p, _f32p, _f32p, _u8p]
         L.ref_material_eval.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, _f32p, _f32p]
-        _ref = L
-    return _ref
+        _ref[path] = L
+    return _ref[path]
 
 
 # ---------------------------------------------------------------------------
@@ -214,8 +242,8 @@ class RefRenderer:
 
     ACC_BVH, ACC_WIDE_BVH = 0, 1
 
-    def __init__(self, width, height, max_depth, accelerator=ACC_BVH, arena_bytes=1 << 30):
-        self.L = ref()
+    def __init__(self, width, height, max_depth, accelerator=ACC_BVH, arena_bytes=1 << 30, timing=False):
+        self.L = ref(timing)
         self.w, self.h = width, height
         if not self.L.ref_render_init(width, height, max_depth, arena_bytes):
             raise RuntimeError("ref_render_init failed")
@@ -368,8 +396,8 @@ class RefAccel:
     BVH = 0
     WIDE_BVH = 1
 
-    def __init__(self, kind, verts, idx, arena_bytes=1 << 30):
-        self.L = ref()
+    def __init__(self, kind, verts, idx, arena_bytes=1 << 30, timing=False):
+        self.L = ref(timing)
         self.h = self.L.ref_accel_create(kind, arena_bytes)
         v = np.ascontiguousarray(verts, np.float32).reshape(-1)
         i = np.ascontiguousarray(idx, np.uint32).reshape(-1)

@@ -25,8 +25,10 @@ W = H = 40
 DEPTH = 8
 
 
-def _gpu_ctx(scene, sampler_kind, rng_mode, w=W, h=H, depth=DEPTH, **opts):
+def _gpu_ctx(scene, sampler_kind, rng_mode, w=W, h=H, depth=DEPTH, triangle_test=gpu.TRIANGLE_TEST_WIDE_BVH,
+             **opts):
     ctx = gpu.Context(0, w, h, depth)
+    ctx.set_traversal_options(triangle_test)
     scenes.load_scene(ctx, scene, w, h)
     ctx.build_light_sampler(sampler_kind)
     ctx.set_render_options(sampler=rng_mode, **opts)
@@ -34,23 +36,26 @@ def _gpu_ctx(scene, sampler_kind, rng_mode, w=W, h=H, depth=DEPTH, **opts):
     return ctx
 
 
-def _ref(scene, sampler_kind, w=W, h=H, depth=DEPTH):
-    # WideBvh: the reference traversal whose triangle test (triangle.ispc) the
-    # GPU reproduces bit-exactly
-    r = oracle.RefRenderer(w, h, depth, accelerator=oracle.RefRenderer.ACC_WIDE_BVH)
+def _ref(scene, sampler_kind, w=W, h=H, depth=DEPTH, accelerator=oracle.RefRenderer.ACC_WIDE_BVH):
+    # WideBvh by default: the reference traversal whose triangle test
+    # (triangle.ispc) the GPU's default rule reproduces bit-exactly; ACC_BVH
+    # pairs with the GPU's binary-BVH rule
+    r = oracle.RefRenderer(w, h, depth, accelerator=accelerator)
     scenes.load_scene(r, scene, w, h)
     r.build_light_sampler(sampler_kind)
     r.reset_accumulation()
     return r
 
 
-def _stream_compare(scene, sampler_kind, spp=1, depth=DEPTH):
-    ref = _ref(scene, sampler_kind, depth=depth)
+def _stream_compare(scene, sampler_kind, spp=1, depth=DEPTH, binary=False):
+    acc = oracle.RefRenderer.ACC_BVH if binary else oracle.RefRenderer.ACC_WIDE_BVH
+    ref = _ref(scene, sampler_kind, depth=depth, accelerator=acc)
     ref.render(spp)
     ra, rn = ref.read_accumulation()
     rs = ref.read_sampler_state()
     ref.close()
-    ctx = _gpu_ctx(scene, sampler_kind, gpu.RNG_REFERENCE_STREAM, depth=depth)
+    mode = gpu.TRIANGLE_TEST_BINARY_BVH if binary else gpu.TRIANGLE_TEST_WIDE_BVH
+    ctx = _gpu_ctx(scene, sampler_kind, gpu.RNG_REFERENCE_STREAM, depth=depth, triangle_test=mode)
     ctx.render(spp)
     ga, gn = ctx.read_accumulation(W, H)
     gs = ctx.read_sampler_state(W, H)
@@ -70,6 +75,16 @@ def _stream_compare(scene, sampler_kind, spp=1, depth=DEPTH):
 def test_stream_parity_room_power_sampler():
     """One sample per pixel, depth 8: the GPU follows the reference path by path."""
     close, same, mean_rel, aov = _stream_compare(scenes.room_scene(), gpu.SAMPLER_POWER)
+    assert close > 0.95 and same > 0.95
+    assert mean_rel < 0.02
+    assert aov < 1e-3
+
+
+def test_stream_parity_room_binary_bvh():
+    """The room as the reference renders it with its binary BVH
+    (AcceleratorType::Bvh, the accelerator of the small-room configuration):
+    the GPU's binary-BVH triangle rule follows it path by path."""
+    close, same, mean_rel, aov = _stream_compare(scenes.room_scene(), gpu.SAMPLER_POWER, binary=True)
     assert close > 0.95 and same > 0.95
     assert mean_rel < 0.02
     assert aov < 1e-3
@@ -174,3 +189,46 @@ def test_stream_parity_city(kind):
     close, same, mean_rel, _ = _stream_compare(scene, kind, spp=2, depth=3)
     assert close > 0.95 and same > 0.97
     assert mean_rel < 0.02
+
+
+def test_fp64_accumulators_match_fp32_and_reference():
+    """FP64 per-pixel accumulators (for convergence runs): the same samples as
+    the FP32 path (counter RNG, same seed) summed in double precision. The
+    sums agree with the FP32 sums to FP32 rounding, the FP64 read-back of the
+    FP32 path and the FP32 read-back of the FP64 path are consistent, and the
+    FP64 image passes the z-test against the reference renderer."""
+    scene = scenes.room_scene(seed=4)
+    w = h = 24
+    sums = {}
+    for fp64 in (False, True):
+        ctx = _gpu_ctx(scene, gpu.SAMPLER_POWER, gpu.RNG_COUNTER, w, h, seed=5, accumulate_fp64=fp64)
+        for _ in range(4):
+            ctx.render(256)
+        s64, n64 = ctx.read_accumulation(w, h, fp64=True)
+        s32, n32 = ctx.read_accumulation(w, h)
+        ctx.close()
+        assert n64 == n32 == 1024
+        if fp64:
+            assert (s32 == s64.astype(np.float32)).all()
+        else:
+            assert (s64 == s32.astype(np.float64)).all()
+        sums[fp64] = s64
+    a, b = sums[False][..., :3], sums[True][..., :3]
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * np.abs(b).mean())
+    print(f"fp32 vs fp64 sums: max rel diff {rel.max():.2e}, mean {rel.mean():.2e}")
+    assert rel.max() < 1e-3 and rel.mean() < 1e-5
+    assert not (a == b).all()  # the FP64 path does sum differently
+    ref = _ref(scene, gpu.SAMPLER_POWER, w, h)
+    ref.render(256)
+    ra, rn = ref.read_accumulation()
+    ref.close()
+    rmean = ra[..., :3].astype(np.float64) / rn
+    gb = _gpu_batches(scene, gpu.SAMPLER_POWER, w, h, 16, 256, seed=6)
+    var1 = gb.var(0, ddof=1) * 256
+    gmean = b[..., :3] / 1024
+    se = np.sqrt(var1 / 256 + var1 / 1024)
+    ok = se > 1e-7
+    z = (rmean - gmean)[ok] / se[ok]
+    print(f"fp64 z-test: |z|>5 fraction {(np.abs(z) > 5).mean():.4f}, mean z {z.mean():.3f}")
+    assert (np.abs(z) > 5).mean() < 0.02
+    assert abs(z.mean()) < 0.25
