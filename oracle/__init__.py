@@ -10,6 +10,9 @@ ctypes bindings to two CPU libraries built by ``oracle/Makefile``:
 * ``_ref/libalpine_ref.so`` -- the unmodified reference sources (Bvh, WideBvh,
   integrator) behind a C-ABI harness (``refshim/ref_harness.cpp``), built for
   parity (IEEE FP32, no FMA contraction).
+* ``_ref/libalpine_ref_plugin.so`` -- the parity build plus the GPU plug-in a
+  maintainer adds to the reference (``alpine_b200/plugin``: GpuAccelerator
+  and the GpuBackend render branch), for the boundary tests (``plugin=True``).
 * ``_ref/libalpine_ref_fast_v3.so`` / ``_v4.so`` -- the same sources built for
   speed (FMA contraction, AVX2 / AVX-512); used only by the timed CPU arms
   (``timing=True``), never for parity.
@@ -27,6 +30,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 REF_SO = os.path.join(_HERE, "_ref", "libalpine_ref.so")
+REF_PLUGIN_SO = os.path.join(_HERE, "_ref", "libalpine_ref_plugin.so")
 REF_FAST_SO = {3: os.path.join(_HERE, "_ref", "libalpine_ref_fast_v3.so"),
                4: os.path.join(_HERE, "_ref", "libalpine_ref_fast_v4.so")}
 
@@ -97,10 +101,15 @@ def timing_build() -> str:
     return REF_SO
 
 
-def ref(timing: bool = False):
-    """The compiled reference: the parity build (``oracle/_ref/libalpine_ref.so``)
-    or, with timing=True, the speed build for this host."""
-    path = timing_build() if timing else REF_SO
+def plugin_available() -> bool:
+    return os.path.exists(REF_PLUGIN_SO)
+
+
+def ref(timing: bool = False, plugin: bool = False):
+    """The compiled reference: the parity build (``oracle/_ref/libalpine_ref.so``),
+    with timing=True the speed build for this host, with plugin=True the
+    parity build with the GPU plug-in installed."""
+    path = REF_PLUGIN_SO if plugin else (timing_build() if timing else REF_SO)
     if path not in _ref:
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
@@ -113,6 +122,12 @@ def ref(timing: bool = False):
         L.ref_accel_build.restype = C.c_double
         L.ref_accel_intersect.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_int, _u32p, _f32p, _f32p, _f32p]
         L.ref_accel_occluded.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_int, _u8p]
+        L.ref_accel_update_vertices.argtypes = [C.c_void_p, C.c_uint32, _f32p, C.c_uint32]
+        L.ref_accel_intersect_ng.argtypes = [C.c_void_p, _f32p, C.c_uint64, C.c_int, _u32p, _f32p, _f32p, _f32p,
+                                             _f32p, _u8p]
+        if plugin:
+            L.ref_render_gpu_branch.argtypes = [C.c_int, C.c_uint32, C.c_int]
+            L.ref_render_gpu_branch.restype = C.c_int
         L.ref_accel_destroy.argtypes = [C.c_void_p]
         L.ref_render_init.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64]
         L.ref_render_init.restype = C.c_int
@@ -241,13 +256,21 @@ class RefRenderer:
     harness: one process-wide instance, as the reference is a singleton."""
 
     ACC_BVH, ACC_WIDE_BVH = 0, 1
+    # plug-in build only: the GpuAccelerator installed as the Alpine's
+    # accelerator (8-wide / binary triangle rule)
+    ACC_GPU, ACC_GPU_BINARY = 3, 4
 
-    def __init__(self, width, height, max_depth, accelerator=ACC_BVH, arena_bytes=1 << 30, timing=False):
-        self.L = ref(timing)
+    def __init__(self, width, height, max_depth, accelerator=ACC_BVH, arena_bytes=1 << 30, timing=False,
+                 plugin=False, gpu_branch=False, seed=0):
+        """plugin: use the plug-in build; gpu_branch: route the Alpine
+        methods through the GpuBackend render branch (counter RNG, `seed`)."""
+        self.L = ref(timing, plugin or gpu_branch)
         self.w, self.h = width, height
         if not self.L.ref_render_init(width, height, max_depth, arena_bytes):
             raise RuntimeError("ref_render_init failed")
         self.L.ref_render_reset_scene(accelerator)
+        if gpu_branch and not self.L.ref_render_gpu_branch(1, seed, int(accelerator == self.ACC_BVH)):
+            raise RuntimeError("ref_render_gpu_branch failed")
 
     def add_mesh(self, verts, idx, normals=None, tri_material=None, materials=((0, (0.5, 0.5, 0.5), 1.0),)):
         v = np.ascontiguousarray(verts, np.float32).reshape(-1)
@@ -321,7 +344,10 @@ class RefRenderer:
         self.L.ref_render_reset_accumulation()
 
     def render(self, spp):
-        return self.L.ref_render(spp)
+        ms = self.L.ref_render(spp)
+        if ms < 0:
+            raise RuntimeError("render failed (GPU render branch)")
+        return ms
 
     def read_accumulation(self):
         out = np.empty((self.h, self.w, 9), np.float32)
@@ -395,9 +421,12 @@ class RefAccel:
 
     BVH = 0
     WIDE_BVH = 1
+    # plug-in build only: the GpuAccelerator (8-wide / binary triangle rule)
+    GPU = 2
+    GPU_BINARY = 3
 
-    def __init__(self, kind, verts, idx, arena_bytes=1 << 30, timing=False):
-        self.L = ref(timing)
+    def __init__(self, kind, verts, idx, arena_bytes=1 << 30, timing=False, plugin=False):
+        self.L = ref(timing, plugin or kind >= self.GPU)
         self.h = self.L.ref_accel_create(kind, arena_bytes)
         v = np.ascontiguousarray(verts, np.float32).reshape(-1)
         i = np.ascontiguousarray(idx, np.uint32).reshape(-1)
@@ -419,6 +448,26 @@ class RefAccel:
         occ = np.empty(rays.shape[0], np.uint8)
         self.L.ref_accel_occluded(self.h, rays.reshape(-1), rays.shape[0], nthreads, occ)
         return occ
+
+    def update_vertices(self, shape, verts):
+        """Mesh::update's path: write the shape's vertex buffer
+        (getVertexBuffer), updateShape, then updateScene (rebuild)."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.L.ref_accel_update_vertices(self.h, shape, v, v.size // 3)
+
+    def intersect_ng(self, rays, nthreads=0):
+        """intersect() plus Intersection::ng (float[n, 3]) and whether the hit
+        carries the mesh's shape pointer."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        prim = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        b1 = np.empty(n, np.float32)
+        b2 = np.empty(n, np.float32)
+        ng = np.empty((n, 3), np.float32)
+        ok = np.empty(n, np.uint8)
+        self.L.ref_accel_intersect_ng(self.h, rays.reshape(-1), n, nthreads, prim, t, b1, b2, ng.reshape(-1), ok)
+        return prim, t, b1, b2, ng, ok.astype(bool)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -16,6 +16,16 @@
 //                   mTotalSamples; src/alpine.cpp:109-112) can be read back.
 //                   No reference file is modified.
 //
+// Built a second time with ALPINE_GPU_PLUGIN defined (oracle/_ref/
+// libalpine_ref_plugin.so), the harness also installs the GPU plug-in that a
+// maintainer adds to the reference (alpine_b200/plugin): accelerator kinds
+// 2 / 3 (ref_accel_create) and AcceleratorType values 3 / 4
+// (ref_render_reset_scene) are the GpuAccelerator with the 8-wide / binary
+// triangle rule, as a new `case AcceleratorType::Gpu` in Alpine::resetScene
+// would create it; ref_render_gpu_branch switches the Alpine methods to the
+// GpuBackend render branch, each entry point below forwarding to it as the
+// maintainer's branch in alpine.cpp would.
+//
 // The reference's loaders need tinyobjloader / tinygltf / stb, which are not
 // vendored; this harness therefore defines loadObj/loadGltf/loadHdr
 // (src/loaders/file_loader.h:10-12): loadObj is a minimal reader for the
@@ -59,6 +69,10 @@
 
 #include <accelerators/bvh.h>
 #include <accelerators/wide_bvh.h>
+#ifdef ALPINE_GPU_PLUGIN
+#include <gpu_accelerator.h>
+#include <gpu_backend.h>
+#endif
 #include <materials/conductor.h>
 #include <materials/dielectric.h>
 #include <shapes/mesh.h>
@@ -279,12 +293,38 @@ make_ref_material(const float* r)
     return std::make_shared<Dielectric>(float2(r[4]), bc, nullptr, nullptr);
 }
 
+#ifdef ALPINE_GPU_PLUGIN
+// The GPU render branch (GpuBackend) when switched on, and the material
+// records of the meshes forwarded to it.
+static std::unique_ptr<GpuBackend> sGpu;
+
+static alpine_gpu_material
+to_gpu_material(const float* r)
+{
+    alpine_gpu_material m{};
+    m.kind = r[0] == 1.0f ? ALPINE_GPU_MATERIAL_CONDUCTOR : ALPINE_GPU_MATERIAL_DIELECTRIC;
+    m.base_color[0] = r[1];
+    m.base_color[1] = r[2];
+    m.base_color[2] = r[3];
+    m.roughness = r[4];
+    return m;
+}
+#endif
+
 extern "C" {
-// kind: 0 = Bvh (binary), 1 = WideBvh (8-wide, ISPC kernels restated).
+// kind: 0 = Bvh (binary), 1 = WideBvh (8-wide, ISPC kernels restated); in the
+// plug-in build 2 / 3 = GpuAccelerator with the 8-wide / binary triangle rule.
 void*
 ref_accel_create(int kind, uint64_t arenaBytes)
 {
     auto* h = new RefAccel;
+#ifdef ALPINE_GPU_PLUGIN
+    if (kind == 2 || kind == 3)
+    {
+        h->acc = std::make_unique<GpuAccelerator>(kind == 3 ? GpuAccelerator::Rule::Binary : GpuAccelerator::Rule::Wide);
+        return h;
+    }
+#endif
     h->arena.resize(arenaBytes);
     if (kind == 1)
     {
@@ -306,6 +346,19 @@ ref_accel_add_mesh(void* hp, const float* verts, uint32_t nverts, const uint32_t
     std::vector<uint3> p(ntris);
     for (uint32_t i = 0; i < ntris; ++i) { p[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]); }
     return h->acc->appendMesh(v, p, &h->dummyShape);
+}
+
+// The path Mesh::update takes (src/shapes/mesh.cpp:29-55): new positions
+// written into the accelerator's vertex buffer of one shape, updateShape, then
+// Accelerator::updateScene (full rebuild).
+void
+ref_accel_update_vertices(void* hp, uint32_t shape, const float* verts, uint32_t nverts)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    auto* vb = static_cast<float3*>(h->acc->getVertexBuffer(shape));
+    for (uint32_t i = 0; i < nverts; ++i) { vb[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    h->acc->updateShape(shape);
+    h->acc->updateScene();
 }
 
 // Returns the wall time of Accelerator::updateScene (full build) in ms.
@@ -346,6 +399,25 @@ ref_accel_intersect(void* hp, const float* rays, uint64_t n, int nthreads,
     });
 }
 
+// ref_accel_intersect plus the shapePtr check and the geometric normal of
+// every hit (Intersection::shapePtr / ng; ng = 0 on a miss). shape_ok[i] = 1
+// when the hit reports the harness's dummy shape pointer.
+void
+ref_accel_intersect_ng(void* hp, const float* rays, uint64_t n, int nthreads,
+    uint32_t* prim, float* t, float* b1, float* b2, float* ng, uint8_t* shape_ok)
+{
+    auto* h = static_cast<RefAccel*>(hp);
+    parallelFor(n, nthreads, [&](uint64_t i) {
+        auto isect = h->acc->intersect(makeRay(rays + 8 * i));
+        prim[i] = isect ? isect->primId : 0xffffffffu;
+        t[i] = isect ? isect->t : FLT_MAX;
+        b1[i] = isect ? isect->barycentric.x : 0.0f;
+        b2[i] = isect ? isect->barycentric.y : 0.0f;
+        for (int k = 0; k < 3; ++k) { ng[3 * i + k] = isect ? isect->ng[k] : 0.0f; }
+        shape_ok[i] = isect && isect->shapePtr == &h->dummyShape ? 1 : 0;
+    });
+}
+
 // intersectAny(ray, tFar = tmax) for each ray; writes 1 when occluded.
 void
 ref_accel_occluded(void* hp, const float* rays, uint64_t n, int nthreads, uint8_t* occluded)
@@ -367,11 +439,50 @@ ref_accel_destroy(void* hp)
 int
 ref_render_init(uint32_t width, uint32_t height, uint32_t maxDepth, uint64_t arenaBytes)
 {
+#ifdef ALPINE_GPU_PLUGIN
+    sGpu.reset();
+#endif
     if (sAlpine) { shutdown(); }
     return initialize(static_cast<uint32_t>(arenaBytes), width, height, maxDepth) ? 1 : 0;
 }
 
-void ref_render_reset_scene(int acc) { resetScene(static_cast<AcceleratorType>(acc)); }
+// acc: AcceleratorType (0 = Bvh, 1 = WideBvh); in the plug-in build 3 / 4 =
+// the GpuAccelerator with the 8-wide / binary triangle rule.
+void
+ref_render_reset_scene(int acc)
+{
+#ifdef ALPINE_GPU_PLUGIN
+    if (acc == 3 || acc == 4)
+    {
+        resetScene(AcceleratorType::Bvh);
+        alpine::alpine().mAccelerator =
+            std::make_unique<GpuAccelerator>(acc == 4 ? GpuAccelerator::Rule::Binary : GpuAccelerator::Rule::Wide);
+        if (sGpu) { sGpu->resetScene(acc == 4); }
+        return;
+    }
+    if (sGpu) { sGpu->resetScene(acc == 0); }
+#endif
+    resetScene(static_cast<AcceleratorType>(acc));
+}
+
+#ifdef ALPINE_GPU_PLUGIN
+// Switches the render branch on (GpuBackend with the Alpine's framebuffer size
+// and path depth, counter RNG with `seed`) or off. Call right after
+// ref_render_reset_scene, before the scene is added. Returns 1 on success.
+int
+ref_render_gpu_branch(int enable, uint32_t seed, int binaryRule)
+{
+    sGpu.reset();
+    if (!enable) { return 1; }
+    auto& a = alpine::alpine();
+    sGpu = std::make_unique<GpuBackend>(a.mWidth, a.mHeight, a.mMaxDepth);
+    if (!sGpu->valid() || !sGpu->resetScene(binaryRule != 0)) { sGpu.reset(); return 0; }
+    alpine_gpu_render_options o{};
+    o.sampler = ALPINE_GPU_SAMPLER_COUNTER;
+    o.seed = seed;
+    return sGpu->setRenderOptions(o) ? 1 : 0;
+}
+#endif
 
 // Adds one mesh. materials: `nmat` records of 5 floats {kind, r, g, b, roughness}
 // with kind 0 = Dielectric, 1 = Conductor (the two material classes the loaders
@@ -399,6 +510,17 @@ ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, u
         if (m >= nmat) { return 0; }
         d.materials[i] = mats[m];
     }
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu)
+    {
+        std::vector<alpine_gpu_material> recs(nmat);
+        for (uint32_t m = 0; m < nmat; ++m) { recs[m] = to_gpu_material(materials + 5 * m); }
+        uint32_t base = sGpu->addMaterials(recs);
+        std::vector<uint32_t> ids(ntris);
+        for (uint32_t i = 0; i < ntris; ++i) { ids[i] = base + triMaterial[i]; }
+        if (sGpu->addMesh(d.vertices, d.normals, d.prims, d.normalPrims, ids) < 0) { return 0; }
+    }
+#endif
     auto mesh = std::make_shared<Mesh>(std::move(d), 0);
     auto& a = alpine::alpine();
     a.mScene.shapes.push_back(mesh);
@@ -502,6 +624,13 @@ ref_render_add_morph_mesh(const float* verts, uint32_t nverts, const uint32_t* t
         if (m >= nmat) { return 0; }
         d.materials[i] = mats[m];
     }
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu)
+    {
+        printf("ERROR: the GPU render branch of this harness does not forward morph targets\n");
+        return 0;
+    }
+#endif
     add_targets(d, nverts, vdeltas, normals ? ndeltas : nullptr, T);
     auto mesh = std::make_shared<Mesh>(std::move(d), T);
     auto& a = alpine::alpine();
@@ -513,36 +642,90 @@ ref_render_add_morph_mesh(const float* verts, uint32_t nverts, const uint32_t* t
 
 int ref_render_load_obj(const char* path) { return loadScene(path, FileType::Obj) ? 1 : 0; }
 
+#ifdef ALPINE_GPU_PLUGIN
+#define GPU_BRANCH(call) do { if (sGpu) { sGpu->call; } } while (0)
+#else
+#define GPU_BRANCH(call) do { } while (0)
+#endif
+
 void
 ref_render_add_disk_light(float power, const float* color, const float* pos, const float* target, float radius)
 {
     addDiskLight(power, color, pos, target, radius);
+    GPU_BRANCH(addDiskLight(power, color, pos, target, radius));
 }
 
-void ref_render_add_point_light(float power, const float* color, const float* pos) { addPointLight(power, color, pos); }
+void
+ref_render_add_point_light(float power, const float* color, const float* pos)
+{
+    addPointLight(power, color, pos);
+    GPU_BRANCH(addPointLight(power, color, pos));
+}
 
 void
 ref_render_add_quad_light(const float* radiance, const float* corner, const float* eu, const float* ev)
 {
     alpine::alpine().mScene.lights.push_back(std::make_shared<QuadLight>(
         float3(radiance), float3(corner), float3(eu), float3(ev)));
+    GPU_BRANCH(addQuadLight(radiance, corner, eu, ev));
 }
 void ref_render_update_scene(float time) { updateScene(time); }
-void ref_render_build_light_sampler(int type) { buildLightSampler(static_cast<LightSamplerType>(type)); }
-void ref_render_set_background(float r, float g, float b) { setBackgroundColor(r, g, b); }
+
+void
+ref_render_build_light_sampler(int type)
+{
+    buildLightSampler(static_cast<LightSamplerType>(type));
+    GPU_BRANCH(buildLightSampler(type));
+}
+
+void
+ref_render_set_background(float r, float g, float b)
+{
+    setBackgroundColor(r, g, b);
+    GPU_BRANCH(setBackgroundColor(r, g, b));
+}
 
 void
 ref_render_set_camera(const float* eye, const float* target, const float* up, float fovy, float aspect)
 {
     getCamera()->setLookAt(eye, target, up, fovy, aspect);
+    GPU_BRANCH(setCamera(eye, target, up, fovy, aspect));
 }
 
-void ref_render_reset_accumulation() { resetAccumulation(); }
+void
+ref_render_reset_accumulation()
+{
+    resetAccumulation();
+    GPU_BRANCH(resetAccumulation());
+}
 
+// Alpine::render; with the GPU render branch on, the GPU renders and its sums
+// become the Alpine's accumulation (mAccumBuffer, mTotalSamples), which the
+// reference's own postProcess / getFrameBuffer then read. Returns ms, or a
+// negative value when the GPU branch failed.
 double
 ref_render(uint32_t spp)
 {
     auto t0 = std::chrono::steady_clock::now();
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu)
+    {
+        std::vector<float> sums;
+        uint32_t total = 0;
+        if (!sGpu->render(spp) || !sGpu->readAccumulation(sums, total)) { return -1.0; }
+        auto& a = alpine::alpine();
+        for (size_t i = 0; i < a.mAccumBuffer.size(); ++i)
+        {
+            const float* s = sums.data() + 9 * i;
+            a.mAccumBuffer[i].color = float3(s[0], s[1], s[2]);
+            a.mAccumBuffer[i].albedo = float3(s[3], s[4], s[5]);
+            a.mAccumBuffer[i].normal = float3(s[6], s[7], s[8]);
+        }
+        a.mTotalSamples = total;
+        auto t1 = std::chrono::steady_clock::now();
+        return std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+#endif
     render(spp);
     auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -582,7 +765,14 @@ ref_render_read_sampler_state(uint32_t* out)
         for (int k = 0; k < 4; ++k) out[4 * i + k] = a.mSamplers[i].mSeed[k];
 }
 
-void ref_render_shutdown() { shutdown(); }
+void
+ref_render_shutdown()
+{
+#ifdef ALPINE_GPU_PLUGIN
+    sGpu.reset();
+#endif
+    shutdown();
+}
 
 // Material::sample for n (wo, u) pairs in the local frame.
 void
