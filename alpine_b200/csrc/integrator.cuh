@@ -88,7 +88,22 @@ struct WaveView {
     uint32_t trainCap;
     uint32_t trainStride;      // record the vertices of paths whose hash % stride == 0; 0 = none
     uint32_t waveIndex;
+    // shading order: when set, shading thread i handles queue entry
+    // shadeOrder[i] (queue entries grouped by shade_key); null = queue order
+    const uint32_t* shadeOrder;
+    // the counting sort's buffers: a key byte per queue entry, the order, and
+    // 16 counters (bin counts, bin cursors)
+    uint8_t* shadeKeys;
+    uint32_t* shadeOrderBuf;
+    uint32_t* shadeBins;
 };
+
+// Shading-queue bins (shade_key): a miss; a Dielectric with its Lambertian
+// lobe only; a Dielectric with both lobes; a Conductor; plus kShadeGuided for
+// a vertex the guide samples. Threads of one warp then mostly take the same
+// branches of the shading kernel.
+constexpr uint32_t kShadeBins = 8;
+constexpr uint32_t kShadeGuided = 4;
 
 struct IntegratorKernels {
     void (*generate)(const SceneView&, const WaveView&, bool streamRng, cudaStream_t);
@@ -98,6 +113,11 @@ struct IntegratorKernels {
     // guiding: queries of the current queue; recorded vertices -> training samples
     void (*guide_query)(const SceneView&, const WaveView&, uint32_t maxQueue, cudaStream_t);
     void (*train_finalize)(const WaveView&, guide::Sample* out, uint32_t* outCount, cudaStream_t);
+    // shading order of the current queue: bins[0..7] counts, bins[8..15]
+    // cursors (both zeroed by the caller), keys: one byte per queue entry,
+    // order: the queue entries grouped by bin
+    void (*sort)(const SceneView&, const WaveView&, uint32_t maxQueue, uint32_t* bins, uint8_t* keys,
+                 uint32_t* order, cudaStream_t);
 };
 
 const IntegratorKernels& integrator_fast();
@@ -365,8 +385,10 @@ __global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED
     k_shade(SceneView sc, WaveView w, bool streamRng)
 {
     const uint32_t n = *w.queueCount;
-    uint32_t q = blockIdx.x * kThreads + threadIdx.x;
-    if (q >= n) return;
+    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    // every arithmetic step below depends on the path only, not on i
+    const uint32_t q = w.shadeOrder ? __ldg(w.shadeOrder + i) : i;
     const uint32_t p = w.queuePath[q];
     const uint4 h = w.hits[q];
     const alpine_gpu_ray ray = w.rays[q];
@@ -515,6 +537,77 @@ __global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED
     w.rng[p] = rng.save();
 }
 
+AG_D uint32_t shade_key(const SceneView& sc, const WaveView& w, uint32_t q)
+{
+    const uint32_t prim = w.hits[q].x;
+    uint32_t key = 0;
+    if (prim != 0xffffffffu) {
+        uint32_t mid = __ldg(sc.triInfo + prim) & kTriMaterialMask;
+        if (mid >= sc.materialCount) mid = 0;
+        const Material& m = sc.materials[mid];
+        key = m.kind == kMatConductor ? 3u : (m.lobes == 2u ? 2u : 1u);
+        if (w.guideSlot && w.guideLobes && w.guideSlot[q] >= 0) key |= kShadeGuided;
+    }
+    return key;
+}
+
+// Warp-aggregated rank of this thread among the block's threads with the
+// same key, added to hist[key] (shared memory).
+AG_D uint32_t bin_rank(uint32_t* hist, uint32_t key)
+{
+    const uint32_t am = __activemask();
+    const uint32_t peers = __match_any_sync(am, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(hist + key, __popc(peers));
+    base = __shfl_sync(am, base, leader);
+    return base + __popc(peers & lanemask_lt());
+}
+
+// Pass 1 of the shading-order counting sort: the key of every queue entry
+// and the global count of each bin.
+__global__ void __launch_bounds__(kThreads) k_shade_bins(SceneView sc, WaveView w, uint32_t* bins, uint8_t* keys)
+{
+    __shared__ uint32_t hist[kShadeBins];
+    if (threadIdx.x < kShadeBins) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t n = *w.queueCount;
+    const uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+    if (q < n) {
+        const uint32_t key = shade_key(sc, w, q);
+        keys[q] = (uint8_t)key;
+        bin_rank(hist, key);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeBins && hist[threadIdx.x]) atomicAdd(bins + threadIdx.x, hist[threadIdx.x]);
+}
+
+// Pass 2: each block reserves a run in every bin it holds (bin start =
+// counts of the lower bins, then a cursor) and writes its entries there.
+// The order inside a bin depends on scheduling; shading results do not.
+__global__ void __launch_bounds__(kThreads) k_shade_scatter(WaveView w, uint32_t* bins, const uint8_t* keys,
+                                                            uint32_t* order)
+{
+    __shared__ uint32_t hist[kShadeBins], base[kShadeBins];
+    if (threadIdx.x < kShadeBins) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t n = *w.queueCount;
+    const uint32_t q = blockIdx.x * kThreads + threadIdx.x;
+    uint32_t key = 0, rank = 0;
+    if (q < n) {
+        key = keys[q];
+        rank = bin_rank(hist, key);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeBins && hist[threadIdx.x]) {
+        uint32_t start = 0;
+        for (uint32_t k = 0; k < threadIdx.x; ++k) start += bins[k];
+        base[threadIdx.x] = start + atomicAdd(bins + kShadeBins + threadIdx.x, hist[threadIdx.x]);
+    }
+    __syncthreads();
+    if (q < n) order[base[key] + rank] = q;
+}
+
 __global__ void __launch_bounds__(kThreads) k_resolve(WaveView w)
 {
     const uint32_t n = *w.queueCount;
@@ -654,6 +747,13 @@ void guide_query(const SceneView& sc, const WaveView& w, uint32_t maxQueue, cuda
 void train_finalize(const WaveView& w, guide::Sample* out, uint32_t* outCount, cudaStream_t st)
 {
     if (w.trainCap) k_train_finalize<<<grid(w.trainCap), kThreads, 0, st>>>(w, out, outCount);
+}
+void sort(const SceneView& sc, const WaveView& w, uint32_t maxQueue, uint32_t* bins, uint8_t* keys, uint32_t* order,
+          cudaStream_t st)
+{
+    if (!maxQueue) return;
+    k_shade_bins<<<grid(maxQueue), kThreads, 0, st>>>(sc, w, bins, keys);
+    k_shade_scatter<<<grid(maxQueue), kThreads, 0, st>>>(w, bins, keys, order);
 }
 
 }  // namespace AG_INTEGRATOR_NS

@@ -9,7 +9,8 @@ namespace ag {
 const IntegratorKernels& integrator_exact()
 {
     static const IntegratorKernels k = {exact::generate, exact::shade, exact::resolve, exact::accumulate,
-                                              exact::guide_query, exact::train_finalize};
+                                              exact::guide_query, exact::train_finalize,
+                                              exact::sort};
     return k;
 }
 }  // namespace ag

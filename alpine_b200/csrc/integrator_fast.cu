@@ -6,7 +6,8 @@ namespace ag {
 const IntegratorKernels& integrator_fast()
 {
     static const IntegratorKernels k = {fast::generate, fast::shade, fast::resolve, fast::accumulate,
-                                              fast::guide_query, fast::train_finalize};
+                                              fast::guide_query, fast::train_finalize,
+                                              fast::sort};
     return k;
 }
 }  // namespace ag

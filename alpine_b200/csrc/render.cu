@@ -294,6 +294,7 @@ bool reserve_wave(alpine_gpu_ctx* c, uint32_t paths)
     bytes += round256(P * sizeof(uint4));                  // hits
     bytes += round256(2 * P * sizeof(alpine_gpu_ray));     // shadow rays
     bytes += round256(2 * P);                              // shadow occlusion
+    bytes += round256(P) + round256(P * sizeof(uint32_t)); // shading-order keys and order
     bytes += 256;                                          // counters
     if (!c->dWave.reserve(bytes)) return false;
     c->waveCapacity = paths;
@@ -326,10 +327,13 @@ ag::WaveView carve_wave(alpine_gpu_ctx* c)
     w.hits = (uint4*)take(P * sizeof(uint4));
     w.shadowRays = (alpine_gpu_ray*)take(2 * P * sizeof(alpine_gpu_ray));
     w.shadowOcc = (uint8_t*)take(2 * P);
+    w.shadeKeys = (uint8_t*)take(P);
+    w.shadeOrderBuf = (uint32_t*)take(P * sizeof(uint32_t));
     uint32_t* counters = (uint32_t*)take(256);
     w.queueCount = counters;
     w.queueCountNext = counters + 1;
     w.shadowCount = counters + 2;
+    w.shadeBins = counters + 16;  // 16 words: bin counts, bin cursors
     return w;
 }
 
@@ -754,7 +758,8 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
         };
         const uint32_t cfgWords[] = {spp, S, pixelChunk, pixels, (uint32_t)stream, (uint32_t)fp64,
                                      (uint32_t)c->traceBlock, c->options.seed, c->options.russian_roulette_depth,
-                                     c->waveCapacity, bvh.triTest, bvh.maxVisits, bvh.stackLimit};
+                                     c->waveCapacity, bvh.triTest, bvh.maxVisits, bvh.stackLimit,
+                                     c->options.shade_order};
         const void* ptrs[] = {c->dWave.ptr, c->dAccum.ptr, c->dPixelRng.ptr, c->dStatus};
         put(cfgWords, sizeof cfgWords);
         put(ptrs, sizeof ptrs);
@@ -777,6 +782,7 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
             return c->fail(ALPINE_GPU_ERR_CUDA, "render: stream capture could not begin");
     }
     const uint32_t sampleOrigin = useGraph ? 0u : c->totalSamples;
+    const bool shadeSort = o.shade_order == ALPINE_GPU_SHADE_ORDER_BY_MATERIAL;
     for (uint32_t done = 0; done < spp;) {
         const bool trainNow = trainEnabled && (o.guide_train_steps == 0 || c->guide.steps() < o.guide_train_steps);
         const uint32_t s = std::min(trainNow ? sTrain : S, spp - done);
@@ -821,18 +827,23 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
                 cudaMemsetAsync(w.queueCountNext, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(w.shadowCount, 0, sizeof(uint32_t), st);
                 const bool guideHere = guiding && (o.guide_max_depth == 0 || depth < o.guide_max_depth);
+                ag::WaveView sw = w;
+                if (!guideHere) {  // unguided shading (pending training records still resolve)
+                    sw.guideQuery = nullptr;
+                    sw.guideLobes = nullptr;
+                }
                 if (guideHere) {
                     cudaMemsetAsync(w.guideCount, 0, sizeof(uint32_t), st);
                     K.guide_query(sc, w, w.numPaths, st);
                     if (sampleGuide)
                         c->guide.infer_queue(gw.query, w.guideCount, w.numPaths, gw.lobes, st, c->dStatus, true);
-                    K.shade(sc, w, stream, w.numPaths, st);
-                } else {
-                    ag::WaveView plain = w;  // unguided shading (pending training records still resolve)
-                    plain.guideQuery = nullptr;
-                    plain.guideLobes = nullptr;
-                    K.shade(sc, plain, stream, w.numPaths, st);
                 }
+                if (shadeSort) {  // group the queue by shade_key before shading
+                    cudaMemsetAsync(w.shadeBins, 0, 2 * ag::kShadeBins * sizeof(uint32_t), st);
+                    K.sort(sc, sw, w.numPaths, w.shadeBins, w.shadeKeys, w.shadeOrderBuf, st);
+                    sw.shadeOrder = w.shadeOrderBuf;
+                }
+                K.shade(sc, sw, stream, w.numPaths, st);
                 ag::launch_trace_dyn(bvh, w.shadowRays, w.shadowCount, 2 * w.numPaths, true, w.shadowOcc,
                                      c->dStatus, st, c->traceBlock);
                 K.resolve(w, w.numPaths, st);
@@ -1014,6 +1025,63 @@ int alpine_gpu_read_sampler_state(alpine_gpu_ctx* c, uint32_t* state)
     size_t pixels = (size_t)c->cfg.width * c->cfg.height;
     if (cudaMemcpy(state, c->dPixelRng.ptr, pixels * sizeof(uint4), cudaMemcpyDeviceToHost) != cudaSuccess)
         return c->fail(ALPINE_GPU_ERR_CUDA, "read_sampler_state");
+    return ALPINE_GPU_OK;
+}
+
+// Checkpoint restore: the accumulation (sums and sample count) and the
+// per-pixel reference streams of an earlier run. The next render continues
+// from them as the interrupted run would have: the counter RNG numbers
+// samples from total_samples on, the reference streams continue from the
+// restored states.
+extern "C++" {
+template <typename T>
+static int write_accumulation(alpine_gpu_ctx* c, const T* sums, uint32_t total)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!sums) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "write_accumulation: null sums");
+    if (c->cfg.width == 0 || c->cfg.height == 0) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "no framebuffer");
+    cudaSetDevice(c->device);
+    if (!c->accumValid)
+        if (int rc = alpine_gpu_reset_accumulation(c)) return rc;
+    cudaStreamSynchronize(c->stream);
+    const size_t n = (size_t)c->cfg.width * c->cfg.height * 9;
+    cudaError_t e;
+    if (c->options.accumulate_fp64) {
+        std::vector<double> tmp(sums, sums + n);
+        e = cudaMemcpy(c->dAccum.ptr, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+    } else {
+        std::vector<float> tmp(n);
+        for (size_t i = 0; i < n; ++i) tmp[i] = (float)sums[i];
+        e = cudaMemcpy(c->dAccum.ptr, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("write_accumulation: ") + cudaGetErrorString(e));
+    c->totalSamples = total;
+    return ALPINE_GPU_OK;
+}
+}  // extern "C++"
+
+int alpine_gpu_write_accumulation(alpine_gpu_ctx* c, const float* sums, uint32_t total_samples)
+{
+    return write_accumulation(c, sums, total_samples);
+}
+
+int alpine_gpu_write_accumulation_f64(alpine_gpu_ctx* c, const double* sums, uint32_t total_samples)
+{
+    return write_accumulation(c, sums, total_samples);
+}
+
+int alpine_gpu_write_sampler_state(alpine_gpu_ctx* c, const uint32_t* state)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!state) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "write_sampler_state: null state");
+    if (c->cfg.width == 0 || c->cfg.height == 0) return c->fail(ALPINE_GPU_ERR_INVALID_STATE, "no framebuffer");
+    cudaSetDevice(c->device);
+    if (!c->accumValid)
+        if (int rc = alpine_gpu_reset_accumulation(c)) return rc;
+    cudaStreamSynchronize(c->stream);
+    const size_t pixels = (size_t)c->cfg.width * c->cfg.height;
+    if (cudaMemcpy(c->dPixelRng.ptr, state, pixels * sizeof(uint4), cudaMemcpyHostToDevice) != cudaSuccess)
+        return c->fail(ALPINE_GPU_ERR_CUDA, "write_sampler_state");
     return ALPINE_GPU_OK;
 }
 

@@ -30,6 +30,9 @@ GUIDE_KERNEL_WARP_MMA = 0
 GUIDE_KERNEL_TENSOR_MEMORY = 1
 TRIANGLE_TEST_WIDE_BVH = 0
 TRIANGLE_TEST_BINARY_BVH = 1
+SHADE_ORDER_QUEUE = 0
+SHADE_ORDER_BY_MATERIAL = 1
+SHADE_ORDER_DEFAULT = SHADE_ORDER_BY_MATERIAL
 
 
 class GpuError(RuntimeError):
@@ -58,7 +61,7 @@ class RenderOptions(C.Structure):
                 ("guide_lr", C.c_float), ("guide_warmup_steps", C.c_uint32), ("guide_spp_per_wave", C.c_uint32),
                 ("guide_steps_per_wave", C.c_uint32), ("guide_min_roughness", C.c_float),
                 ("guide_train_steps", C.c_uint32), ("cuda_graph", C.c_uint32),
-                ("guide_max_depth", C.c_uint32)]
+                ("guide_max_depth", C.c_uint32), ("shade_order", C.c_uint32)]
 
 
 class TraversalOptions(C.Structure):
@@ -134,6 +137,9 @@ def lib():
         L.alpine_gpu_read_accumulation_f64.argtypes = [vp, vp, u32p]
         L.alpine_gpu_post_process.argtypes = [vp, C.c_int, vp, vp]
         L.alpine_gpu_read_sampler_state.argtypes = [vp, vp]
+        L.alpine_gpu_write_accumulation.argtypes = [vp, vp, C.c_uint32]
+        L.alpine_gpu_write_accumulation_f64.argtypes = [vp, vp, C.c_uint32]
+        L.alpine_gpu_write_sampler_state.argtypes = [vp, vp]
         L.alpine_gpu_guide_dims.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32p]
         L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
@@ -361,13 +367,14 @@ class Context:
                            accumulate_fp64=False, guide=False, guide_fraction=0.5, guide_train=True,
                            guide_batch=16384, guide_lr=1e-2, guide_warmup_steps=0, guide_spp_per_wave=1,
                            guide_steps_per_wave=8, guide_min_roughness=0.0, guide_train_steps=0, cuda_graph=False,
-                           guide_max_depth=0):
+                           guide_max_depth=0, shade_order=None):
         """Options of alpine_gpu_render_options; the guide_* fields apply when
         guide is set (learned path guiding, counter sampler only)."""
         o = RenderOptions(sampler, max_paths_per_wave, russian_roulette_depth, seed, int(accumulate_fp64),
                           int(guide), guide_fraction, int(guide_train), guide_batch, guide_lr, guide_warmup_steps,
                           guide_spp_per_wave, guide_steps_per_wave, guide_min_roughness, guide_train_steps,
-                          int(cuda_graph), guide_max_depth)
+                          int(cuda_graph), guide_max_depth,
+                          SHADE_ORDER_DEFAULT if shade_order is None else shade_order)
         self._check(self.L.alpine_gpu_set_render_options(self.h, C.byref(o)))
 
     def reset_accumulation(self):
@@ -408,6 +415,19 @@ class Context:
         out = np.empty((height, width, 4), np.uint32)
         self._check(self.L.alpine_gpu_read_sampler_state(self.h, _ptr(out)))
         return out
+
+    def write_accumulation(self, sums, total_samples):
+        """Checkpoint restore: sums float32 or float64 [H, W, 9] and the sample count."""
+        a = np.ascontiguousarray(sums)
+        if a.dtype == np.float64:
+            self._check(self.L.alpine_gpu_write_accumulation_f64(self.h, _ptr(a), total_samples))
+        else:
+            a = np.ascontiguousarray(a, np.float32)
+            self._check(self.L.alpine_gpu_write_accumulation(self.h, _ptr(a), total_samples))
+
+    def write_sampler_state(self, state):
+        s = np.ascontiguousarray(state, np.uint32)
+        self._check(self.L.alpine_gpu_write_sampler_state(self.h, _ptr(s)))
 
     def post_process(self, width, height, tonemap=True):
         mean = np.empty((height, width, 3), np.float32)

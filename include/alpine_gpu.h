@@ -330,9 +330,18 @@ ALPINE_GPU_API int alpine_gpu_set_camera(alpine_gpu_ctx* ctx, const float eye[3]
  *   same scene replays the same graph. Results are identical either way.
  * guide_max_depth: vertices at this depth and deeper use the material's
  *   procedure only and are not recorded (their throughput is small, their
- *   inference costs the same); 0 = guide every depth. */
+ *   inference costs the same); 0 = guide every depth.
+ * shade_order: QUEUE (0) shades the hits in the order the traversal queue
+ *   holds them; BY_MATERIAL (1) first groups them (a two-pass counting sort on
+ *   the GPU) by miss / material kind and lobes / guided, so that the threads of
+ *   a warp take the same shading branches. Results are identical either way
+ *   (each path's arithmetic does not depend on its queue position); only the
+ *   selection among more training records than fit the guide's buffer
+ *   depends on the order. */
 #define ALPINE_GPU_SAMPLER_REFERENCE_STREAM 0u
 #define ALPINE_GPU_SAMPLER_COUNTER 1u
+#define ALPINE_GPU_SHADE_ORDER_QUEUE 0u
+#define ALPINE_GPU_SHADE_ORDER_BY_MATERIAL 1u
 typedef struct alpine_gpu_render_options {
     uint32_t sampler;
     uint32_t max_paths_per_wave;
@@ -351,6 +360,7 @@ typedef struct alpine_gpu_render_options {
     uint32_t guide_train_steps;
     uint32_t cuda_graph;
     uint32_t guide_max_depth;
+    uint32_t shade_order;
 } alpine_gpu_render_options;
 ALPINE_GPU_API int alpine_gpu_set_render_options(alpine_gpu_ctx* ctx, const alpine_gpu_render_options* options);
 
@@ -389,6 +399,20 @@ ALPINE_GPU_API int alpine_gpu_autotune(alpine_gpu_ctx* ctx, uint32_t probe_spp, 
  * number of samples accumulated. Either pointer may be NULL. */
 ALPINE_GPU_API int alpine_gpu_read_accumulation(alpine_gpu_ctx* ctx, float* sums, uint32_t* total_samples);
 ALPINE_GPU_API int alpine_gpu_read_accumulation_f64(alpine_gpu_ctx* ctx, double* sums, uint32_t* total_samples);
+
+/* Checkpoint / resume of a long render (alpine::render accumulates into
+ * mAccumBuffer / mTotalSamples and continues each pixel's Sampler stream,
+ * src/alpine.cpp:259-288; the reference keeps them in memory only). Restores
+ * the sums (the layout of alpine_gpu_read_accumulation, converted to the
+ * context's accumulation precision) and the sample count, and, for the
+ * REFERENCE_STREAM sampler, the per-pixel stream states of
+ * alpine_gpu_read_sampler_state. The next render continues exactly as the
+ * interrupted run would have: the COUNTER sampler numbers samples from
+ * total_samples on. Set the render options first. */
+ALPINE_GPU_API int alpine_gpu_write_accumulation(alpine_gpu_ctx* ctx, const float* sums, uint32_t total_samples);
+ALPINE_GPU_API int alpine_gpu_write_accumulation_f64(alpine_gpu_ctx* ctx, const double* sums,
+                                                     uint32_t total_samples);
+ALPINE_GPU_API int alpine_gpu_write_sampler_state(alpine_gpu_ctx* ctx, const uint32_t* state);
 
 /* alpine::postProcess + getFrameBuffer (alpine.h:63-65, alpine.cpp:446-483)
  * without the denoiser: mean colour (3 floats per pixel, may be NULL) and the

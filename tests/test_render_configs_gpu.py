@@ -9,11 +9,17 @@ Test: per-pixel z-test of the reference mean (R spp) against the GPU mean
 (counter RNG, 16 batches of B spp); the per-sample variance of each pixel is
 estimated from the GPU batches and scaled to each side's sample count. Pass:
 at most 2% of pixels with |z| > 5 and |mean z| < 0.25 (the bar of the
-existing small-scene z-tests), plus the same on 4x4-pixel block means, where
-heavy-tailed per-pixel estimates average out. Pixels whose GPU variance is 0
-(deterministic, e.g. sky seen directly) must agree to 1e-4 relative. relMSE of
-the GPU image against the reference image is printed beside the statistics
-(it is dominated by the reference's own noise at R spp).
+existing small-scene z-tests), the same on 4x4-pixel block means, where
+heavy-tailed per-pixel estimates average out, and |z| < 5 for the image mean
+itself (its standard error from the summed per-pixel variances). Pixels whose
+GPU variance is 0 (deterministic, e.g. sky seen directly) must agree to 1e-4
+relative. relMSE of the GPU image against the reference image is printed
+beside the statistics (it is dominated by the reference's own noise at R spp).
+
+The uniform and power samplers over the city's 131,011 lights are extremely
+heavy-tailed estimators (a rare nearby light carries most of a pixel's
+value), so their image means scatter by tens of percent between runs even at
+tens of thousands of spp; the test's bar for them is statistical, as above.
 """
 from __future__ import annotations
 
@@ -63,6 +69,8 @@ def _zstats(rmean, gb, r_spp, b_spp, block=4):
         "block_frac_z5": float((np.abs(zb) > 5).mean()), "block_mean_z": float(zb.mean()),
         "deterministic": int(det.sum()), "deterministic_bad": det_bad,
         "relmse": _relmse(gmean, rmean), "image_mean_ref": float(rmean.mean()), "image_mean_gpu": float(gmean.mean()),
+        "image_mean_z": float((rmean.mean() - gmean.mean()) /
+                              max(np.sqrt(var1.sum() / r_spp + var1.sum() / (BATCHES * b_spp)) / var1.size, 1e-30)),
     }
 
 
@@ -71,7 +79,7 @@ def _check(st):
     assert st["deterministic_bad"] == 0
     assert st["frac_z5"] < 0.02 and abs(st["mean_z"]) < 0.25
     assert st["block_frac_z5"] < 0.02 and abs(st["block_mean_z"]) < 0.25
-    assert abs(st["image_mean_gpu"] - st["image_mean_ref"]) / st["image_mean_gpu"] < 0.02
+    assert abs(st["image_mean_z"]) < 5
 
 
 def _gpu_batches(ctx, w, h, b_spp):
@@ -128,6 +136,8 @@ def test_room_config_vs_reference(rr):
 # image is 96x54 (1920x1080 / 20, same camera).
 
 CITY_W, CITY_H = 96, 54
+CITY_REF_SPP = 1024
+CITY_GPU_SPP = 4096  # per batch
 
 
 @functools.lru_cache(maxsize=1)
@@ -143,7 +153,7 @@ def city_reference():
     out = {}
     for kind in (gpu.SAMPLER_UNIFORM, gpu.SAMPLER_POWER, gpu.SAMPLER_BVH):
         r.build_light_sampler(kind)
-        out[kind] = _ref_mean(r, 256)
+        out[kind] = _ref_mean(r, CITY_REF_SPP)
     r.close()
     return out
 
@@ -157,10 +167,10 @@ def test_city_config_vs_reference(city_reference, kind):
         scenes.load_scene(ctx, scene, CITY_W, CITY_H)
         ctx.build_light_sampler(kind)
         ctx.set_render_options(sampler=gpu.RNG_COUNTER, seed=31 + kind)
-        gb = _gpu_batches(ctx, CITY_W, CITY_H, 1024)
+        gb = _gpu_batches(ctx, CITY_W, CITY_H, CITY_GPU_SPP)
     finally:
         ctx.close()
-    _check(_zstats(city_reference[kind], gb, 256, 1024))
+    _check(_zstats(city_reference[kind], gb, CITY_REF_SPP, CITY_GPU_SPP))
 
 
 # ---------------------------------------------------------------------------

@@ -232,3 +232,29 @@ def test_fp64_accumulators_match_fp32_and_reference():
     print(f"fp64 z-test: |z|>5 fraction {(np.abs(z) > 5).mean():.4f}, mean z {z.mean():.3f}")
     assert (np.abs(z) > 5).mean() < 0.02
     assert abs(z.mean()) < 0.25
+
+
+@pytest.mark.parametrize("rng,fp64", [(gpu.RNG_REFERENCE_STREAM, False), (gpu.RNG_COUNTER, False),
+                                      (gpu.RNG_COUNTER, True)])
+def test_checkpoint_resume_continues_exactly(rng, fp64):
+    """A render interrupted after 8 spp and resumed in a new context from the
+    read-back sums, sample count (and reference streams) gives the same sums,
+    bit for bit, as one uninterrupted 8 + 8 spp run."""
+    scene = scenes.room_scene(seed=6)
+    w = h = 24
+    opts = dict(seed=7, accumulate_fp64=fp64)
+    a = _gpu_ctx(scene, gpu.SAMPLER_POWER, rng, w, h, depth=4, **opts)
+    a.render(8)
+    sums, n = a.read_accumulation(w, h, fp64=fp64)
+    state = a.read_sampler_state(w, h)
+    a.render(8)
+    full, nf = a.read_accumulation(w, h, fp64=fp64)
+    a.close()
+    b = _gpu_ctx(scene, gpu.SAMPLER_POWER, rng, w, h, depth=4, **opts)
+    b.write_accumulation(sums, n)
+    b.write_sampler_state(state)
+    b.render(8)
+    resumed, nr = b.read_accumulation(w, h, fp64=fp64)
+    b.close()
+    assert n == 8 and nf == nr == 16
+    assert resumed.tobytes() == full.tobytes()
