@@ -493,24 +493,27 @@ def traversal_split(ctx, d_closest, d_shadow, d_hits, d_occ, stream, half, reps=
     return out
 
 
-def l2_copy_bandwidth(stream, mib=24, reps=200):
+def l2_copy_bandwidth(stream, sizes_mib=(4, 8, 16, 24), reps=400):
     """GB/s (read + write bytes) of a device copy whose source and
-    destination stay resident in the 126 MB L2: the denominator for kernels
-    whose working set is served from L2."""
+    destination stay resident in the 126 MB L2 (best over a few sizes): the
+    denominator for kernels whose working set is served from L2."""
     import torch
 
-    n = mib * (1 << 20) // 4
-    a = torch.ones(n, dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
-    for _ in range(10):
-        b.copy_(a)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    ev[0].record(stream)
-    for _ in range(reps):
-        b.copy_(a)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    return 2 * a.numel() * 4 * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9
+    best = 0.0
+    for mib in sizes_mib:
+        n = mib * (1 << 20) // 4
+        a = torch.ones(n, dtype=torch.float32, device="cuda")
+        b = torch.empty_like(a)
+        for _ in range(10):
+            b.copy_(a)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(reps):
+            b.copy_(a)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        best = max(best, 2 * a.numel() * 4 * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9)
+    return best
 
 
 def run_reference(args):
@@ -674,7 +677,7 @@ def run_ours(args):
         "limiter": "instruction issue and SIMD divergence: the BVH (about 57 MB) is served from L2, so DRAM "
                    "traffic is a small fraction of the algorithmic bytes",
         "l2": {"achieved": achieved, "peak": l2_gbs, "frac": achieved / l2_gbs if l2_gbs else None,
-               "peak_source": "L2-resident device copy (2 x 24 MiB) measured in this run"},
+               "peak_source": "L2-resident device copy (best of 4-24 MiB buffers) measured in this run"},
         "algorithmic_bytes_per_launch": bytes_closest,
         "per_ray": {"node_visits": nv_c / n, "tri_tests": tv_c / n, "bytes": bytes_closest / n},
         "any_hit": {"ms": any_ms, "achieved_gbs": bytes_any / (any_ms / 1e3) / 1e9,
