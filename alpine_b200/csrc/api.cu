@@ -202,6 +202,8 @@ int alpine_gpu_reset_scene(alpine_gpu_ctx* c)
     // Scene::reset also drops the lights (src/scenes/scene.h:21-26)
     c->triInfo.clear();
     c->normals.clear();
+    c->uvs.clear();
+    c->tangents.clear();
     c->attribsDirty = true;
     c->lights.clear();
     c->lightsDirty = true;

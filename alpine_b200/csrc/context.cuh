@@ -75,6 +75,8 @@ inline bool make_material(const alpine_gpu_material& in, Material& x)
     x.ax = a > 0.001f ? a : 0.001f;
     x.ay = x.ax;
     x.lobes = (a * a + a * a < 1.0f) ? 2u : 1u;
+    x.baseTex = 0u;
+    x.normalTex = 0u;
     return true;
 }
 
@@ -112,8 +114,19 @@ struct alpine_gpu_ctx {
     // rendering: per-triangle material/normal flags and per-vertex normals
     std::vector<uint32_t> triInfo;  // material id | kTriHasNormals | kTriMorphedNormals
     std::vector<float> normals;     // 3 per vertex (zero for meshes without normals)
+    std::vector<float> uvs;         // 2 per vertex (zero for meshes without texture coordinates)
+    std::vector<float> tangents;    // 4 per vertex: xyz and the bitangent sign
     bool attribsDirty = true;
-    ag::DeviceBuffer dTriInfo, dNormals;
+    ag::DeviceBuffer dTriInfo, dNormals, dUvs, dTangents;
+    // textures (the loaders' Texture4f) and the environment map
+    std::vector<ag::TextureInfo> textures;
+    std::vector<float4> texels;
+    bool texturesDirty = false;
+    ag::DeviceBuffer dTextures, dTexels;
+    std::vector<float> env;         // lat-long, 3 floats per texel, row-major
+    uint32_t envW = 0, envH = 0;
+    bool envDirty = false;
+    ag::DeviceBuffer dEnv;
     std::vector<ag::Material> materials;
     bool materialsDirty = true;
     ag::DeviceBuffer dMaterials;

@@ -31,7 +31,14 @@ struct SceneView {
     const float* verts;
     const uint32_t* idx;
     const float* normals;      // per vertex, may be null
-    const uint32_t* triInfo;   // per triangle: material id | kTriHasNormals | kTriMorphedNormals
+    const uint32_t* triInfo;   // per triangle: material id | kTri* flags
+    const float* uvs;          // per vertex (2 floats), read for kTriHasUvs triangles
+    const float* tangents;     // per vertex (xyz, bitangent sign), read for kTriHasTangents triangles
+    const TextureInfo* textures;
+    const float4* texels;
+    uint32_t textureCount;
+    const float* env;          // lat-long environment map (3 floats per texel), null = background colour
+    uint32_t envW, envH;
     const Material* materials;
     uint32_t materialCount;
     LightSamplerView lights;
@@ -279,14 +286,51 @@ AG_D void surface_at(const SceneView& sc, const uint4 h, Surface& s)
     uint32_t mid = info & kTriMaterialMask;
     if (mid >= sc.materialCount) mid = 0;
     s.mat = sc.materials[mid];
+    const float b0 = 1.0f - b1 - b2;
+    float2 uv = make_float2(0.0f, 0.0f);
+    if (info & kTriHasUvs) {  // mesh.cpp:66-74
+        uv.x = sc.uvs[2ull * i0] * b0 + sc.uvs[2ull * i1] * b1 + sc.uvs[2ull * i2] * b2;
+        uv.y = sc.uvs[2ull * i0 + 1] * b0 + sc.uvs[2ull * i1 + 1] * b1 + sc.uvs[2ull * i2 + 1] * b2;
+    }
+    // Material::getBaseColor(uv) (dielectric.cpp:97-101, conductor.cpp:45-49):
+    // the texture replaces the constant colour everywhere the material uses it
+    if (s.mat.baseTex && s.mat.baseTex <= sc.textureCount) {
+        const float4 t = texture_sample(sc.textures[s.mat.baseTex - 1u], sc.texels, uv.x, uv.y);
+        s.mat.r = t.x;
+        s.mat.g = t.y;
+        s.mat.b = t.z;
+    }
     if (info & kTriHasNormals) {
-        const float b0 = 1.0f - b1 - b2;
         const float3 n0 = mk3(sc.normals[3ull * i0], sc.normals[3ull * i0 + 1], sc.normals[3ull * i0 + 2]);
         const float3 n1 = mk3(sc.normals[3ull * i1], sc.normals[3ull * i1 + 1], sc.normals[3ull * i1 + 2]);
         const float3 n2 = mk3(sc.normals[3ull * i2], sc.normals[3ull * i2 + 1], sc.normals[3ull * i2 + 2]);
         s.ns = n0 * b0 + n1 * b1 + n2 * b2;
         // a morphed normal is re-normalised (mesh.cpp:86-101)
         if (info & kTriMorphedNormals) s.ns = normalize3(s.ns);
+        if (info & kTriHasTangents) {
+            // tangent space (mesh.cpp:104-144): per corner the tangent and the
+            // bitangent normalize(cross(n, t) * sign), both interpolated; the
+            // normal-map value v (0, 0, 1 without a map) gives
+            // ns = normalize(bitangent v.x + tangent v.y + ns v.z)
+            const uint32_t ci[3] = {i0, i1, i2};
+            const float3 nc[3] = {n0, n1, n2};
+            const float bw[3] = {b0, b1, b2};
+            float3 tan = mk3(0.0f, 0.0f, 0.0f), bit = mk3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float* tp = sc.tangents + 4ull * ci[k];
+                const float3 t = mk3(tp[0], tp[1], tp[2]);
+                const float3 bt = normalize3(cross(nc[k], t) * tp[3]);
+                tan = k == 0 ? t * bw[0] : tan + t * bw[k];
+                bit = k == 0 ? bt * bw[0] : bit + bt * bw[k];
+            }
+            float3 v = mk3(0.0f, 0.0f, 1.0f);
+            if (s.mat.normalTex && s.mat.normalTex <= sc.textureCount) {
+                const float4 t = texture_sample(sc.textures[s.mat.normalTex - 1u], sc.texels, uv.x, uv.y);
+                v = mk3(t.x, t.y, t.z);
+            }
+            s.ns = normalize3(bit * v.x + tan * v.y + s.ns * v.z);
+        }
     } else {
         s.ns = s.ng;
     }
@@ -402,9 +446,9 @@ __global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED
     bool cont = false;
 
     if (h.x == 0xffffffffu) {
-        // miss: background (alpine.cpp:318-324; no environment map in this backend)
+        // miss: the environment map, else the background colour (alpine.cpp:318-324)
         float3 rad = f3(w.rad[p]);
-        rad += thr * sc.background;
+        rad += thr * (sc.env ? environment_sample(sc.env, sc.envW, sc.envH, rd) : sc.background);
         w.rad[p] = f4(rad);
     } else {
         const float t = __uint_as_float(h.y);

@@ -267,9 +267,19 @@ int upload_scene_data(alpine_gpu_ctx* c)
         c->materialsDirty = false;
     }
     if (c->attribsDirty) {
-        if (!upload(c->dTriInfo, c->triInfo, st) || !upload(c->dNormals, c->normals, st))
+        if (!upload(c->dTriInfo, c->triInfo, st) || !upload(c->dNormals, c->normals, st) ||
+            !upload(c->dUvs, c->uvs, st) || !upload(c->dTangents, c->tangents, st))
             return c->fail(ALPINE_GPU_ERR_CUDA, "attribute upload failed");
         c->attribsDirty = false;
+    }
+    if (c->texturesDirty) {
+        if (!upload(c->dTextures, c->textures, st) || !upload(c->dTexels, c->texels, st))
+            return c->fail(ALPINE_GPU_ERR_CUDA, "texture upload failed");
+        c->texturesDirty = false;
+    }
+    if (c->envDirty) {
+        if (!upload(c->dEnv, c->env, st)) return c->fail(ALPINE_GPU_ERR_CUDA, "environment map upload failed");
+        c->envDirty = false;
     }
     if (c->lightsDirty) {
         if (!upload(c->dLights, c->lights, st)) return c->fail(ALPINE_GPU_ERR_CUDA, "light upload failed");
@@ -483,10 +493,89 @@ int alpine_gpu_set_triangle_attributes(alpine_gpu_ctx* c, uint32_t shape, const 
     for (uint32_t t = 0; t < tc; ++t) {
         uint32_t mid = tri_material ? tri_material[t] : 0u;
         if (mid & ~ag::kTriMaterialMask) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "material id too large");
-        const uint32_t morphN = c->triInfo[tb + t] & ag::kTriMorphedNormals;  // kept: set by the morph targets
-        c->triInfo[tb + t] = mid | (normals ? ag::kTriHasNormals : 0u) | morphN;
+        // kept: the morph-target and texture-coordinate flags, set by their own calls
+        const uint32_t kept = c->triInfo[tb + t] & (ag::kTriMorphedNormals | ag::kTriHasUvs | ag::kTriHasTangents);
+        c->triInfo[tb + t] = mid | (normals ? ag::kTriHasNormals : 0u) | kept;
     }
     c->attribsDirty = true;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_set_triangle_uvs(alpine_gpu_ctx* c, uint32_t shape, const float* uvs, const float* tangents)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (shape >= c->shapeVertBase.size()) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "bad shape id");
+    if (tangents && !uvs)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_triangle_uvs: tangents need texture coordinates");
+    const uint32_t vb = c->shapeVertBase[shape], vc = c->shapeVertCount[shape];
+    const uint32_t tb = c->shapeTriBase[shape], tc = c->shapeTriCount[shape];
+    if (c->triInfo.size() < c->idx.size() / 3) c->triInfo.resize(c->idx.size() / 3, 0u);
+    if (tangents)
+        for (uint32_t t = 0; t < tc; ++t)
+            if (!(c->triInfo[tb + t] & ag::kTriHasNormals))
+                return c->fail(ALPINE_GPU_ERR_INVALID_STATE,
+                               "set_triangle_uvs: tangents need vertex normals (alpine_gpu_set_triangle_attributes)");
+    const size_t V = c->verts.size() / 3;
+    if (uvs) {
+        if (c->uvs.size() < 2 * V) c->uvs.resize(2 * V, 0.0f);
+        std::memcpy(c->uvs.data() + 2ull * vb, uvs, 2ull * vc * sizeof(float));
+    }
+    if (tangents) {
+        if (c->tangents.size() < 4 * V) c->tangents.resize(4 * V, 0.0f);
+        std::memcpy(c->tangents.data() + 4ull * vb, tangents, 4ull * vc * sizeof(float));
+    }
+    for (uint32_t t = 0; t < tc; ++t) {
+        uint32_t& f = c->triInfo[tb + t];
+        f = (f & ~(ag::kTriHasUvs | ag::kTriHasTangents)) | (uvs ? ag::kTriHasUvs : 0u) |
+            (tangents ? ag::kTriHasTangents : 0u);
+    }
+    c->attribsDirty = true;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_add_texture(alpine_gpu_ctx* c, const float* texels, uint32_t width, uint32_t height, uint32_t* id)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!texels || width == 0 || height == 0)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_texture: empty texture");
+    const uint64_t n = (uint64_t)width * height;
+    if (c->texels.size() + n >= 0xffffffffull) return c->fail(ALPINE_GPU_ERR_LIMIT, "add_texture: texel pool full");
+    ag::TextureInfo t{(uint32_t)c->texels.size(), width, height, 0u};
+    c->texels.resize(c->texels.size() + n);
+    std::memcpy(c->texels.data() + t.offset, texels, n * sizeof(float4));
+    c->textures.push_back(t);
+    c->texturesDirty = true;
+    if (id) *id = (uint32_t)(c->textures.size() - 1);
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_set_material_textures(alpine_gpu_ctx* c, uint32_t material, int32_t base_color_texture,
+                                     int32_t normal_texture)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (material >= c->materials.size())
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_material_textures: bad material id");
+    const int32_t nt = (int32_t)c->textures.size();
+    if (base_color_texture >= nt || normal_texture >= nt || base_color_texture < -1 || normal_texture < -1)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_material_textures: bad texture id");
+    c->materials[material].baseTex = (uint32_t)(base_color_texture + 1);
+    c->materials[material].normalTex = (uint32_t)(normal_texture + 1);
+    c->materialsDirty = true;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_set_environment_map(alpine_gpu_ctx* c, const float* rgb, uint32_t width, uint32_t height)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!rgb || width == 0 || height == 0) {
+        c->env.clear();
+        c->envW = c->envH = 0;
+        return ALPINE_GPU_OK;
+    }
+    c->env.assign(rgb, rgb + 3ull * width * height);
+    c->envW = width;
+    c->envH = height;
+    c->envDirty = true;
     return ALPINE_GPU_OK;
 }
 
@@ -722,6 +811,14 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
     sc.idx = c->dIdx.as<uint32_t>();
     sc.normals = c->dNormals.as<float>();
     sc.triInfo = c->dTriInfo.as<uint32_t>();
+    sc.uvs = c->dUvs.as<float>();
+    sc.tangents = c->dTangents.as<float>();
+    sc.textures = c->dTextures.as<ag::TextureInfo>();
+    sc.texels = c->dTexels.as<float4>();
+    sc.textureCount = (uint32_t)c->textures.size();
+    sc.env = c->envW ? c->dEnv.as<float>() : nullptr;
+    sc.envW = c->envW;
+    sc.envH = c->envH;
     sc.materials = c->dMaterials.as<ag::Material>();
     sc.materialCount = c->materialCount;
     sc.lights.kind = c->samplerKind;

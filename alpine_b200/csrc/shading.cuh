@@ -152,15 +152,51 @@ enum MaterialKind : uint32_t { kMatDielectric = 0, kMatConductor = 1 };
 // Per-triangle render attributes: material id and flags.
 constexpr uint32_t kTriHasNormals = 0x80000000u;      // interpolate the vertex normals
 constexpr uint32_t kTriMorphedNormals = 0x40000000u;  // the mesh has normal morph targets
-constexpr uint32_t kTriMaterialMask = 0x3fffffffu;
+constexpr uint32_t kTriHasUvs = 0x20000000u;          // interpolate the vertex texture coordinates
+constexpr uint32_t kTriHasTangents = 0x10000000u;     // tangent-space shading normals (needs normals)
+constexpr uint32_t kTriMaterialMask = 0x0fffffffu;
 
 struct Material {
     uint32_t kind;
     float r, g, b;    // base colour (Dielectric: diffuse albedo; Conductor: F0)
     float ax, ay;     // microfacet alpha, already clamped to >= 0.001
     uint32_t lobes;   // Dielectric: 1 (Lambertian) or 2 (+ Microfacet, when ax^2 + ay^2 < 1 unclamped)
-    float pad;
+    uint32_t baseTex;    // base-colour texture id + 1 (0 = the constant colour above)
+    uint32_t normalTex;  // normal-map texture id + 1 (0 = none: the tangent-space normal (0, 0, 1))
 };
+
+// One texture of the texel pool: texels [offset, offset + width * height),
+// row-major float4 (the loader's Texture4f, src/texture.h).
+struct TextureInfo {
+    uint32_t offset, width, height, pad;
+};
+
+// Texture<T>::sample (src/texture.h:19-35): nearest texel, coordinates
+// wrapped to [0, 1) by u - floor(u), scaled by the size, clamped.
+AG_D float4 texture_sample(const TextureInfo& t, const float4* texels, float u, float v)
+{
+    u = u - floorf(u);
+    v = v - floorf(v);
+    uint32_t x = (uint32_t)(u * (float)t.width);
+    uint32_t y = (uint32_t)(v * (float)t.height);
+    x = min(x, t.width - 1u);
+    y = min(y, t.height - 1u);
+    return texels[t.offset + x + y * t.width];
+}
+
+// EnvironmentMap::sample (src/environment_map.cpp:14-37): the lat-long map
+// at u = atan2(d.z, d.x) / 2pi + 0.5, v = acos(clamp(d.y)) / pi, nearest texel.
+AG_D float3 environment_sample(const float* env, uint32_t w, uint32_t h, float3 d)
+{
+    float u = atan2f(d.z, d.x) / (2.0f * kPi) + 0.5f;
+    float v = acosf(fminf(fmaxf(d.y, -1.0f), 1.0f)) / kPi;
+    u = u - floorf(u);
+    v = fminf(fmaxf(v, 0.0f), 1.0f);
+    const uint32_t x = min((uint32_t)(u * (float)w), w - 1u);
+    const uint32_t y = min((uint32_t)(v * (float)h), h - 1u);
+    const float* t = env + 3ull * (y * (size_t)w + x);
+    return mk3(t[0], t[1], t[2]);
+}
 
 struct BsdfSample {
     float3 estimator;  // bsdf * cos / pdf

@@ -119,6 +119,10 @@ def lib():
         L.alpine_gpu_material_sample.argtypes = [vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
         L.alpine_gpu_material_eval.argtypes = [vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
         L.alpine_gpu_set_triangle_attributes.argtypes = [vp, C.c_uint32, vp, vp]
+        L.alpine_gpu_set_triangle_uvs.argtypes = [vp, C.c_uint32, vp, vp]
+        L.alpine_gpu_add_texture.argtypes = [vp, vp, C.c_uint32, C.c_uint32, u32p]
+        L.alpine_gpu_set_material_textures.argtypes = [vp, C.c_uint32, C.c_int32, C.c_int32]
+        L.alpine_gpu_set_environment_map.argtypes = [vp, vp, C.c_uint32, C.c_uint32]
         L.alpine_gpu_add_point_light.argtypes = [vp, C.c_float, f3, f3, u32p]
         L.alpine_gpu_add_disk_light.argtypes = [vp, C.c_float, f3, f3, f3, C.c_float, u32p]
         L.alpine_gpu_add_quad_light.argtypes = [vp, f3, f3, f3, f3, u32p]
@@ -279,11 +283,18 @@ class Context:
 
     # ---- rendering -------------------------------------------------------
     def set_materials(self, materials):
-        """materials: sequence of (kind, (r, g, b), roughness)."""
+        """materials: sequence of (kind, (r, g, b), roughness[, base texture,
+        normal texture]); texture ids from add_texture, None / -1 = none."""
         m = np.zeros(len(materials), MATERIAL_DTYPE)
-        for i, (k, col, r) in enumerate(materials):
+        for i, (k, col, r, *_) in enumerate(materials):
             m[i] = (k, col, r)
         self._check(self.L.alpine_gpu_set_materials(self.h, _ptr(m) if len(m) else None, len(m)))
+        for i, mat in enumerate(materials):
+            if len(mat) > 3:
+                bt = -1 if mat[3] is None else mat[3]
+                nt = -1 if len(mat) < 5 or mat[4] is None else mat[4]
+                if bt >= 0 or nt >= 0:
+                    self.set_material_textures(i, bt, nt)
 
     @staticmethod
     def _material(material):
@@ -333,6 +344,31 @@ class Context:
         t = None if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
         self._check(self.L.alpine_gpu_set_triangle_attributes(self.h, shape, None if n is None else _ptr(n),
                                                               None if t is None else _ptr(t)))
+
+    def set_triangle_uvs(self, shape, uvs=None, tangents=None):
+        """Per-vertex texture coordinates float[V, 2] and tangents float[V, 4]."""
+        u = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
+        t = None if tangents is None else np.ascontiguousarray(tangents, np.float32)
+        self._check(self.L.alpine_gpu_set_triangle_uvs(self.h, shape, None if u is None else _ptr(u),
+                                                       None if t is None else _ptr(t)))
+
+    def add_texture(self, rgba) -> int:
+        """float32 [H, W, 4] texels; returns the texture id."""
+        t = np.ascontiguousarray(rgba, np.float32)
+        i = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_texture(self.h, _ptr(t), t.shape[1], t.shape[0], C.byref(i)))
+        return i.value
+
+    def set_material_textures(self, material, base_color=-1, normal=-1):
+        self._check(self.L.alpine_gpu_set_material_textures(self.h, material, base_color, normal))
+
+    def set_environment_map(self, rgb):
+        """float32 [H, W, 3] lat-long map (None removes it)."""
+        if rgb is None:
+            self._check(self.L.alpine_gpu_set_environment_map(self.h, None, 0, 0))
+            return
+        e = np.ascontiguousarray(rgb, np.float32)
+        self._check(self.L.alpine_gpu_set_environment_map(self.h, _ptr(e), e.shape[1], e.shape[0]))
 
     def add_point_light(self, power, color, position):
         i = C.c_uint32()

@@ -449,10 +449,84 @@ def add_random_lights(scene, n, seed=5, kinds=("disk", "point")):
     return scene
 
 
+def textured_scene(seed=1, tex=64, env=(128, 64)):
+    """An open scene for the texture paths: a floor with a repeating
+    checkerboard base-colour texture (texture coordinates up to 4, so the
+    lookup wraps), a UV sphere with vertex normals, tangents and a bumpy
+    normal map on a GGX conductor, a box with a base-colour texture on every
+    face, under a lat-long environment map (sky gradient and a bright sun
+    patch) that escaping rays read, plus one disk light."""
+    rng = np.random.default_rng(seed)
+    textures = []
+    # checkerboard (linear colours)
+    yy, xx = np.mgrid[0:tex, 0:tex]
+    chk = ((xx // 8 + yy // 8) % 2).astype(np.float32)
+    a, b = rng.uniform(0.1, 0.4, 3), rng.uniform(0.5, 0.9, 3)
+    t0 = np.concatenate([a[None, None] * (1 - chk[..., None]) + b[None, None] * chk[..., None],
+                         np.ones((tex, tex, 1))], -1).astype(np.float32)
+    textures.append(t0)
+    # normal map in [-1, 1]: a bump pattern in tangent space
+    u = (xx + 0.5) / tex
+    v = (yy + 0.5) / tex
+    n = np.stack([0.35 * np.sin(6 * math.pi * u), 0.35 * np.cos(4 * math.pi * v), np.ones_like(u)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    textures.append(np.concatenate([n, np.ones((tex, tex, 1))], -1).astype(np.float32))
+    # noise colours
+    textures.append(np.concatenate([rng.uniform(0.05, 0.95, (tex, tex, 3)), np.ones((tex, tex, 1))], -1)
+                    .astype(np.float32))
+    materials = [(0, (0.5, 0.5, 0.5), 1.0, 0, None),        # floor: checkerboard Lambertian
+                 (1, (0.9, 0.7, 0.4), 0.25, None, 1),       # sphere: normal-mapped conductor
+                 (0, (0.5, 0.5, 0.5), 0.3, 2, None)]        # box: textured two-lobe dielectric
+    meshes = []
+    fv = np.array([[-4, 0, -4], [4, 0, -4], [4, 0, 4], [-4, 0, 4]], np.float32)
+    fi = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)  # normal +y
+    fuv = np.array([[0, 0], [4, 0], [4, 4], [0, 4]], np.float32)
+    meshes.append({"verts": fv, "idx": fi, "normals": None, "tri_material": np.zeros(2, np.uint32), "uvs": fuv})
+    seg, bands = 48, 24
+    sv, si, sn = uv_sphere((0.0, 1.0, 0.0), 1.0, seg, bands)
+    th = math.pi * np.arange(bands + 1) / bands
+    ph = 2 * math.pi * np.arange(seg) / seg
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    suv = np.stack([P / (2 * math.pi), T / math.pi], -1).reshape(-1, 2).astype(np.float32)
+    tang = np.stack([-np.sin(P), np.zeros_like(P), np.cos(P), np.ones_like(P)], -1).reshape(-1, 4).astype(np.float32)
+    meshes.append({"verts": sv, "idx": si, "normals": sn, "tri_material": np.ones(si.shape[0], np.uint32),
+                   "uvs": suv, "tangents": tang})
+    # box with per-face vertices (24) so every face has its own coordinates
+    lo, hi = np.array([1.3, 0.0, -0.8]), np.array([2.3, 1.0, 0.2])
+    bv, bi = box_mesh(lo, hi)
+    verts, idx, uvs = [], [], []
+    for t in bi:
+        base = len(verts)
+        for k in t:
+            verts.append(bv[k])
+        p0, p1, p2 = bv[t[0]], bv[t[1]], bv[t[2]]
+        nrm = np.cross(p1 - p0, p2 - p0)
+        ax = int(np.argmax(np.abs(nrm)))
+        o = [d for d in range(3) if d != ax]
+        for k in t:
+            uvs.append([(bv[k][o[0]] - lo[o[0]]) / (hi[o[0]] - lo[o[0]]),
+                        (bv[k][o[1]] - lo[o[1]]) / (hi[o[1]] - lo[o[1]])])
+        idx.append([base, base + 1, base + 2])
+    meshes.append({"verts": np.array(verts, np.float32), "idx": np.array(idx, np.uint32), "normals": None,
+                   "tri_material": np.full(len(idx), 2, np.uint32), "uvs": np.array(uvs, np.float32)})
+    ew, eh = env
+    ey, ex = np.mgrid[0:eh, 0:ew]
+    vv = (ey + 0.5) / eh
+    sky = np.stack([0.3 + 0.7 * (1 - vv), 0.5 + 0.5 * (1 - vv), np.ones_like(vv)], -1) * 0.8
+    sun = (np.abs(ex - ew * 0.3) < ew / 32) & (np.abs(ey - eh * 0.25) < eh / 16)
+    sky[sun] = (40.0, 36.0, 30.0)
+    lights = [("disk", 60.0, (1.0, 0.9, 0.8), (-2.0, 4.0, -1.0), (0.0, 0.0, 0.0), 0.4)]
+    camera = ((0.5, 2.2, -5.5), (0.5, 0.8, 0.0), (0.0, 1.0, 0.0), math.radians(55.0))
+    return {"meshes": meshes, "materials": materials, "lights": lights, "camera": camera,
+            "background": (0.0, 0.0, 0.0), "textures": textures, "environment": sky.astype(np.float32)}
+
+
 def load_scene(target, scene, width, height):
     """Loads a scene description into an alpine_b200 gpu.Context or an
     oracle RefRenderer (same method names)."""
     is_gpu = hasattr(target, "set_triangle_attributes")
+    for t in scene.get("textures", ()):  # ids 0, 1, ... in order on both sides
+        target.add_texture(t)
     if is_gpu:
         target.reset_scene()
         target.set_materials(scene["materials"])
@@ -463,6 +537,8 @@ def load_scene(target, scene, width, height):
         if is_gpu:
             sid = target.add_mesh(m["verts"], m["idx"])
             target.set_triangle_attributes(sid, m["normals"], m["tri_material"])
+            if m.get("uvs") is not None:
+                target.set_triangle_uvs(sid, m["uvs"], m.get("tangents"))
             if mo is not None:
                 target.set_morph_targets(sid, mo["deltas"], mo.get("normal_deltas"))
                 target.add_animation_channel(sid, mo["times"], mo["weights"])
@@ -470,7 +546,10 @@ def load_scene(target, scene, width, height):
             target.add_morph_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"],
                                   mo["deltas"], mo.get("normal_deltas"), mo["times"], mo["weights"])
         else:
-            target.add_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"])
+            target.add_mesh(m["verts"], m["idx"], m["normals"], m["tri_material"], scene["materials"],
+                            uvs=m.get("uvs"), tangents=m.get("tangents"))
+    if scene.get("environment") is not None:
+        target.set_environment_map(scene["environment"])
     for l in scene["lights"]:
         if l[0] == "disk":
             target.add_disk_light(*l[1:])

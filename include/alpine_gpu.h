@@ -256,6 +256,42 @@ ALPINE_GPU_API int alpine_gpu_material_eval(alpine_gpu_ctx* ctx, const alpine_gp
 ALPINE_GPU_API int alpine_gpu_set_triangle_attributes(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* normals,
                                                       const uint32_t* triangle_material);
 
+/* Texture coordinates and tangents of one mesh (Mesh::Data uvs / tangents,
+ * src/shapes/mesh.h:16-36), per vertex, indexed like the positions:
+ * uvs float[2 * vertex_count] (NULL: none), tangents float[4 * vertex_count]
+ * = xyz and the bitangent sign (NULL: none; needs uvs and the vertex normals
+ * of alpine_gpu_set_triangle_attributes). With tangents the shading normal is
+ * the reference's tangent-space normal (mesh.cpp:104-144):
+ * normalize(B v.x + T v.y + N v.z), T and B = normalize(cross(n, t) sign)
+ * interpolated per corner, v the material's normal map at uv or (0, 0, 1).
+ * Tangent morph targets are not supported (the tangents stay as given). */
+ALPINE_GPU_API int alpine_gpu_set_triangle_uvs(alpine_gpu_ctx* ctx, uint32_t shape_id, const float* uvs,
+                                               const float* tangents);
+
+/* Textures (Texture4f, src/texture.h): width x height float4 texels,
+ * row-major, already converted as the loader does (sRGB base colours
+ * linearised, normal maps remapped to [-1, 1]: gltf_loader.cpp:417-460).
+ * Sampled with the reference's nearest lookup (texture.h:19-35). Writes the
+ * texture id (0, 1, ... in call order). */
+ALPINE_GPU_API int alpine_gpu_add_texture(alpine_gpu_ctx* ctx, const float* texels, uint32_t width, uint32_t height,
+                                          uint32_t* texture_id);
+
+/* Binds textures to one material of the table set by alpine_gpu_set_materials
+ * (Dielectric / Conductor baseColorTex and normalTex, dielectric.cpp:14-21;
+ * -1 = none). The base-colour texture replaces the constant colour in every
+ * use (sampling, evaluation, the albedo AOV), as getBaseColor(uv) does.
+ * alpine_gpu_set_materials resets the bindings. */
+ALPINE_GPU_API int alpine_gpu_set_material_textures(alpine_gpu_ctx* ctx, uint32_t material,
+                                                    int32_t base_color_texture, int32_t normal_texture);
+
+/* alpine::loadEnvironmentMap (alpine.h:57; src/environment_map.cpp): a
+ * lat-long map of width x height RGB texels (3 floats each, row-major) that
+ * escaping rays read instead of the background colour (alpine.cpp:318-323),
+ * with the reference's direction-to-texel mapping (environment_map.cpp:14-37).
+ * rgb = NULL removes it. */
+ALPINE_GPU_API int alpine_gpu_set_environment_map(alpine_gpu_ctx* ctx, const float* rgb, uint32_t width,
+                                                  uint32_t height);
+
 /* Lights (alpine::addPointLight / addDiskLight, include/alpine/alpine.h:35-42;
  * src/lights/). A quad light is a one-sided emitting parallelogram
  * corner + [0,1] edge_u + [0,1] edge_v with constant radiance, emitting on the

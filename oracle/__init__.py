@@ -140,6 +140,12 @@ def ref(timing: bool = False, plugin: bool = False):
         L.ref_render_add_morph_mesh.restype = C.c_int
         L.ref_morph_vertices.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, _f32p, C.c_uint32, _f32p, _f32p,
                                          C.c_uint32, C.c_float, _f32p]
+        L.ref_render_add_texture.argtypes = [_f32p, C.c_uint32, C.c_uint32]
+        L.ref_render_add_texture.restype = C.c_int
+        L.ref_render_add_mesh_ex.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, _u32p, _f32p, C.c_uint32]
+        L.ref_render_add_mesh_ex.restype = C.c_int
+        L.ref_render_set_environment.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.ref_render_load_obj.argtypes = [C.c_char_p]
         L.ref_render_load_obj.restype = C.c_int
         L.ref_render_add_disk_light.argtypes = [C.c_float, _f32p, _f32p, _f32p, C.c_float]
@@ -272,18 +278,50 @@ class RefRenderer:
         if gpu_branch and not self.L.ref_render_gpu_branch(1, seed, int(accelerator == self.ACC_BVH)):
             raise RuntimeError("ref_render_gpu_branch failed")
 
-    def add_mesh(self, verts, idx, normals=None, tri_material=None, materials=((0, (0.5, 0.5, 0.5), 1.0),)):
+    def add_texture(self, rgba):
+        """Texture4f from float32 [H, W, 4]; returns its id."""
+        t = np.ascontiguousarray(rgba, np.float32)
+        return self.L.ref_render_add_texture(t.reshape(-1), t.shape[1], t.shape[0])
+
+    def set_environment_map(self, rgb):
+        """Alpine::mEnvironmentMap from float32 [H, W, 3] (None removes it)."""
+        if rgb is None:
+            self.L.ref_render_set_environment(None, 0, 0)
+            return
+        self._env = np.ascontiguousarray(rgb, np.float32)
+        self.L.ref_render_set_environment(self._env.ctypes.data, self._env.shape[1], self._env.shape[0])
+
+    def add_mesh(self, verts, idx, normals=None, tri_material=None, materials=((0, (0.5, 0.5, 0.5), 1.0),),
+                 uvs=None, tangents=None):
+        """materials: (kind, (r, g, b), roughness[, base texture, normal texture])."""
         v = np.ascontiguousarray(verts, np.float32).reshape(-1)
         i = np.ascontiguousarray(idx, np.uint32).reshape(-1)
         nt = i.size // 3
         tm = np.zeros(nt, np.uint32) if tri_material is None else np.ascontiguousarray(tri_material, np.uint32)
-        mats = np.array([[k, *c, r] for k, c, r in materials], np.float32).reshape(-1)
         nptr = None
         if normals is not None:
             self._normals = np.ascontiguousarray(normals, np.float32).reshape(-1)
             nptr = self._normals.ctypes.data
-        if not self.L.ref_render_add_mesh(v, v.size // 3, i, nt, nptr, tm, mats, len(materials)):
-            raise RuntimeError("ref_render_add_mesh failed")
+        textured = uvs is not None or tangents is not None or any(len(m) > 3 for m in materials)
+        if not textured:
+            mats = np.array([[k, *c, r] for k, c, r, *_ in materials], np.float32).reshape(-1)
+            if not self.L.ref_render_add_mesh(v, v.size // 3, i, nt, nptr, tm, mats, len(materials)):
+                raise RuntimeError("ref_render_add_mesh failed")
+            return
+        recs = []
+        for m in materials:
+            k, c, r = m[:3]
+            bt = m[3] if len(m) > 3 and m[3] is not None else -1
+            ntex = m[4] if len(m) > 4 and m[4] is not None else -1
+            recs.append([k, *c, r, bt, ntex])
+        mats = np.array(recs, np.float32).reshape(-1)
+        self._uvs = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1)
+        self._tangents = None if tangents is None else np.ascontiguousarray(tangents, np.float32).reshape(-1)
+        if not self.L.ref_render_add_mesh_ex(v, v.size // 3, i, nt, nptr,
+                                             None if self._uvs is None else self._uvs.ctypes.data,
+                                             None if self._tangents is None else self._tangents.ctypes.data,
+                                             tm, mats, len(materials)):
+            raise RuntimeError("ref_render_add_mesh_ex failed")
 
     def add_morph_mesh(self, verts, idx, normals, tri_material, materials, deltas, normal_deltas, times, weights):
         """A mesh with morph targets deltas float[T, V, 3] (and normal deltas)

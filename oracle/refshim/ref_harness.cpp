@@ -73,6 +73,8 @@
 #include <gpu_accelerator.h>
 #include <gpu_backend.h>
 #endif
+#include <environment_map.h>
+#include <texture.h>
 #include <materials/conductor.h>
 #include <materials/dielectric.h>
 #include <shapes/mesh.h>
@@ -283,14 +285,27 @@ inline Ray makeRay(const float* r)
 }
 }
 
-// One material record {kind, r, g, b, roughness} as the reference class
-// (kind 0 = Dielectric, 1 = Conductor; the loaders' alpha = roughness).
+// Textures added through ref_render_add_texture (the loaders' Texture4f).
+static std::vector<std::shared_ptr<Texture4f>> sTextures;
+
+static std::shared_ptr<Texture4f>
+texture_or_null(float id)
+{
+    int32_t i = static_cast<int32_t>(id);
+    return (i >= 0 && i < static_cast<int32_t>(sTextures.size())) ? sTextures[i] : nullptr;
+}
+
+// One material record {kind, r, g, b, roughness[, base texture, normal
+// texture]} as the reference class (kind 0 = Dielectric, 1 = Conductor; the
+// loaders' alpha = roughness; texture ids -1 = none).
 static std::shared_ptr<Material>
-make_ref_material(const float* r)
+make_ref_material(const float* r, uint32_t stride = 5)
 {
     float3 bc(r[1], r[2], r[3]);
-    if (r[0] == 1.0f) { return std::make_shared<Conductor>(float2(r[4]), bc, nullptr, nullptr); }
-    return std::make_shared<Dielectric>(float2(r[4]), bc, nullptr, nullptr);
+    auto bt = stride >= 7 ? texture_or_null(r[5]) : nullptr;
+    auto nt = stride >= 7 ? texture_or_null(r[6]) : nullptr;
+    if (r[0] == 1.0f) { return std::make_shared<Conductor>(float2(r[4]), bc, bt, nt); }
+    return std::make_shared<Dielectric>(float2(r[4]), bc, bt, nt);
 }
 
 #ifdef ALPINE_GPU_PLUGIN
@@ -442,6 +457,7 @@ ref_render_init(uint32_t width, uint32_t height, uint32_t maxDepth, uint64_t are
 #ifdef ALPINE_GPU_PLUGIN
     sGpu.reset();
 #endif
+    sTextures.clear();
     if (sAlpine) { shutdown(); }
     return initialize(static_cast<uint32_t>(arenaBytes), width, height, maxDepth) ? 1 : 0;
 }
@@ -526,6 +542,74 @@ ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, u
     a.mScene.shapes.push_back(mesh);
     mesh->appendTo(a.mAccelerator.get());
     return 1;
+}
+
+// Texture4f of w x h float4 texels (row-major); returns its id.
+int
+ref_render_add_texture(const float* rgba, uint32_t w, uint32_t h)
+{
+    std::vector<float4> d((size_t)w * h);
+    for (size_t i = 0; i < d.size(); ++i) { d[i] = float4(rgba[4 * i], rgba[4 * i + 1], rgba[4 * i + 2], rgba[4 * i + 3]); }
+    sTextures.push_back(std::make_shared<Texture4f>(w, h, std::move(d)));
+    return static_cast<int>(sTextures.size() - 1);
+}
+
+// ref_render_add_mesh with texture coordinates (2 per vertex, may be null),
+// tangents (4 per vertex, may be null) and 7-float material records
+// {kind, r, g, b, roughness, base texture, normal texture}.
+int
+ref_render_add_mesh_ex(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
+    const float* normals, const float* uvs, const float* tangents, const uint32_t* triMaterial,
+    const float* materials, uint32_t nmat)
+{
+    Mesh::Data d;
+    d.vertices.resize(nverts);
+    for (uint32_t i = 0; i < nverts; ++i) { d.vertices[i] = float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); }
+    if (normals)
+    {
+        d.normals.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i) { d.normals[i] = float3(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]); }
+    }
+    if (uvs)
+    {
+        d.uvs.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i) { d.uvs[i] = float2(uvs[2 * i], uvs[2 * i + 1]); }
+    }
+    if (tangents)
+    {
+        d.tangents.resize(nverts);
+        for (uint32_t i = 0; i < nverts; ++i)
+        {
+            d.tangents[i] = float4(tangents[4 * i], tangents[4 * i + 1], tangents[4 * i + 2], tangents[4 * i + 3]);
+        }
+    }
+    std::vector<std::shared_ptr<Material>> mats(nmat);
+    for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 7 * m, 7); }
+    d.prims.resize(ntris);
+    d.materials.resize(ntris);
+    for (uint32_t i = 0; i < ntris; ++i)
+    {
+        d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]);
+        uint32_t m = triMaterial[i];
+        if (m >= nmat) { return 0; }
+        d.materials[i] = mats[m];
+    }
+    auto mesh = std::make_shared<Mesh>(std::move(d), 0);
+    auto& a = alpine::alpine();
+    a.mScene.shapes.push_back(mesh);
+    mesh->appendTo(a.mAccelerator.get());
+    return 1;
+}
+
+// Alpine::mEnvironmentMap (what loadEnvironmentMap installs): w x h RGB texels.
+void
+ref_render_set_environment(const float* rgb, uint32_t w, uint32_t h)
+{
+    auto& a = alpine::alpine();
+    if (!rgb) { a.mEnvironmentMap.reset(); return; }
+    std::vector<float3> d((size_t)w * h);
+    for (size_t i = 0; i < d.size(); ++i) { d[i] = float3(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]); }
+    a.mEnvironmentMap = std::make_unique<EnvironmentMap>(std::move(d), w, h);
 }
 
 // Morph targets (Mesh::Data::targets) and one animation channel for a mesh
