@@ -26,12 +26,12 @@ rendered together (morph + BVH rebuild + render per scene per frame).
 `guiding` (rank 0, one GPU): time to relMSE 0.01, guided vs plain MIS, on the
 glossy interior (20 x 4 x 12 m room, 2.0M triangles, 70% GGX with roughness
 in [0.02, 0.4], sky of radiance 5 through two 1 x 2 m window openings, depth
-12) at 320 x 180 against a 65,536-spp plain image rendered in the same run.
-relMSE = mean over pixels and channels of (x - r)^2 / (r^2 + 0.01 mean(r)^2).
-Time is the wall time of the render calls (synchronous), guided training
-included; both curves are sampled at doubling spp and interpolated in log-log.
-Each arm runs three times (different seeds) and reports its median time
-(all three are listed).
+12) at 1920 x 1080, against a 1,024-spp plain image rendered in the same run
+in two independent halves, whose own error is removed from every relMSE (see
+guiding_benchmark). relMSE = mean over pixels and channels of
+(x - r)^2 / (r^2 + 0.01 mean(r)^2). Time is the wall time of the render calls
+(synchronous), guided training included; the time to the target is
+interpolated in log-log between the curve points that bracket it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: one process per GPU under torchrun; each rank is an independent
@@ -70,7 +70,8 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided vs plain time-to-relMSE measurement")
-    p.add_argument("--guiding-ref-spp", type=int, default=65536)
+    p.add_argument("--guiding-ref-spp", type=int, default=1024)
+    p.add_argument("--guiding-res", type=str, default="1920x1080", help="WxH of the guided vs plain measurement")
     p.add_argument("--batch-frames", type=int, default=2,
                    help="frames of the 48-scene animated batch to time (0 = skip)")
     p.add_argument("--no-many-lights", action="store_true", help="skip the many-light city measurement")
@@ -200,7 +201,7 @@ def cpu_baseline(verts, idx, closest, shadow, budget_s):
             "seconds": t_total}
 
 
-GUIDING_RES = (320, 180)
+GUIDING_RES = (1920, 1080)
 GUIDING_DEPTH = 12
 # training schedule measured best on B200 (waves of 8 spp, up to 32 Adam
 # steps of about 16,384 samples after each, 512 steps in all)
@@ -212,16 +213,25 @@ def relmse(x, ref):
     return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2 * ref.mean() ** 2)))
 
 
-def guiding_benchmark(device, ref_spp, target=0.01):
+def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
     """Time to relMSE `target` of plain and guided rendering on the glossy
-    interior (see the module docstring), and the reference CPU renderer's
-    projected time for the plain estimator (its measured samples/s on the
-    same scene x the spp the plain estimator needs)."""
+    interior at res (see the module docstring), and the reference CPU
+    renderer's projected time for the plain estimator (its measured
+    samples/s on the same scene x the spp the plain estimator needs).
+
+    The reference image r is a plain render of ref_spp in two independent
+    halves h1, h2 (different seeds). Its own error is removed from every
+    relMSE: for unbiased x and r, E[(x - r)^2] = Var x + Var r, and
+    (h1 - h2)^2 / 4 is an unbiased per-pixel estimate of Var r, so
+    relMSE(x) = mean(((x - r)^2 - (h1 - h2)^2 / 4) / (r^2 + 0.01 mean(r)^2)).
+    A curve is sampled at growing spp (doubling, then a step aimed just past
+    the target from the measured 1/spp trend) and the time to the target is
+    interpolated in log-log between the two points that bracket it."""
     import math
 
     from alpine_b200 import gpu, scenes
 
-    W, H = GUIDING_RES
+    W, H = res
     scene = scenes.glossy_interior_scene()
 
     def context(**opts):
@@ -238,15 +248,21 @@ def guiding_benchmark(device, ref_spp, target=0.01):
     t0 = time.perf_counter()
     halves = []
     for seed in (1000, 2000):
-        c = context(seed=seed)
+        c = context(seed=seed, shade_order=gpu.SHADE_ORDER_QUEUE)
         c.render(ref_spp // 2)
         halves.append(mean(c))
         c.close()
     ref = 0.5 * (halves[0] + halves[1])
+    ref_var = (halves[0] - halves[1]) ** 2 / 4.0
     ref_s = time.perf_counter() - t0
-    ref_err = relmse(halves[0], halves[1]) / 4  # relMSE of the average against the truth, estimated
+    denom = ref ** 2 + 1e-2 * ref.mean() ** 2
+    ref_err = float(np.mean(ref_var / denom))  # the reference's own relMSE, removed below
+    del halves
 
-    def curve(opts, max_spp=1 << 16):
+    def err(x):
+        return float(np.mean(((x - ref) ** 2 - ref_var) / denom))
+
+    def curve(opts, max_spp=1 << 15):
         c = context(**opts)
         done, elapsed, pts = 0, 0.0, []
         spp = 4
@@ -255,59 +271,54 @@ def guiding_benchmark(device, ref_spp, target=0.01):
             c.render(spp)
             elapsed += time.perf_counter() - t1
             done += spp
-            pts.append((done, elapsed, relmse(mean(c), ref)))
-            if pts[-1][2] < 0.7 * target:
+            e = err(mean(c))
+            pts.append((done, elapsed, e))
+            if e < target:
                 break
-            spp = done
+            # double, or jump to just past the target when the 1/spp trend says it is near
+            want = int(done * e / (0.9 * target)) if e > 0 else 2 * done
+            spp = max(4, min(done, want - done) if want < 2 * done else done)
         steps = c.guide_steps()[0] if opts.get("guide") else 0
         c.close()
         at = None
         for i in range(1, len(pts)):
             (s0, t_0, e0), (s1, t_1, e1) = pts[i - 1], pts[i]
-            if e1 <= target < e0:
+            if e1 <= target < e0 and e0 > 0 and e1 > 0:
                 f = (math.log(target) - math.log(e0)) / (math.log(e1) - math.log(e0))
                 at = (t_0 + f * (t_1 - t_0), math.exp(math.log(s0) + f * (math.log(s1) - math.log(s0))))
                 break
         return at, pts, steps
 
     warm = context(seed=5, **GUIDE_OPTIONS)  # module loading, allocations
-    warm.render(4)
+    warm.render(2)
     warm.close()
-
-    def median_of(opts, repeats):
-        """Each curve `repeats` times (seeds differ): training is online and
-        its gradient sums are unordered, and the machine is shared, so one
-        curve varies by about +-10 %. The run with the median time to the
-        target is reported, and every repeat is listed."""
-        runs = [curve(dict(opts, seed=opts["seed"] + 100 * k)) for k in range(repeats)]
-        timed = sorted((r for r in runs if r[0] is not None), key=lambda r: r[0][0])
-        mid = timed[len(timed) // 2] if timed else runs[0]
-        return mid, [r[0][0] if r[0] else None for r in runs]
-
-    (plain_at, plain_pts, _), plain_all = median_of(dict(seed=1), 3)
-    (guided_at, guided_pts, steps), guided_all = median_of(dict(seed=2, **GUIDE_OPTIONS), 3)
+    # each arm with its measured-best shading order: grouping the queue by
+    # material costs the plain interior 10% and gains the guided one 2%
+    plain_at, plain_pts, _ = curve(dict(seed=1, shade_order=gpu.SHADE_ORDER_QUEUE))
+    guided_at, guided_pts, steps = curve(dict(seed=2, shade_order=gpu.SHADE_ORDER_BY_MATERIAL, **GUIDE_OPTIONS))
     out = {
         "metric": "time to relMSE 0.01, guided vs plain MIS", "unit": "s", "target_relmse": target,
         "scene": "glossy interior, 2.0M triangles, sky 5 through two 1x2 m windows, depth 12, no lights",
         "resolution": [W, H], "reference_spp": ref_spp, "reference_s": ref_s,
-        "reference_relmse_estimate": ref_err,
-        "relmse": "mean((x - r)^2 / (r^2 + 0.01 mean(r)^2))",
+        "reference_relmse_removed": ref_err,
+        "relmse": "mean(((x - r)^2 - (h1 - h2)^2 / 4) / (r^2 + 0.01 mean(r)^2)), r = (h1 + h2) / 2",
         "plain_s": plain_at[0] if plain_at else None, "plain_spp": plain_at[1] if plain_at else None,
         "guided_s": guided_at[0] if guided_at else None, "guided_spp": guided_at[1] if guided_at else None,
         "speedup": (plain_at[0] / guided_at[0]) if plain_at and guided_at else None,
-        "repeats_s": {"plain": plain_all, "guided": guided_all},
         "guide": {k: v for k, v in GUIDE_OPTIONS.items() if k != "guide"} | {"adam_steps": steps},
+        "shade_order": {"plain": "queue", "guided": "by material"},
         "plain_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in plain_pts],
         "guided_curve": [[s, round(t, 4), round(e, 5)] for s, t, e in guided_pts],
     }
-    out["cpu_reference"] = cpu_render_baseline(scene, W, H, out["plain_spp"])
+    out["cpu_reference"] = cpu_render_baseline(scene, 320, 180, out["plain_spp"], W * H)
     return out
 
 
-def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
+def cpu_render_baseline(scene, W, H, plain_spp, pixels, spp=2):
     """The reference renderer (oracle/_ref: class Alpine with its WideBvh) on
-    all host cores: samples/s on the same scene and image, and the time the
-    plain estimator (the same algorithm) would need for plain_spp."""
+    all host cores: samples/s on the same scene at W x H, and the time the
+    plain estimator (the same algorithm) would need for plain_spp samples of
+    `pixels` pixels at that rate."""
     import oracle
 
     from alpine_b200 import scenes
@@ -327,7 +338,7 @@ def cpu_render_baseline(scene, W, H, plain_spp, spp=2):
     rate = spp * W * H / dt
     return {"samples_per_s": rate, "cores": os.cpu_count() or 1, "kind": "reference", "build": ref_build_label(),
             "sample": f"{spp} spp at {W}x{H} after 1 warm-up spp; scene load + BVH build {load_s:.1f} s",
-            "projected_time_to_target_s": (plain_spp * W * H / rate) if plain_spp else None}
+            "projected_time_to_target_s": (plain_spp * pixels / rate) if plain_spp else None}
 
 
 def batch_benchmark(device, frames):
@@ -697,7 +708,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_many_lights:
         many = many_lights_benchmark(local)
     if rank == 0 and world == 1 and not args.no_guiding:
-        guiding = guiding_benchmark(local, args.guiding_ref_spp)
+        gw, gh = (int(x) for x in args.guiding_res.split("x"))
+        guiding = guiding_benchmark(local, args.guiding_ref_spp, res=(gw, gh))
     if rank == 0 and world == 1 and args.batch_frames:
         batched = batch_benchmark(local, args.batch_frames)
     if rank == 0:
