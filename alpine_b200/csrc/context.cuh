@@ -57,6 +57,7 @@ inline std::string status_msg(uint32_t bits)
 }
 
 int upload_render_scene(alpine_gpu_ctx* c);  // render.cu: materials, attributes, lights to the device
+int add_point_light_intensity(alpine_gpu_ctx* c, float3 intensity, float3 position, uint32_t* id);  // render.cu
 int upload_geometry(alpine_gpu_ctx* c);      // api.cu: vertices and indices to the device
 
 // A material record of the C ABI as the device Material: Dielectric or

@@ -1209,3 +1209,20 @@ int alpine_gpu_post_process(alpine_gpu_ctx* c, int tonemap, float* mean_rgb, uin
 namespace ag {
 int upload_render_scene(alpine_gpu_ctx* c) { return upload_scene_data(c); }
 }  // namespace ag
+
+namespace ag {
+// PointLight(intensity, position) (src/lights/point_light.cpp:8-13): the
+// radiant intensity given directly, power = intensity * 4 * pi.
+int add_point_light_intensity(alpine_gpu_ctx* c, float3 intensity, float3 position, uint32_t* id)
+{
+    ag::Light l{};
+    l.kind = ag::kLightPoint;
+    l.scale = 1.0f;
+    l.position = position;
+    l.radiance = intensity;
+    l.power = hmul(hmul(intensity, 4.0f), ag::kPi);
+    float3 corners[1] = {l.position};
+    finish_light(l, corners, 1);
+    return add_light(c, l, id);
+}
+}  // namespace ag

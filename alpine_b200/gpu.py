@@ -68,6 +68,15 @@ class TraversalOptions(C.Structure):
     _fields_ = [("triangle_test", C.c_uint32), ("max_visits", C.c_uint32), ("stack_limit", C.c_uint32)]
 
 
+class GlbInfo(C.Structure):
+    _fields_ = [("shapes", C.c_uint32), ("first_shape", C.c_uint32), ("triangles", C.c_uint32),
+                ("materials", C.c_uint32), ("first_material", C.c_uint32), ("textures", C.c_uint32),
+                ("images", C.c_uint32), ("lights", C.c_uint32), ("channels", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Tuning(C.Structure):
     _fields_ = [("max_paths_per_wave", C.c_uint32), ("trace_block", C.c_uint32), ("samples_per_second", C.c_float)]
 
@@ -123,6 +132,8 @@ def lib():
         L.alpine_gpu_add_texture.argtypes = [vp, vp, C.c_uint32, C.c_uint32, u32p]
         L.alpine_gpu_set_material_textures.argtypes = [vp, C.c_uint32, C.c_int32, C.c_int32]
         L.alpine_gpu_set_environment_map.argtypes = [vp, vp, C.c_uint32, C.c_uint32]
+        L.alpine_gpu_load_glb.argtypes = [vp, C.c_char_p, C.POINTER(GlbInfo)]
+        L.alpine_gpu_glb_inspect.argtypes = [C.c_char_p, C.POINTER(GlbInfo)]
         L.alpine_gpu_add_point_light.argtypes = [vp, C.c_float, f3, f3, u32p]
         L.alpine_gpu_add_disk_light.argtypes = [vp, C.c_float, f3, f3, f3, C.c_float, u32p]
         L.alpine_gpu_add_quad_light.argtypes = [vp, f3, f3, f3, f3, u32p]
@@ -159,6 +170,15 @@ def lib():
                                                  C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
+
+
+def glb_inspect(path) -> dict:
+    """Counts of a .glb file's contents (no context or GPU needed)."""
+    info = GlbInfo()
+    rc = lib().alpine_gpu_glb_inspect(str(path).encode(), C.byref(info))
+    if rc != OK:
+        raise GpuError(rc, f"cannot read {path} as binary glTF")
+    return info.as_dict()
 
 
 def _ptr(a: np.ndarray):
@@ -361,6 +381,12 @@ class Context:
 
     def set_material_textures(self, material, base_color=-1, normal=-1):
         self._check(self.L.alpine_gpu_set_material_textures(self.h, material, base_color, normal))
+
+    def load_glb(self, path) -> dict:
+        """Appends a binary glTF scene (alpine::loadScene, FileType::Gltf)."""
+        info = GlbInfo()
+        self._check(self.L.alpine_gpu_load_glb(self.h, str(path).encode(), C.byref(info)))
+        return info.as_dict()
 
     def set_environment_map(self, rgb):
         """float32 [H, W, 3] lat-long map (None removes it)."""

@@ -292,6 +292,35 @@ ALPINE_GPU_API int alpine_gpu_set_material_textures(alpine_gpu_ctx* ctx, uint32_
 ALPINE_GPU_API int alpine_gpu_set_environment_map(alpine_gpu_ctx* ctx, const float* rgb, uint32_t width,
                                                   uint32_t height);
 
+/* Binary glTF scenes (alpine::loadScene with FileType::Gltf, alpine.h:30;
+ * src/loaders/gltf_loader.cpp). alpine_gpu_load_glb appends a .glb file's
+ * scene to the context with the reference loader's semantics: its materials
+ * (Conductor when metallicFactor > 0, else Dielectric; alpha =
+ * roughnessFactor; base-colour and normal textures from 8-bit PNG images) to
+ * the material table; one mesh per glTF mesh, in mesh order, with the
+ * positions, normals and tangents transformed by the node's matrix, vertex
+ * normals, texture coordinates and tangents; morph targets and LINEAR
+ * "weights" animation channels (alpine_gpu_update_scene then animates them);
+ * KHR_lights_punctual lights as point lights of intensity colour *
+ * intensity. Call alpine_gpu_build afterwards. The file is read by the
+ * project's own GLB parser (the reference uses tinygltf). Writes what was
+ * added (info may be NULL).
+ * alpine_gpu_glb_inspect parses a file without a context (no GPU needed) and
+ * writes its counts (shapes = glTF meshes, first_* = 0). */
+typedef struct alpine_gpu_glb_info {
+    uint32_t shapes;          /* meshes added (shape ids first_shape, first_shape + 1, ...) */
+    uint32_t first_shape;
+    uint32_t triangles;
+    uint32_t materials;       /* materials appended (ids first_material, ...) */
+    uint32_t first_material;
+    uint32_t textures;        /* textures created */
+    uint32_t images;
+    uint32_t lights;
+    uint32_t channels;        /* animation channels (inspect: all; load: the ones applied) */
+} alpine_gpu_glb_info;
+ALPINE_GPU_API int alpine_gpu_load_glb(alpine_gpu_ctx* ctx, const char* path, alpine_gpu_glb_info* info);
+ALPINE_GPU_API int alpine_gpu_glb_inspect(const char* path, alpine_gpu_glb_info* info);
+
 /* Lights (alpine::addPointLight / addDiskLight, include/alpine/alpine.h:35-42;
  * src/lights/). A quad light is a one-sided emitting parallelogram
  * corner + [0,1] edge_u + [0,1] edge_v with constant radiance, emitting on the

@@ -147,6 +147,14 @@ def ref(timing: bool = False, plugin: bool = False):
         L.ref_render_add_mesh_ex.restype = C.c_int
         L.ref_render_set_environment.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.ref_render_load_obj.argtypes = [C.c_char_p]
+        L.ref_render_load_glb.argtypes = [C.c_char_p]
+        L.ref_render_load_glb.restype = C.c_int
+        L.ref_render_shape_count.restype = C.c_uint32
+        L.ref_render_mesh_data.argtypes = [C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_render_mesh_data.restype = C.c_uint32
+        L.ref_render_light_count.restype = C.c_uint32
+        L.ref_render_light_info.argtypes = [C.c_uint32, _f32p, _f32p]
         L.ref_render_load_obj.restype = C.c_int
         L.ref_render_add_disk_light.argtypes = [C.c_float, _f32p, _f32p, _f32p, C.c_float]
         L.ref_render_add_point_light.argtypes = [C.c_float, _f32p, _f32p]
@@ -282,6 +290,37 @@ class RefRenderer:
         """Texture4f from float32 [H, W, 4]; returns its id."""
         t = np.ascontiguousarray(rgba, np.float32)
         return self.L.ref_render_add_texture(t.reshape(-1), t.shape[1], t.shape[0])
+
+    def load_glb(self, path):
+        """alpine::loadScene(path, FileType::Gltf): the reference's GltfLoader."""
+        if not self.L.ref_render_load_glb(str(path).encode()):
+            raise RuntimeError(f"reference loader failed on {path}")
+
+    def meshes(self):
+        """The loaded scene's meshes as the reference holds them: dicts of
+        positions, normals, uvs, tangents (Mesh::Data), prims and the current
+        (possibly morphed) vertex buffer."""
+        out = []
+        for i in range(self.L.ref_render_shape_count()):
+            nt = C.c_uint32()
+            nv = self.L.ref_render_mesh_data(i, C.byref(nt), None, None, None, None, None, None)
+            d = {k: np.zeros((nv, c), np.float32) for k, c in (("pos", 3), ("nrm", 3), ("uv", 2), ("tan", 4),
+                                                                 ("current", 3))}
+            d["prims"] = np.zeros((nt.value, 3), np.uint32)
+            self.L.ref_render_mesh_data(i, C.byref(nt), d["pos"].ctypes.data, d["nrm"].ctypes.data,
+                                        d["uv"].ctypes.data, d["tan"].ctypes.data, d["prims"].ctypes.data,
+                                        d["current"].ctypes.data)
+            out.append(d)
+        return out
+
+    def lights(self):
+        """(power RGB, position) of every light of the loaded scene."""
+        res = []
+        for i in range(self.L.ref_render_light_count()):
+            p, q = np.zeros(3, np.float32), np.zeros(3, np.float32)
+            self.L.ref_render_light_info(i, p, q)
+            res.append((p, q))
+        return res
 
     def set_environment_map(self, rgb):
         """Alpine::mEnvironmentMap from float32 [H, W, 3] (None removes it)."""

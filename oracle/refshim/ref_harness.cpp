@@ -27,10 +27,13 @@
 // maintainer's branch in alpine.cpp would.
 //
 // The reference's loaders need tinyobjloader / tinygltf / stb, which are not
-// vendored; this harness therefore defines loadObj/loadGltf/loadHdr
+// vendored; this harness therefore defines loadObj and loadHdr
 // (src/loaders/file_loader.h:10-12): loadObj is a minimal reader for the
 // `v / vn / f / usemtl / mtllib Kd` subset, building Mesh::Data the way
-// src/loaders/obj_loader.cpp:45-119 does; GLB and HDR loading report failure.
+// src/loaders/obj_loader.cpp:45-119 does; HDR loading reports failure. The
+// reference's own GLB loader (src/loaders/gltf_loader.cpp) is compiled
+// unchanged against refshim/tinygltf/tiny_gltf.h, a stand-in for tinygltf's
+// model filled by the project's GLB reader.
 
 // Standard headers first, so that the `private` redefinition below only
 // reaches the reference's own headers.
@@ -171,12 +174,6 @@ loadObj(Scene* scene, std::string_view filename)
     return true;
 }
 
-bool
-loadGltf(Scene*, std::string_view)
-{
-    printf("ERROR: GLB loading needs tinygltf, which is not vendored.\n");
-    return false;
-}
 
 bool
 loadHdr(std::unique_ptr<EnvironmentMap>&, std::string_view)
@@ -725,6 +722,53 @@ ref_render_add_morph_mesh(const float* verts, uint32_t nverts, const uint32_t* t
 }
 
 int ref_render_load_obj(const char* path) { return loadScene(path, FileType::Obj) ? 1 : 0; }
+
+// alpine::loadScene(path, FileType::Gltf): the reference's GltfLoader.
+int ref_render_load_glb(const char* path) { return loadScene(path, FileType::Gltf) ? 1 : 0; }
+
+// The loaded scene as the reference holds it: shape count, and one mesh's
+// Mesh::Data (positions / normals / uvs / tangents: floats, may be null;
+// prims: 3 per triangle) and the current (possibly morphed) vertex buffer
+// the accelerator holds. Returns the vertex count and writes the triangle count.
+uint32_t ref_render_shape_count() { return (uint32_t)alpine::alpine().mScene.shapes.size(); }
+
+uint32_t
+ref_render_mesh_data(uint32_t i, uint32_t* ntris, float* pos, float* nrm, float* uv, float* tan, uint32_t* prims,
+    float* current)
+{
+    auto& a = alpine::alpine();
+    auto* mesh = dynamic_cast<Mesh*>(a.mScene.shapes[i].get());
+    if (!mesh) { return 0; }
+    const auto& d = mesh->mData;
+    *ntris = (uint32_t)d.prims.size();
+    for (size_t v = 0; v < d.vertices.size(); ++v)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            if (pos) { pos[3 * v + k] = d.vertices[v][k]; }
+            if (nrm && v < d.normals.size()) { nrm[3 * v + k] = d.normals[v][k]; }
+            if (current) { current[3 * v + k] = mesh->mVertexBuffer[v][k]; }
+        }
+        if (uv && v < d.uvs.size()) { uv[2 * v] = d.uvs[v].x; uv[2 * v + 1] = d.uvs[v].y; }
+        if (tan && v < d.tangents.size()) { for (int k = 0; k < 4; ++k) { tan[4 * v + k] = d.tangents[v][k]; } }
+    }
+    if (prims)
+    {
+        for (size_t t = 0; t < d.prims.size(); ++t) { for (int k = 0; k < 3; ++k) { prims[3 * t + k] = d.prims[t][k]; } }
+    }
+    return (uint32_t)d.vertices.size();
+}
+
+// Light i of the loaded scene: power (getPower, RGB) and position.
+void
+ref_render_light_info(uint32_t i, float* power, float* position)
+{
+    auto& l = alpine::alpine().mScene.lights[i];
+    float3 p = l->getPower();
+    float3 c = l->getBoundingBox().getCenter();  // a point light's box is its position
+    for (int k = 0; k < 3; ++k) { power[k] = p[k]; position[k] = c[k]; }
+}
+uint32_t ref_render_light_count() { return (uint32_t)alpine::alpine().mScene.lights.size(); }
 
 #ifdef ALPINE_GPU_PLUGIN
 #define GPU_BRANCH(call) do { if (sGpu) { sGpu->call; } } while (0)
