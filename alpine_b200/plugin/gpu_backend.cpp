@@ -41,6 +41,8 @@ GpuBackend::resetScene(bool binaryRule)
 {
     if (!mCtx) { return false; }
     mMaterials.clear();
+    mTextureBindings.clear();
+    mGlbMaterials = 0;
     mMaterialsDirty = true;
     mGeometryDirty = true;
     alpine_gpu_traversal_options o{
@@ -114,6 +116,78 @@ GpuBackend::addMesh(const std::vector<float3>& vertices, const std::vector<float
     return (int)id;
 }
 
+bool
+GpuBackend::setMeshUvs(int shape, const std::vector<float2>& uvs, const std::vector<float4>& tangents)
+{
+    if (!mCtx || shape < 0 || uvs.empty()) { return uvs.empty(); }
+    return ok(alpine_gpu_set_triangle_uvs(mCtx, (uint32_t)shape, &uvs[0][0], tangents.empty() ? nullptr : &tangents[0][0]),
+              "setMeshUvs");
+}
+
+int
+GpuBackend::addTexture(const std::vector<float4>& texels, uint32_t width, uint32_t height)
+{
+    uint32_t id = 0;
+    if (!mCtx || texels.size() != (size_t)width * height) { return -1; }
+    return ok(alpine_gpu_add_texture(mCtx, &texels[0][0], width, height, &id), "addTexture") ? (int)id : -1;
+}
+
+bool
+GpuBackend::setMaterialTextures(uint32_t material, int baseColorTexture, int normalTexture)
+{
+    // the material table reaches the context at the next render: bind then
+    mTextureBindings.push_back({material, baseColorTexture, normalTexture});
+    mMaterialsDirty = true;
+    return true;
+}
+
+bool
+GpuBackend::loadGlb(const char* path)
+{
+    if (!mCtx) { return false; }
+    // materials added before stay in front of the file's
+    if (mMaterialsDirty && !flushMaterials()) { return false; }
+    alpine_gpu_glb_info info{};
+    if (!ok(alpine_gpu_load_glb(mCtx, path, &info), "loadGlb")) { return false; }
+    mGlbMaterials += info.materials;
+    mGeometryDirty = true;
+    return true;
+}
+
+bool
+GpuBackend::setEnvironmentMap(const std::vector<float3>& texels, uint32_t width, uint32_t height)
+{
+    if (!mCtx) { return false; }
+    if (texels.empty()) { return ok(alpine_gpu_set_environment_map(mCtx, nullptr, 0, 0), "setEnvironmentMap"); }
+    return ok(alpine_gpu_set_environment_map(mCtx, &texels[0][0], width, height), "setEnvironmentMap");
+}
+
+bool
+GpuBackend::flushMaterials()
+{
+    if (mGlbMaterials)
+    {
+        // a loaded GLB appended its own materials to the context's table; the
+        // records added here come first and are set again with them
+        mError = "GpuBackend: addMaterials after loadGlb is not supported";
+        return false;
+    }
+    if (!ok(alpine_gpu_set_materials(mCtx, mMaterials.empty() ? nullptr : mMaterials.data(), (uint32_t)mMaterials.size()),
+            "render"))
+    {
+        return false;
+    }
+    for (const auto& b : mTextureBindings)
+    {
+        if (!ok(alpine_gpu_set_material_textures(mCtx, b.material, b.base, b.normal), "setMaterialTextures"))
+        {
+            return false;
+        }
+    }
+    mMaterialsDirty = false;
+    return true;
+}
+
 int
 GpuBackend::addPointLight(float power, const float color[3], const float position[3])
 {
@@ -171,16 +245,7 @@ bool
 GpuBackend::render(uint32_t spp)
 {
     if (!mCtx) { return false; }
-    if (mMaterialsDirty)
-    {
-        if (!ok(alpine_gpu_set_materials(mCtx, mMaterials.empty() ? nullptr : mMaterials.data(),
-                    (uint32_t)mMaterials.size()),
-                "render"))
-        {
-            return false;
-        }
-        mMaterialsDirty = false;
-    }
+    if (mMaterialsDirty && !flushMaterials()) { return false; }
     if (mGeometryDirty)
     {
         if (!ok(alpine_gpu_build(mCtx, nullptr), "render")) { return false; }

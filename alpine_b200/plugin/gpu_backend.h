@@ -8,6 +8,8 @@
 //   Alpine::resetScene                       -> resetScene
 //   Alpine::loadScene (per Mesh::Data)       -> addMesh (positions, normals,
 //                                               material ids) + materials
+//   Alpine::loadScene (FileType::Gltf)       -> loadGlb (the whole file)
+//   Alpine::loadEnvironmentMap               -> setEnvironmentMap
 //   Alpine::addPointLight / addDiskLight     -> addPointLight / addDiskLight
 //   LightHandle::setScale                    -> setLightScale
 //   Alpine::buildLightSampler                -> buildLightSampler
@@ -56,6 +58,21 @@ public:
         const std::vector<uint3>& prims, const std::vector<uint3>& normalPrims,
         const std::vector<uint32_t>& materialIds);
 
+    // Texture coordinates and tangents of a mesh added by addMesh, per vertex
+    // (Mesh::Data uvs / tangents); either may be empty.
+    bool setMeshUvs(int shape, const std::vector<float2>& uvs, const std::vector<float4>& tangents);
+
+    // A texture (the loader's Texture4f data); returns its id or -1.
+    int addTexture(const std::vector<float4>& texels, uint32_t width, uint32_t height);
+    // Binds textures (-1 = none) to a material appended by addMaterials.
+    bool setMaterialTextures(uint32_t material, int baseColorTexture, int normalTexture);
+
+    // A whole binary glTF file (alpine_gpu_load_glb); false on failure.
+    bool loadGlb(const char* path);
+
+    // The lat-long environment map (width x height RGB texels); empty removes it.
+    bool setEnvironmentMap(const std::vector<float3>& texels, uint32_t width, uint32_t height);
+
     // Appends material records (the loaders' Dielectric / Conductor with
     // alpha = roughness); returns the index of the first one.
     uint32_t addMaterials(const std::vector<alpine_gpu_material>& materials);
@@ -80,6 +97,15 @@ public:
 
 private:
     bool ok(int rc, const char* what);
+    bool flushMaterials();
+
+    struct TextureBinding
+    {
+        uint32_t material;
+        int base, normal;
+    };
+    std::vector<TextureBinding> mTextureBindings;
+    uint32_t mGlbMaterials = 0;
 
     alpine_gpu_ctx* mCtx = nullptr;
     uint32_t mWidth = 0, mHeight = 0;

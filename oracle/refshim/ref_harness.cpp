@@ -541,12 +541,21 @@ ref_render_add_mesh(const float* verts, uint32_t nverts, const uint32_t* tris, u
     return 1;
 }
 
+#ifdef ALPINE_GPU_PLUGIN
+#define GPU_BRANCH(call) do { if (sGpu) { sGpu->call; } } while (0)
+#else
+#define GPU_BRANCH(call) do { } while (0)
+#endif
+
 // Texture4f of w x h float4 texels (row-major); returns its id.
 int
 ref_render_add_texture(const float* rgba, uint32_t w, uint32_t h)
 {
     std::vector<float4> d((size_t)w * h);
     for (size_t i = 0; i < d.size(); ++i) { d[i] = float4(rgba[4 * i], rgba[4 * i + 1], rgba[4 * i + 2], rgba[4 * i + 3]); }
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu && sGpu->addTexture(d, w, h) != (int)sTextures.size()) { return -1; }
+#endif
     sTextures.push_back(std::make_shared<Texture4f>(w, h, std::move(d)));
     return static_cast<int>(sTextures.size() - 1);
 }
@@ -580,6 +589,23 @@ ref_render_add_mesh_ex(const float* verts, uint32_t nverts, const uint32_t* tris
             d.tangents[i] = float4(tangents[4 * i], tangents[4 * i + 1], tangents[4 * i + 2], tangents[4 * i + 3]);
         }
     }
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu)
+    {
+        std::vector<alpine_gpu_material> recs(nmat);
+        for (uint32_t m = 0; m < nmat; ++m) { recs[m] = to_gpu_material(materials + 7 * m); }
+        uint32_t base = sGpu->addMaterials(recs);
+        for (uint32_t m = 0; m < nmat; ++m)
+        {
+            const int bt = (int)materials[7 * m + 5], nt = (int)materials[7 * m + 6];
+            if (bt >= 0 || nt >= 0) { sGpu->setMaterialTextures(base + m, bt, nt); }
+        }
+        std::vector<uint32_t> ids(ntris);
+        for (uint32_t i = 0; i < ntris; ++i) { ids[i] = base + triMaterial[i]; }
+        int sid = sGpu->addMesh(d.vertices, d.normals, d.prims, d.normalPrims, ids);
+        if (sid < 0 || !sGpu->setMeshUvs(sid, d.uvs, d.tangents)) { return 0; }
+    }
+#endif
     std::vector<std::shared_ptr<Material>> mats(nmat);
     for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 7 * m, 7); }
     d.prims.resize(ntris);
@@ -603,9 +629,14 @@ void
 ref_render_set_environment(const float* rgb, uint32_t w, uint32_t h)
 {
     auto& a = alpine::alpine();
-    if (!rgb) { a.mEnvironmentMap.reset(); return; }
+    if (!rgb) {
+        a.mEnvironmentMap.reset();
+        GPU_BRANCH(setEnvironmentMap({}, 0, 0));
+        return;
+    }
     std::vector<float3> d((size_t)w * h);
     for (size_t i = 0; i < d.size(); ++i) { d[i] = float3(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]); }
+    GPU_BRANCH(setEnvironmentMap(d, w, h));
     a.mEnvironmentMap = std::make_unique<EnvironmentMap>(std::move(d), w, h);
 }
 
@@ -724,7 +755,14 @@ ref_render_add_morph_mesh(const float* verts, uint32_t nverts, const uint32_t* t
 int ref_render_load_obj(const char* path) { return loadScene(path, FileType::Obj) ? 1 : 0; }
 
 // alpine::loadScene(path, FileType::Gltf): the reference's GltfLoader.
-int ref_render_load_glb(const char* path) { return loadScene(path, FileType::Gltf) ? 1 : 0; }
+int
+ref_render_load_glb(const char* path)
+{
+#ifdef ALPINE_GPU_PLUGIN
+    if (sGpu && !sGpu->loadGlb(path)) { return 0; }
+#endif
+    return loadScene(path, FileType::Gltf) ? 1 : 0;
+}
 
 // The loaded scene as the reference holds it: shape count, and one mesh's
 // Mesh::Data (positions / normals / uvs / tangents: floats, may be null;
@@ -770,11 +808,6 @@ ref_render_light_info(uint32_t i, float* power, float* position)
 }
 uint32_t ref_render_light_count() { return (uint32_t)alpine::alpine().mScene.lights.size(); }
 
-#ifdef ALPINE_GPU_PLUGIN
-#define GPU_BRANCH(call) do { if (sGpu) { sGpu->call; } } while (0)
-#else
-#define GPU_BRANCH(call) do { } while (0)
-#endif
 
 void
 ref_render_add_disk_light(float power, const float* color, const float* pos, const float* target, float radius)

@@ -98,13 +98,15 @@ def test_alpine_render_with_gpu_accelerator(binary):
     assert same > 0.995
 
 
-def test_alpine_render_through_gpu_branch():
+@pytest.mark.parametrize("which", ["room", "textured"])
+def test_alpine_render_through_gpu_branch(which):
     """The GpuBackend render branch: Alpine's render state forwarded to the GPU
     integrator (counter RNG). z-test of the reference's own render (256 spp)
     against the branch's batches (16 x 1024 spp), both read back through the
-    Alpine's accumulation; the reference's postProcess runs on the GPU sums."""
+    Alpine's accumulation; the reference's postProcess runs on the GPU sums.
+    The textured scene adds textures, tangents and the environment map."""
     w = h = 24
-    scene = scenes.room_scene(seed=4, light="quad")
+    scene = scenes.room_scene(seed=4, light="quad") if which == "room" else scenes.textured_scene(seed=3)
     R = oracle.RefRenderer
     r = R(w, h, 8, accelerator=R.ACC_WIDE_BVH)
     scenes.load_scene(r, scene, w, h)
@@ -134,6 +136,7 @@ def test_alpine_render_through_gpu_branch():
     se = np.sqrt(var1 / 256 + var1 / (16 * 1024))
     ok = se > 1e-7
     z = (rmean - gmean)[ok] / se[ok]
-    print(f"GPU render branch z-test: |z|>5 fraction {(np.abs(z) > 5).mean():.4f}, mean z {z.mean():.3f}")
+    print(f"GPU render branch z-test ({which}): |z|>5 fraction {(np.abs(z) > 5).mean():.4f}, mean z {z.mean():.3f}")
+    assert np.allclose(rmean[~ok], gmean[~ok], rtol=1e-4, atol=1e-6)
     assert (np.abs(z) > 5).mean() < 0.02 and abs(z.mean()) < 0.25
     assert ldr.shape == (h, w, 3) and ldr.max() > 0
