@@ -26,9 +26,9 @@ rendered together (morph + BVH rebuild + render per scene per frame).
 `guiding` (rank 0, one GPU): time to relMSE 0.01, guided vs plain MIS, on the
 glossy interior (20 x 4 x 12 m room, 2.0M triangles, 70% GGX with roughness
 in [0.02, 0.4], sky of radiance 5 through two 1 x 2 m window openings, depth
-12) at 1920 x 1080, against a 1,024-spp plain image rendered in the same run
-in two independent halves, whose own error is removed from every relMSE (see
-guiding_benchmark). relMSE = mean over pixels and channels of
+12) at 1920 x 1080, against a 2,048-spp image rendered in the same run by the
+trained, frozen guided estimator in two independent halves, whose own error is
+removed from every relMSE (see guiding_benchmark). relMSE = mean over pixels and channels of
 (x - r)^2 / (r^2 + 0.01 mean(r)^2). Time is the wall time of the render calls
 (synchronous), guided training included; the time to the target is
 interpolated in log-log between the curve points that bracket it.
@@ -70,7 +70,7 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided vs plain time-to-relMSE measurement")
-    p.add_argument("--guiding-ref-spp", type=int, default=1024)
+    p.add_argument("--guiding-ref-spp", type=int, default=2048)
     p.add_argument("--guiding-res", type=str, default="1920x1080", help="WxH of the guided vs plain measurement")
     p.add_argument("--batch-frames", type=int, default=2,
                    help="frames of the 48-scene animated batch to time (0 = skip)")
@@ -165,8 +165,8 @@ def ref_build_label():
     import oracle
 
     name = os.path.basename(oracle.timing_build())
-    flags = {"libalpine_ref_fast_v4.so": "-O3 -march=x86-64-v4 (AVX-512) -mtune=native, FMA contraction",
-             "libalpine_ref_fast_v3.so": "-O3 -march=x86-64-v3 (AVX2) -mtune=native, FMA contraction",
+    flags = {"libalpine_ref_fast_v4.so": "-O3 -march=x86-64-v4 (AVX-512) -ffp-contract=off",
+             "libalpine_ref_fast_v3.so": "-O3 -march=x86-64-v3 (AVX2) -ffp-contract=off",
              "libalpine_ref.so": "-O3 -march=x86-64-v3 -ffp-contract=off (parity build)"}
     return f"{name}: {flags.get(name, '?')}"
 
@@ -219,11 +219,18 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
     renderer's projected time for the plain estimator (its measured
     samples/s on the same scene x the spp the plain estimator needs).
 
-    The reference image r is a plain render of ref_spp in two independent
+    The reference image r is ref_spp samples of the guided estimator (its
+    guide trained, then frozen: an unbiased estimator for that fixed guide,
+    with far less variance per second than plain MIS) in two independent
     halves h1, h2 (different seeds). Its own error is removed from every
     relMSE: for unbiased x and r, E[(x - r)^2] = Var x + Var r, and
     (h1 - h2)^2 / 4 is an unbiased per-pixel estimate of Var r, so
     relMSE(x) = mean(((x - r)^2 - (h1 - h2)^2 / 4) / (r^2 + 0.01 mean(r)^2)).
+    (A plain 1,024-spp reference at this resolution has about 8x the target
+    error itself; its noise then correlates with the denominator enough that
+    the subtraction leaves a bias near the target.) A curve that has not
+    reached the target after max_s seconds reports the 1/spp extrapolation
+    of its last point, marked as such.
     A curve is sampled at growing spp (doubling, then a step aimed just past
     the target from the measured 1/spp trend) and the time to the target is
     interpolated in log-log between the two points that bracket it."""
@@ -246,12 +253,19 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
         return a[..., :3].astype(np.float64) / n
 
     t0 = time.perf_counter()
+    # the reference: the guided estimator, trained and then frozen, in two
+    # halves of independent samples (for a fixed guide the estimator is
+    # unbiased; per unit time it has far less variance than plain MIS)
+    c = context(seed=999, **GUIDE_OPTIONS)
+    c.render(64)  # trains the guide (512 Adam steps) and warms up
     halves = []
     for seed in (1000, 2000):
-        c = context(seed=seed, shade_order=gpu.SHADE_ORDER_QUEUE)
+        c.set_render_options(sampler=gpu.RNG_COUNTER, accumulate_fp64=True, seed=seed,
+                             **dict(GUIDE_OPTIONS, guide_train=False))
+        c.reset_accumulation()
         c.render(ref_spp // 2)
         halves.append(mean(c))
-        c.close()
+    c.close()
     ref = 0.5 * (halves[0] + halves[1])
     ref_var = (halves[0] - halves[1]) ** 2 / 4.0
     ref_s = time.perf_counter() - t0
@@ -262,17 +276,19 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
     def err(x):
         return float(np.mean(((x - ref) ** 2 - ref_var) / denom))
 
-    def curve(opts, max_spp=1 << 15):
+    def curve(opts, max_spp=1 << 15, max_s=240.0):
         c = context(**opts)
         done, elapsed, pts = 0, 0.0, []
         spp = 4
-        while done < max_spp:
+        while done < max_spp and elapsed < max_s:
             t1 = time.perf_counter()
             c.render(spp)
             elapsed += time.perf_counter() - t1
             done += spp
             e = err(mean(c))
             pts.append((done, elapsed, e))
+            print(f"guiding curve {'guided' if opts.get('guide') else 'plain'}: {done} spp {elapsed:.2f} s "
+                  f"relMSE {e:.5f}", file=sys.stderr, flush=True)
             if e < target:
                 break
             # double, or jump to just past the target when the 1/spp trend says it is near
@@ -287,6 +303,11 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
                 f = (math.log(target) - math.log(e0)) / (math.log(e1) - math.log(e0))
                 at = (t_0 + f * (t_1 - t_0), math.exp(math.log(s0) + f * (math.log(s1) - math.log(s0))))
                 break
+        if at is None and pts and pts[-1][2] > 0:
+            # not reached within the time cap: the 1/spp trend of the last
+            # point, marked as extrapolated
+            s_, t_, e_ = pts[-1]
+            at = (t_ * e_ / target, s_ * e_ / target, "extrapolated")
         return at, pts, steps
 
     warm = context(seed=5, **GUIDE_OPTIONS)  # module loading, allocations
@@ -302,6 +323,9 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES):
         "resolution": [W, H], "reference_spp": ref_spp, "reference_s": ref_s,
         "reference_relmse_removed": ref_err,
         "relmse": "mean(((x - r)^2 - (h1 - h2)^2 / 4) / (r^2 + 0.01 mean(r)^2)), r = (h1 + h2) / 2",
+        "reference": "the guided estimator after its 512 training steps, frozen, in two independent halves",
+        "plain_extrapolated": bool(plain_at and len(plain_at) > 2),
+        "guided_extrapolated": bool(guided_at and len(guided_at) > 2),
         "plain_s": plain_at[0] if plain_at else None, "plain_spp": plain_at[1] if plain_at else None,
         "guided_s": guided_at[0] if guided_at else None, "guided_spp": guided_at[1] if guided_at else None,
         "speedup": (plain_at[0] / guided_at[0]) if plain_at and guided_at else None,

@@ -13,9 +13,9 @@ ctypes bindings to two CPU libraries built by ``oracle/Makefile``:
 * ``_ref/libalpine_ref_plugin.so`` -- the parity build plus the GPU plug-in a
   maintainer adds to the reference (``alpine_b200/plugin``: GpuAccelerator
   and the GpuBackend render branch), for the boundary tests (``plugin=True``).
-* ``_ref/libalpine_ref_fast_v3.so`` / ``_v4.so`` -- the same sources built for
-  speed (FMA contraction, AVX2 / AVX-512); used only by the timed CPU arms
-  (``timing=True``), never for parity.
+* ``_ref/libalpine_ref_fast_v3.so`` / ``_v4.so`` -- the same sources built with
+  the host's vector ISA (AVX2 / AVX-512, no FMA contraction); used only by the
+  timed CPU arms (``timing=True``).
 
 Only the tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline and
 reference arms use this package. The product (``alpine_b200``) never imports it.
