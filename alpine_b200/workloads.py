@@ -12,6 +12,8 @@ first render's launches.
     python -m alpine_b200.workloads interior_guided # the same guided with the time-to-relMSE schedule
                                                     # (8 spp waves, 32 Adam steps per wave, 512 steps):
                                                     # 256 spp while training, then 64 spp
+    python -m alpine_b200.workloads interior_guided_1080  # the same schedule at 1920x1080: 32 spp
+                                                          # (training ends within them), then 8 spp
 """
 from __future__ import annotations
 
@@ -31,10 +33,15 @@ def run(mode: str, device: int = 0) -> float:
         opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
                     guide_min_roughness=0.2, guide_train_steps=16)
         sampler, spp = None, (32, 32)
-    elif mode in ("interior", "interior_guided"):
-        sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
+    elif mode in ("interior", "interior_guided", "interior_guided_1080"):
+        big = mode == "interior_guided_1080"
+        sc, (W, H), depth = scenes.glossy_interior_scene(), ((1920, 1080) if big else (320, 180)), 12
         opts, sampler, spp = dict(accumulate_fp64=True), None, (64, 64)
-        if mode == "interior_guided":
+        if big:
+            opts.update(guide=True, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=32, guide_lr=1e-2,
+                        guide_min_roughness=0.2, guide_train_steps=512, shade_order=gpu.SHADE_ORDER_BY_MATERIAL)
+            spp = (32, 8)
+        elif mode == "interior_guided":
             opts.update(guide=True, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=32, guide_lr=1e-2,
                         guide_min_roughness=0.2, guide_train_steps=512)
             spp = (256, 64)
