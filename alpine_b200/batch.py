@@ -11,7 +11,9 @@ with a per-object phase, keyed at 60 frames. The BVH is rebuilt every frame.
 graph) per scene. A frame morphs and rebuilds every scene, enqueues every
 render without waiting, then waits for all. Contexts are independent, so the
 GPU runs the renders of different scenes concurrently, overlapping them with
-the host-driven rebuilds of the next scenes.
+the rebuilds of other scenes; the scenes' morph + rebuild + enqueue run on a
+pool of host threads, so the per-level host waits of their rebuilds overlap
+too.
 """
 from __future__ import annotations
 
@@ -130,10 +132,15 @@ class BatchRenderer:
     """One context per scene; frames are rendered concurrently (see the
     module docstring)."""
 
-    def __init__(self, configs, device=0, depth=8, cuda_graph=True, sampler=gpu.SAMPLER_BVH, autotune=False):
+    def __init__(self, configs, device=0, depth=8, cuda_graph=True, sampler=gpu.SAMPLER_BVH, autotune=False,
+                 threads=16):
+        import concurrent.futures as cf
+
         self.configs = configs
         self.ctxs = []
         self.triangles = 0
+        self.threads = threads
+        self._pool = cf.ThreadPoolExecutor(max_workers=max(1, threads))
         for cfg in configs:
             scene = batch_scene(cfg["seed"], cfg["tris"])
             c = gpu.Context(device, cfg["width"], cfg["height"], depth)
@@ -147,23 +154,35 @@ class BatchRenderer:
             self.triangles += sum(m["idx"].shape[0] for m in scene["meshes"])
             self.ctxs.append(c)
 
-    def frame(self, t):
+    def frame(self, t, threads=None):
         """Morph + rebuild + render every scene at time t; returns the summed
-        device build time (ms)."""
-        build_ms = 0.0
-        for c, cfg in zip(self.ctxs, self.configs):
-            build_ms += c.update_scene(t)["build_ms"]
+        device build time (ms). A scene's rebuild waits on the host once per
+        BVH level; with threads > 1 the scenes' morph + rebuild + render
+        enqueue run on a pool of host threads (each context is used by one
+        thread at a time; the C calls release the GIL), so those waits
+        overlap instead of adding up."""
+        threads = self.threads if threads is None else threads
+
+        def one(i):
+            c, cfg = self.ctxs[i], self.configs[i]
+            ms = c.update_scene(t)["build_ms"]
             c.render_async(cfg["spp"])
+            return ms
+
+        if threads > 1:
+            build_ms = sum(self._pool.map(one, range(len(self.ctxs))))
+        else:
+            build_ms = sum(one(i) for i in range(len(self.ctxs)))
         for c in self.ctxs:
             c.render_wait()
         return build_ms
 
-    def run(self, frames, start=0):
+    def run(self, frames, start=0, threads=None):
         """Renders `frames` frames; returns wall time, build time and rates."""
         t0 = time.perf_counter()
         build = 0.0
         for f in range(start, start + frames):
-            build += self.frame(float(f))
+            build += self.frame(float(f), threads)
         dt = time.perf_counter() - t0
         samples = frames * sum(c["width"] * c["height"] * c["spp"] for c in self.configs)
         return {"frames": frames, "seconds": dt, "frames_per_s": frames / dt, "samples_per_s": samples / dt,
@@ -173,3 +192,4 @@ class BatchRenderer:
         for c in self.ctxs:
             c.close()
         self.ctxs = []
+        self._pool.shutdown()

@@ -377,7 +377,10 @@ def batch_benchmark(device, frames):
     br = batch.BatchRenderer(cfgs, device=device, cuda_graph=True)
     setup = time.perf_counter() - t0
     br.run(1, start=0)
-    r = br.run(frames, start=1)
+    serial = br.run(frames, start=1, threads=1)
+    r = br.run(frames, start=1 + frames)
+    r["one_host_thread"] = {k: serial[k] for k in ("seconds", "frames_per_s", "samples_per_s", "build_ms_per_frame")}
+    r["host_threads"] = br.threads
     r.update({"scenes": len(cfgs), "triangles": br.triangles, "setup_s": setup,
               "samples_per_frame": sum(c["width"] * c["height"] * c["spp"] for c in cfgs),
               "workload": "48 scenes, tris log-uniform 1k-500k, res 128^2-1024^2, spp 4/16/64, 1-64 quad lights, "
