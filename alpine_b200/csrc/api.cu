@@ -42,6 +42,12 @@ int upload_geometry_now(alpine_gpu_ctx* c)
     cudaError_t e = cudaSuccess;
     if (vb) e = cudaMemcpyAsync(c->dVerts.ptr, c->verts.data(), vb, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess && ib) e = cudaMemcpyAsync(c->dIdx.ptr, c->idx.data(), ib, cudaMemcpyHostToDevice, c->stream);
+    const size_t sb = c->spheres.size() * sizeof(float4), mb = c->sphereMaterial.size() * sizeof(uint32_t);
+    if (!c->dSpheres.reserve(sb) || !c->dSphereMaterial.reserve(mb))
+        return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "sphere upload: cudaMalloc failed");
+    if (e == cudaSuccess && sb) e = cudaMemcpyAsync(c->dSpheres.ptr, c->spheres.data(), sb, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && mb)
+        e = cudaMemcpyAsync(c->dSphereMaterial.ptr, c->sphereMaterial.data(), mb, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, cuda_msg("geometry upload", e));
     c->geometryDirty = false;
     return ALPINE_GPU_OK;
@@ -188,6 +194,8 @@ int alpine_gpu_reset_scene(alpine_gpu_ctx* c)
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     c->verts.clear();
     c->idx.clear();
+    c->spheres.clear();
+    c->sphereMaterial.clear();
     c->morphs.clear();
     c->channels.clear();
     c->hostVertsStale = c->hostNormalsStale = false;
@@ -239,6 +247,27 @@ int alpine_gpu_add_mesh(alpine_gpu_ctx* c, const float* vertices, uint32_t vcoun
     return ALPINE_GPU_OK;
 }
 
+int alpine_gpu_add_spheres(alpine_gpu_ctx* c, const float* spheres, uint32_t count, const uint32_t* material,
+                           uint32_t* first_sphere)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (count && !spheres) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_spheres: null array");
+    if (c->spheres.size() + count >= (size_t)ag::kSpherePrim)
+        return c->fail(ALPINE_GPU_ERR_LIMIT, "add_spheres: more than 2^31 - 1 spheres");
+    if (first_sphere) *first_sphere = (uint32_t)c->spheres.size();
+    for (uint32_t i = 0; i < count; ++i) {
+        float4 v;
+        std::memcpy(&v, spheres + 4ull * i, sizeof v);
+        const uint32_t m = material ? material[i] : 0u;
+        if (m & ~ag::kTriMaterialMask) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "add_spheres: material id too large");
+        c->spheres.push_back(v);
+        c->sphereMaterial.push_back(m);
+    }
+    c->geometryDirty = true;
+    c->bvhDirty = true;
+    return ALPINE_GPU_OK;
+}
+
 int alpine_gpu_update_vertices(alpine_gpu_ctx* c, uint32_t shape, const float* vertices)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
@@ -258,22 +287,26 @@ int alpine_gpu_build(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats)
     cudaSetDevice(c->device);
     if (int rc = upload_geometry_now(c)) return rc;
     uint32_t n = (uint32_t)(c->idx.size() / 3);
-    if (!c->dNodes.reserve((size_t(n) + 1) * sizeof(ag::WideNode)) || !c->dTris.reserve(size_t(n) * sizeof(ag::TriRecord)))
+    const uint32_t ns = (uint32_t)c->spheres.size();
+    const size_t prims = size_t(n) + ns;
+    if (!c->dNodes.reserve((prims + 1) * sizeof(ag::WideNode)) || !c->dTris.reserve(prims * sizeof(ag::TriRecord)))
         return c->fail(ALPINE_GPU_ERR_OUT_OF_MEMORY, "build: cudaMalloc failed");
     ag::BuildStats bs;
     char err[256] = {0};
-    int rc = c->builder.build(c->dVerts.as<float>(), c->dIdx.as<uint32_t>(), n, c->dNodes.as<ag::WideNode>(),
-                              c->dTris.as<ag::TriRecord>(), c->dStatus, c->stream, &bs, err, sizeof err);
+    int rc = c->builder.build(c->dVerts.as<float>(), c->dIdx.as<uint32_t>(), n, c->dSpheres.as<float4>(), ns,
+                              c->dNodes.as<ag::WideNode>(), c->dTris.as<ag::TriRecord>(), c->dStatus, c->stream, &bs,
+                              err, sizeof err);
     if (rc) {
         c->nodeCount = 0;
         c->triCount = 0;
         int code = rc == -2 ? ALPINE_GPU_ERR_CUDA : (rc == -5 ? ALPINE_GPU_ERR_OUT_OF_MEMORY : ALPINE_GPU_ERR_LIMIT);
         return c->fail(code, err);
     }
-    c->nodeCount = n ? bs.wideNodes : 0;
-    c->triCount = n;
+    c->nodeCount = prims ? bs.wideNodes : 0;
+    c->triCount = (uint32_t)prims;
     c->bvhDirty = false;
     c->stats.triangles = n;
+    c->stats.spheres = ns;
     c->stats.binary_nodes = bs.binaryNodes;
     c->stats.binary_levels = bs.binaryLevels;
     c->stats.wide_nodes = bs.wideNodes;

@@ -251,25 +251,37 @@ AG_D void write_cand(Cand* c, const float* b, uint32_t begin, uint32_t count)
 
 // --------------------------------------------------------------------------
 // Preparation: primitive boxes and root bounds.
-__global__ void k_prep_prims(const float* __restrict__ verts, const uint32_t* __restrict__ idx, uint32_t n,
-                             float4* __restrict__ primLo, float4* __restrict__ primHi, uint32_t* __restrict__ refs,
-                             uint32_t* __restrict__ bounds)
+// Primitives 0 .. ntris-1 are triangles, ntris .. n-1 spheres (centre +
+// radius): their box is centre -+ radius.
+__global__ void k_prep_prims(const float* __restrict__ verts, const uint32_t* __restrict__ idx, uint32_t ntris,
+                             const float4* __restrict__ spheres, uint32_t n, float4* __restrict__ primLo,
+                             float4* __restrict__ primHi, uint32_t* __restrict__ refs, uint32_t* __restrict__ bounds)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     float c[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, cmx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     if (i < n) {
-        const uint32_t* t = idx + 3ull * i;
-        float p[3][3];
-#pragma unroll
-        for (int v = 0; v < 3; ++v)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) p[v][k] = verts[3ull * t[v] + k];
         float l[3], h[3];
+        if (i < ntris) {
+            const uint32_t* t = idx + 3ull * i;
+            float p[3][3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) p[v][k] = verts[3ull * t[v] + k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                l[k] = fminf(fminf(p[0][k], p[1][k]), p[2][k]);
+                h[k] = fmaxf(fmaxf(p[0][k], p[1][k]), p[2][k]);
+            }
+        } else {
+            const float4 sp = spheres[i - ntris];
+            const float r = fabsf(sp.w);
+            l[0] = __fsub_rd(sp.x, r); l[1] = __fsub_rd(sp.y, r); l[2] = __fsub_rd(sp.z, r);
+            h[0] = __fadd_ru(sp.x, r); h[1] = __fadd_ru(sp.y, r); h[2] = __fadd_ru(sp.z, r);
+        }
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            l[k] = fminf(fminf(p[0][k], p[1][k]), p[2][k]);
-            h[k] = fmaxf(fmaxf(p[0][k], p[1][k]), p[2][k]);
             lo[k] = l[k];
             hi[k] = h[k];
             c[k] = cmx[k] = centroid(l[k], h[k]);
@@ -817,7 +829,8 @@ __global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numIte
                                 const int32_t* __restrict__ slots, const uint32_t* __restrict__ intOff,
                                 const uint32_t* __restrict__ triOff, uint32_t wideBase, uint32_t triBase0,
                                 const uint32_t* __restrict__ order, const float* __restrict__ verts,
-                                const uint32_t* __restrict__ idx, WideNode* __restrict__ nodes,
+                                const uint32_t* __restrict__ idx, uint32_t ntris, const float4* __restrict__ spheres,
+                                WideNode* __restrict__ nodes,
                                 TriRecord* __restrict__ tris, uint2* __restrict__ itemsNext, float* sahAccum,
                                 float rootAreaInv, uint32_t nodeCap, uint32_t triCap, uint32_t* __restrict__ status)
 {
@@ -866,6 +879,16 @@ __global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numIte
             meta[s] = (uint8_t)((((1u << c.count) - 1u) << 5) | toff);
             for (uint32_t k = 0; k < c.count; ++k) {
                 uint32_t prim = order[c.begin + k];
+                if (prim >= ntris) {  // a sphere record
+                    const float4 sp = spheres[prim - ntris];
+                    TriRecord r;
+                    r.v0 = make_float4(sp.x, sp.y, sp.z, __uint_as_float(kSpherePrim | (prim - ntris)));
+                    r.e0 = make_float4(fabsf(sp.w), 0.0f, 0.0f, __uint_as_float(kSphereTag));
+                    r.e1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (triBase + toff + k < triCap) tris[triBase + toff + k] = r;
+                    else atomicOr(status, kErrBadIndex);
+                    continue;
+                }
                 const uint32_t* ti = idx + 3ull * prim;
                 float v0[3], v1[3], v2[3];
                 for (int a = 0; a < 3; ++a) {
@@ -1015,9 +1038,11 @@ int Builder::reserve(uint32_t n, char* err, size_t errLen)
     return 0;
 }
 
-int Builder::build(const float* verts, const uint32_t* idx, uint32_t n, WideNode* nodes, TriRecord* tris,
-                   uint32_t* deviceStatus, cudaStream_t st, BuildStats* stats, char* err, size_t errLen)
+int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres, uint32_t nspheres,
+                   WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t st, BuildStats* stats,
+                   char* err, size_t errLen)
 {
+    const uint32_t n = ntris + nspheres;
     BuildStats local;
     if (n == 0) {
         if (stats) *stats = local;
@@ -1033,7 +1058,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t n, WideNode
 
     cudaEventRecord(ev0_, st);
     k_init_bounds<<<1, 32, 0, st>>>(bounds);
-    k_prep_prims<<<blocks_for(N, 256), 256, 0, st>>>(verts, idx, n, primLo_, primHi_, refs_[0], bounds);
+    k_prep_prims<<<blocks_for(N, 256), 256, 0, st>>>(verts, idx, ntris, spheres, n, primLo_, primHi_, refs_[0], bounds);
     uint32_t numTasks = 1;
     uint32_t numBig = n > kSmallMax ? 1u : 0u;
     uint32_t totalChunks = numBig ? (n + kChunk - 1) / kChunk : 0u;
@@ -1110,7 +1135,8 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t n, WideNode
         exclusive_scan(intCount_, intOff_, numItems, counters_ + kCntInt, scanScratch_, st);
         exclusive_scan(triCount_, triOff_, numItems, counters_ + kCntTri, scanScratch_, st);
         k_collapse_emit<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intOff_, triOff_,
-                                                                    wideCount, triCount, order_, verts, idx, nodes,
+                                                                    wideCount, triCount, order_, verts, idx, ntris,
+                                                                    spheres, nodes,
                                                                     tris, itemsNext, sahAccum_, rootAreaInv, n + 1, n,
                                                                     deviceStatus);
         cudaMemcpyAsync(hostCounters_ + kCntInt, counters_ + kCntInt, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,

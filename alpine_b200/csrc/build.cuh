@@ -26,11 +26,14 @@ public:
     Builder(const Builder&) = delete;
     Builder& operator=(const Builder&) = delete;
 
-    // verts: float[3 * nverts] (device), idx: uint32[3 * ntris] (device).
-    // Outputs: nodes (nodeCapacity >= ntris + 1), tris (ntris records).
+    // verts: float[3 * nverts] (device), idx: uint32[3 * ntris] (device),
+    // spheres: float4[nspheres] centre + radius (device, may be null when 0).
+    // Primitives are the triangles, then the spheres. Outputs: nodes
+    // (capacity >= ntris + nspheres + 1), tris (ntris + nspheres records).
     // Returns 0 on success, a negative code on failure (message in err).
-    int build(const float* verts, const uint32_t* idx, uint32_t ntris, WideNode* nodes, TriRecord* tris,
-              uint32_t* deviceStatus, cudaStream_t stream, BuildStats* stats, char* err, size_t errLen);
+    int build(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres, uint32_t nspheres,
+              WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t stream, BuildStats* stats,
+              char* err, size_t errLen);
 
 private:
     int reserve(uint32_t ntris, char* err, size_t errLen);

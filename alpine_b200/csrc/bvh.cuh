@@ -23,6 +23,9 @@
 // Triangle record (48 bytes, three 128-bit loads): {v0.xyz, prim id},
 // {e0.xyz, 0}, {e1.xyz, 0} with e0 = v1 - v0 and e1 = v2 - v0, the same FP32
 // values the reference intersects (src/accelerators/bvh_common.cpp:105-125).
+// A sphere (an analytic primitive, Sphere::Data vertices: centre + radius)
+// shares the record: {centre.xyz, kSpherePrim | sphere index},
+// {radius, 0, 0, tag kSphereTag}, unused; a triangle's e0.w is 0.
 #pragma once
 
 #include "common.cuh"
@@ -58,6 +61,9 @@ struct alignas(16) BinNode {
     uint32_t pad[2];
 };
 static_assert(sizeof(BinNode) == 48, "binary node is 48 bytes");
+
+constexpr uint32_t kSpherePrim = 0x80000000u;  // hit / record prim ids of spheres carry this bit
+constexpr uint32_t kSphereTag = 1u;            // e0.w bits of a sphere record
 
 constexpr int kWidth = 8;
 constexpr int kMaxLeafTris = 3;          // unary count field holds 1..3

@@ -97,6 +97,10 @@ struct alpine_gpu_ctx {
     bool geometryDirty = true;      // device vertex/index copy out of date
     bool bvhDirty = true;           // BVH out of date w.r.t. geometry
     ag::DeviceBuffer dVerts, dIdx;
+    // analytic spheres (Sphere::Data: centre + radius, material per sphere)
+    std::vector<float4> spheres;
+    std::vector<uint32_t> sphereMaterial;
+    ag::DeviceBuffer dSpheres, dSphereMaterial;
 
     // acceleration structure
     ag::Builder builder;

@@ -39,6 +39,9 @@ struct SceneView {
     uint32_t textureCount;
     const float* env;          // lat-long environment map (3 floats per texel), null = background colour
     uint32_t envW, envH;
+    const float4* spheres;     // analytic spheres: centre, radius
+    const uint32_t* sphereMaterial;
+    uint32_t sphereCount;
     const Material* materials;
     uint32_t materialCount;
     LightSamplerView lights;
@@ -272,9 +275,29 @@ struct Surface {
     Material mat;
 };
 
-AG_D void surface_at(const SceneView& sc, const uint4 h, Surface& s)
+AG_D void surface_at(const SceneView& sc, const uint4 h, float3 ro, float3 rd, Surface& s)
 {
     const uint32_t prim = h.x;
+    if (prim & kSpherePrim) {
+        // Sphere::getIntersectionAttributes (src/shapes/sphere.cpp:23-37):
+        // ns = ng, the outward normal at the hit; the sphere's material
+        uint32_t k = prim & ~kSpherePrim;
+        if (k >= sc.sphereCount) k = 0;
+        const float4 sp = sc.spheres[k];
+        const float3 hit = ro + rd * __uint_as_float(h.y);
+        s.ng = normalize3(hit - mk3(sp.x, sp.y, sp.z));
+        s.ns = s.ng;
+        uint32_t mid = sc.sphereMaterial[k];
+        if (mid >= sc.materialCount) mid = 0;
+        s.mat = sc.materials[mid];
+        if (s.mat.baseTex && s.mat.baseTex <= sc.textureCount) {  // uv = 0 on a sphere
+            const float4 t = texture_sample(sc.textures[s.mat.baseTex - 1u], sc.texels, 0.0f, 0.0f);
+            s.mat.r = t.x;
+            s.mat.g = t.y;
+            s.mat.b = t.z;
+        }
+        return;
+    }
     const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
     const uint32_t* ti = sc.idx + 3ull * prim;
     const uint32_t i0 = ti[0], i1 = ti[1], i2 = ti[2];
@@ -393,8 +416,8 @@ __global__ void __launch_bounds__(kThreads) k_guide_query(SceneView sc, WaveView
     if (h.x != 0xffffffffu) {
         const alpine_gpu_ray ray = w.rays[q];
         Surface sf;
-        surface_at(sc, h, sf);
         const float3 rd = mk3(ray.dir[0], ray.dir[1], ray.dir[2]);
+        surface_at(sc, h, mk3(ray.org[0], ray.org[1], ray.org[2]), rd, sf);
         // wo.z of the shading frame: to_local(-rd, ss, ts, ns).z
         guided = dot(sf.ns, -rd) > 0.0f && sf.mat.ax >= w.guideMinRough;
         if (guided) {
@@ -453,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, kGuided ? AG_SHADE_MIN_BLOCKS_GUIDED
     } else {
         const float t = __uint_as_float(h.y);
         Surface sf;
-        surface_at(sc, h, sf);
+        surface_at(sc, h, ro, rd, sf);
         const float3 ng = sf.ng, ns = sf.ns;
         const Material mat = sf.mat;
         float3 ss, ts;
@@ -586,7 +609,8 @@ AG_D uint32_t shade_key(const SceneView& sc, const WaveView& w, uint32_t q)
     const uint32_t prim = w.hits[q].x;
     uint32_t key = 0;
     if (prim != 0xffffffffu) {
-        uint32_t mid = __ldg(sc.triInfo + prim) & kTriMaterialMask;
+        uint32_t mid = (prim & kSpherePrim) ? sc.sphereMaterial[min(prim & ~kSpherePrim, sc.sphereCount - 1u)]
+                                            : __ldg(sc.triInfo + prim) & kTriMaterialMask;
         if (mid >= sc.materialCount) mid = 0;
         const Material& m = sc.materials[mid];
         key = m.kind == kMatConductor ? 3u : (m.lobes == 2u ? 2u : 1u);

@@ -817,6 +817,9 @@ static int render_enqueue(alpine_gpu_ctx* c, uint32_t spp)
     sc.texels = c->dTexels.as<float4>();
     sc.textureCount = (uint32_t)c->textures.size();
     sc.env = c->envW ? c->dEnv.as<float>() : nullptr;
+    sc.spheres = c->dSpheres.as<float4>();
+    sc.sphereMaterial = c->dSphereMaterial.as<uint32_t>();
+    sc.sphereCount = (uint32_t)c->spheres.size();
     sc.envW = c->envW;
     sc.envH = c->envH;
     sc.materials = c->dMaterials.as<ag::Material>();

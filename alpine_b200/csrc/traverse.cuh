@@ -100,6 +100,28 @@ AG_D bool tri_test_binary(float3 o, float3 d, float4 v0, float4 e0, float4 e1, f
     return true;
 }
 
+// Ray / sphere: the geometric form (the projection of the centre on the
+// ray and the squared distance of the ray from it), front hit first, then the
+// back hit for a ray starting inside, each accepted in [tmin, tmax).
+// Embree's point-sphere intersector (Embree 4.3, the reference's only sphere
+// path, src/accelerators/embree.cpp:107-122) publishes this method; it is
+// restated here.
+AG_D bool sphere_test(float3 o, float3 d, float4 c, float r, float tmin, float tmax, float& t)
+{
+    const float cx = c.x - o.x, cy = c.y - o.y, cz = c.z - o.z;
+    const float rd2 = 1.0f / (d.x * d.x + d.y * d.y + d.z * d.z);
+    const float proj = (cx * d.x + cy * d.y + cz * d.z) * rd2;
+    const float px = cx - proj * d.x, py = cy - proj * d.y, pz = cz - proj * d.z;
+    const float l2 = px * px + py * py + pz * pz;
+    const float r2 = r * r;
+    if (!(l2 <= r2)) return false;
+    const float td = sqrtf((r2 - l2) * rd2);
+    const float tf = proj - td, tb = proj + td;
+    if (tf >= tmin && tf < tmax) { t = tf; return true; }
+    if (tb >= tmin && tb < tmax) { t = tb; return true; }
+    return false;
+}
+
 struct TraceResult {
     uint32_t prim;
     float t, b1, b2;
@@ -240,8 +262,14 @@ AG_D bool ray_step(const BvhView& bvh, RayState& s, uint2* stack, int stride, ui
         const TriRecord* r = bvh.tris + ti;
         float4 v0 = __ldg(&r->v0), e0 = __ldg(&r->e0), e1 = __ldg(&r->e1);
         float t, b1, b2;
-        const bool accepted = kBinary ? tri_test_binary(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2)
-                                      : tri_test(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2);
+        bool accepted;
+        if (__float_as_uint(e0.w) == kSphereTag) {
+            accepted = sphere_test(s.o, s.d, v0, e0.x, s.tmin, s.tmax, t);
+            b1 = b2 = 0.0f;
+        } else {
+            accepted = kBinary ? tri_test_binary(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2)
+                               : tri_test(s.o, s.d, v0, e0, e1, s.tmin, s.tmax, t, b1, b2);
+        }
         if (accepted) {
             s.res.prim = __float_as_uint(v0.w);
             s.res.t = t;

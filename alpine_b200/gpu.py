@@ -48,7 +48,7 @@ class Config(C.Structure):
 class BvhStats(C.Structure):
     _fields_ = [("triangles", C.c_uint32), ("binary_nodes", C.c_uint32), ("binary_levels", C.c_uint32),
                 ("wide_nodes", C.c_uint32), ("wide_depth", C.c_uint32), ("sah_cost", C.c_float),
-                ("build_ms", C.c_float)]
+                ("build_ms", C.c_float), ("spheres", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -109,6 +109,7 @@ def lib():
         L.alpine_gpu_last_error.restype = C.c_char_p
         L.alpine_gpu_reset_scene.argtypes = [vp]
         L.alpine_gpu_add_mesh.argtypes = [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.alpine_gpu_add_spheres.argtypes = [vp, vp, C.c_uint32, vp, C.POINTER(C.c_uint32)]
         L.alpine_gpu_update_vertices.argtypes = [vp, C.c_uint32, vp]
         L.alpine_gpu_build.argtypes = [vp, C.POINTER(BvhStats)]
         L.alpine_gpu_set_morph_targets.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint32]
@@ -222,6 +223,16 @@ class Context:
         sid = C.c_uint32()
         self._check(self.L.alpine_gpu_add_mesh(self.h, _ptr(v), v.shape[0], _ptr(i), i.shape[0], C.byref(sid)))
         return sid.value
+
+    def add_spheres(self, spheres, material=None) -> int:
+        """Analytic spheres float[N, 4] (centre, radius), material id per
+        sphere; returns the index of the first (hits report 0x80000000 | index)."""
+        s = np.ascontiguousarray(spheres, np.float32).reshape(-1, 4)
+        m = None if material is None else np.ascontiguousarray(material, np.uint32)
+        first = C.c_uint32()
+        self._check(self.L.alpine_gpu_add_spheres(self.h, _ptr(s), s.shape[0], None if m is None else _ptr(m),
+                                                  C.byref(first)))
+        return first.value
 
     def update_vertices(self, shape, verts):
         v = np.ascontiguousarray(verts, np.float32)

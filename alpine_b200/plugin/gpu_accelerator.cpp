@@ -80,9 +80,18 @@ GpuAccelerator::appendMesh(const std::vector<float3>& vertices, const std::vecto
 }
 
 void
-GpuAccelerator::appendSphere(const std::vector<float4>&, const void*)
+GpuAccelerator::appendSphere(const std::vector<float4>& vertices, const void* ptr)
 {
-    printf("ERROR: Sphere intersection has not been implemented yet.");
+    std::lock_guard<std::mutex> lock(mMutex);
+    if (!mCtx || vertices.empty()) { return; }
+    uint32_t first = 0;
+    int rc = alpine_gpu_add_spheres(mCtx, &vertices[0][0], (uint32_t)vertices.size(), nullptr, &first);
+    if (rc != ALPINE_GPU_OK)
+    {
+        report(rc, "appendSphere");
+        return;
+    }
+    mSphereShapes.push_back({ptr, first, vertices});
 }
 
 void*
@@ -109,8 +118,23 @@ GpuAccelerator::updateScene()
 }
 
 Intersection
-GpuAccelerator::toIntersection(const alpine_gpu_hit& h) const
+GpuAccelerator::toIntersection(const alpine_gpu_hit& h, const Ray& ray) const
 {
+    if (h.prim & 0x80000000u)
+    {
+        const uint32_t k = h.prim & 0x7fffffffu;
+        size_t s = mSphereShapes.size() - 1;
+        while (s > 0 && mSphereShapes[s].first > k) { --s; }
+        const SphereShape& sh = mSphereShapes[s];
+        const float4& c = sh.spheres[k - sh.first];
+        Intersection i;
+        i.shapePtr = sh.ptr;
+        i.primId = k - sh.first;
+        i.ng = normalize(ray.org + ray.dir * h.t - float3(c.x, c.y, c.z));
+        i.barycentric = float2(0.0f, 0.0f);
+        i.t = h.t;
+        return i;
+    }
     // the shape holding global triangle h.prim (shapes are in triBase order)
     size_t lo = 0, hi = mShapes.size();
     while (hi - lo > 1)
@@ -161,7 +185,7 @@ GpuAccelerator::intersectBatch(const Ray* rays, size_t n, std::optional<Intersec
     for (size_t i = 0; i < n; ++i)
     {
         if (h[i].prim == 0xffffffffu) { out[i].reset(); }
-        else { out[i] = toIntersection(h[i]); }
+        else { out[i] = toIntersection(h[i], rays[i]); }
     }
 }
 

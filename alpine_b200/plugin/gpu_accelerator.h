@@ -19,8 +19,11 @@
 //   the per-ray path is correct but slow (one round trip per ray). Callers
 //   that can batch use intersectBatch / intersectAnyBatch, and the whole
 //   integrator runs on the GPU through GpuBackend (gpu_backend.h).
-// * Spheres: appendSphere reports an error, as the reference's own Bvh and
-//   WideBvh do (src/accelerators/bvh.cpp:107-111).
+// * Spheres: appendSphere adds analytic spheres (Sphere::Data vertices:
+//   centre + radius) to the same BVH, as the reference's Embree accelerator
+//   does (src/accelerators/embree.cpp:107-122; its Bvh and WideBvh print an
+//   error instead). A sphere hit reports the sphere's index in its shape as
+//   primId and ng = normalize(hit - centre), as Embree's normalised Ng.
 #pragma once
 
 #include <accelerators/accelerator.h>
@@ -76,12 +79,20 @@ private:
         std::vector<float3> ng;               // per triangle, as Primitive::ng
     };
 
+    struct SphereShape
+    {
+        const void* ptr = nullptr;
+        uint32_t first = 0;                   // global index of the shape's first sphere
+        std::vector<float4> spheres;
+    };
+
     static void computeNormals(Shape& s);
-    Intersection toIntersection(const alpine_gpu_hit& h) const;
+    Intersection toIntersection(const alpine_gpu_hit& h, const Ray& ray) const;
     void report(int rc, const char* what) const;
 
     alpine_gpu_ctx* mCtx = nullptr;
     std::vector<Shape> mShapes;
+    std::vector<SphereShape> mSphereShapes;
     uint32_t mTriCount = 0;
     mutable std::mutex mMutex;
 };

@@ -76,6 +76,7 @@ typedef struct alpine_gpu_bvh_stats {
     uint32_t wide_depth;
     float sah_cost;      /* SAH cost of the wide tree, relative to the root area */
     float build_ms;      /* device time of the last build */
+    uint32_t spheres;    /* analytic spheres in the BVH */
 } alpine_gpu_bvh_stats;
 
 /* Creates a context on cfg->device (replaces alpine::initialize,
@@ -98,6 +99,20 @@ ALPINE_GPU_API int alpine_gpu_reset_scene(alpine_gpu_ctx* ctx);
  * (0, 1, ... in call order). */
 ALPINE_GPU_API int alpine_gpu_add_mesh(alpine_gpu_ctx* ctx, const float* vertices, uint32_t vertex_count, const uint32_t* indices,
                         uint32_t triangle_count, uint32_t* shape_id);
+
+/* Appends analytic spheres (Accelerator::appendSphere,
+ * src/accelerators/accelerator.h:24; Sphere::Data, src/shapes/sphere.h:14-18):
+ * float[4 * count] = centre xyz, radius; a material id per sphere (NULL:
+ * material 0). They share the BVH with the triangles (next build). A hit on
+ * sphere k reports prim = 0x80000000 | k (spheres numbered across calls in
+ * the order added), t, and b1 = b2 = 0. The ray / sphere test takes the
+ * front hit, else the back hit of a ray starting inside, in [tmin, tmax);
+ * rendering shades a sphere with its outward normal (Sphere::
+ * getIntersectionAttributes, sphere.cpp:23-37: ns = ng). In the reference
+ * only the Embree accelerator intersects spheres. Writes the index of the
+ * first sphere added. */
+ALPINE_GPU_API int alpine_gpu_add_spheres(alpine_gpu_ctx* ctx, const float* spheres, uint32_t count,
+                                          const uint32_t* material, uint32_t* first_sphere);
 
 /* Replaces the vertex positions of one mesh (Accelerator::getVertexBuffer +
  * updateShape, accelerator.h:27-29). Takes effect at the next build. */

@@ -206,6 +206,33 @@ def tri_test_batch(rays, tris, prim, sem=TRI_ISPC):
     return hit.astype(bool), t, b1, b2
 
 
+def sphere_hits_fp64(rays, spheres):
+    """Analytic ray / sphere intersections in FP64 (numpy): for rays [N, 8]
+    and spheres [M, 4] (centre, radius), the front hit, else the back hit of
+    a ray starting inside, in [tmin, tmax). Returns t [N, M] (inf on a miss)
+    and the tangency margin |r^2 - l^2| / r^2 (l the ray's distance from the
+    centre), small where FP32 and FP64 may disagree on hit or miss."""
+    r = np.asarray(rays, np.float64)
+    sp = np.asarray(spheres, np.float64)
+    o, tmin, d, tmax = r[:, None, 0:3], r[:, None, 3], r[:, None, 4:7], r[:, None, 7]
+    c = sp[None, :, 0:3] - o
+    rad = np.abs(sp[None, :, 3])
+    dd = np.sum(d * d, -1)
+    proj = np.sum(c * d, -1) / dd
+    perp = c - proj[..., None] * d
+    l2 = np.sum(perp * perp, -1)
+    r2 = rad * rad
+    with np.errstate(invalid="ignore"):
+        td = np.sqrt(np.maximum(r2 - l2, 0.0) / dd)
+    tf, tb = proj - td, proj + td
+    hit = l2 <= r2
+    front = hit & (tf >= tmin) & (tf < tmax)
+    back = hit & ~front & (tb >= tmin) & (tb < tmax)
+    t = np.where(front, tf, np.where(back, tb, np.inf))
+    margin = np.abs(r2 - l2) / np.maximum(r2, 1e-300)
+    return t, margin
+
+
 def tri_fp64(ray, tri):
     t, b1, b2 = C.c_double(), C.c_double(), C.c_double()
     cond = np.zeros(3, np.float64)
