@@ -1,6 +1,7 @@
 """Small fixed rendering workloads for profiling (ncu launch lists and
 captures) and quick timing. Each renders twice, so a capture can skip the
-first render's launches.
+first render's launches (or, with AG_NVTX=1, select the second render's by
+its NVTX range "measure").
 
     python -m alpine_b200.workloads room     # 256x256, 2 x 16 spp, depth 8, RR from depth 3,
                                              # power sampler, quad ceiling light (the small room)
@@ -17,6 +18,7 @@ first render's launches.
 """
 from __future__ import annotations
 
+import os
 import sys
 import time
 
@@ -59,9 +61,19 @@ def run(mode: str, device: int = 0) -> float:
     c.set_render_options(sampler=gpu.RNG_COUNTER, **opts)
     c.reset_accumulation()
     c.render(spp[0])
+    # an NVTX range "measure" around the second render when AG_NVTX=1, so a
+    # profiler can capture its launches alone (ncu --nvtx --nvtx-include measure/)
+    nvtx = None
+    if os.environ.get("AG_NVTX") == "1":
+        import torch
+
+        nvtx = torch.cuda.nvtx
+        nvtx.range_push("measure")
     t0 = time.perf_counter()
     c.render(spp[1])
     dt = time.perf_counter() - t0
+    if nvtx is not None:
+        nvtx.range_pop()
     c.close()
     return dt
 
