@@ -5,6 +5,7 @@ its NVTX range "measure").
 
     python -m alpine_b200.workloads room     # 256x256, 2 x 16 spp, depth 8, RR from depth 3,
                                              # power sampler, quad ceiling light (the small room)
+    python -m alpine_b200.workloads room_queue  # the same, shading in queue order (not grouped by material)
     python -m alpine_b200.workloads guided   # glossy interior 320x180, depth 12, guided:
                                              # 16 Adam steps, then 2 x 32 spp
     python -m alpine_b200.workloads guided_tc  # the same with the tcgen05 inference kernel
@@ -27,9 +28,11 @@ from . import gpu, scenes
 
 def run(mode: str, device: int = 0) -> float:
     """Runs one workload; returns the wall time of its second render (s)."""
-    if mode == "room":
+    if mode in ("room", "room_queue"):
         sc, (W, H), depth = scenes.room_scene(light="quad"), (256, 256), 8
         opts, sampler, spp = dict(russian_roulette_depth=3), gpu.SAMPLER_POWER, (16, 16)
+        if mode == "room_queue":  # shading in traversal-queue order
+            opts["shade_order"] = gpu.SHADE_ORDER_QUEUE
     elif mode in ("guided", "guided_tc"):
         sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
         opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
