@@ -589,6 +589,17 @@ ref_render_add_mesh_ex(const float* verts, uint32_t nverts, const uint32_t* tris
             d.tangents[i] = float4(tangents[4 * i], tangents[4 * i + 1], tangents[4 * i + 2], tangents[4 * i + 3]);
         }
     }
+    std::vector<std::shared_ptr<Material>> mats(nmat);
+    for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 7 * m, 7); }
+    d.prims.resize(ntris);
+    d.materials.resize(ntris);
+    for (uint32_t i = 0; i < ntris; ++i)
+    {
+        d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]);
+        uint32_t m = triMaterial[i];
+        if (m >= nmat) { return 0; }
+        d.materials[i] = mats[m];
+    }
 #ifdef ALPINE_GPU_PLUGIN
     if (sGpu)
     {
@@ -606,17 +617,6 @@ ref_render_add_mesh_ex(const float* verts, uint32_t nverts, const uint32_t* tris
         if (sid < 0 || !sGpu->setMeshUvs(sid, d.uvs, d.tangents)) { return 0; }
     }
 #endif
-    std::vector<std::shared_ptr<Material>> mats(nmat);
-    for (uint32_t m = 0; m < nmat; ++m) { mats[m] = make_ref_material(materials + 7 * m, 7); }
-    d.prims.resize(ntris);
-    d.materials.resize(ntris);
-    for (uint32_t i = 0; i < ntris; ++i)
-    {
-        d.prims[i] = uint3(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]);
-        uint32_t m = triMaterial[i];
-        if (m >= nmat) { return 0; }
-        d.materials[i] = mats[m];
-    }
     auto mesh = std::make_shared<Mesh>(std::move(d), 0);
     auto& a = alpine::alpine();
     a.mScene.shapes.push_back(mesh);
