@@ -675,6 +675,127 @@ __global__ void __launch_bounds__(32) k_dw(const __nv_bfloat16* __restrict__ XT,
     }
 }
 
+// k_dw_tc: the same product on the 5th-generation tensor cores. One CTA of
+// 128 threads per (split of the samples, layer) accumulates
+// dW_l = dY_l^T X_l in tensor memory: per chunk of 64 samples it stages
+// A = dY_l^T (the layer's output rows, zero-padded to M = 128 so that the
+// accumulator has the lane-per-row layout of k_infer_tc) and B = X_l^T
+// (N = 64 input rows), both K-major over the samples, in the no-swizzle
+// core-matrix layout, and one elected thread issues four tcgen05.mma
+// (K = 16 each) and commits them to an mbarrier. Samples beyond n are staged
+// as zeros. Warps 0 and 1 then read rows 0..63 back (tcgen05.ld) into the
+// split's partial dW, summed by k_reduce_dw like k_dw's. Every wait is
+// bounded: a CTA that runs out records kErrTensorWait, writes nothing, and
+// still frees its tensor memory.
+constexpr int kDwTcChunk = 64;                                   // samples per stage (K)
+constexpr int kDwTcATile = kTcRows * kDwTcChunk * 2;             // 16 KiB
+constexpr int kDwTcBTile = kHidden * kDwTcChunk * 2;             // 8 KiB
+constexpr int kDwTcSmem = kDwTcATile + kDwTcBTile + 16;
+static_assert(kTrainSlice % kDwTcChunk == 0, "whole chunks per slice");
+
+__global__ void __launch_bounds__(kTcRows) k_dw_tc(const __nv_bfloat16* __restrict__ XT,
+                                                   const __nv_bfloat16* __restrict__ DT, uint32_t n,
+                                                   float* __restrict__ partial, uint32_t* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* at = smem;
+    unsigned char* bt = smem + kDwTcATile;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(bt + kDwTcBTile);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bt + kDwTcBTile + 8);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const int l = blockIdx.y;
+    const int rows = layer_out(l);
+    const uint32_t split = blockIdx.x, splits = gridDim.x;
+    const uint32_t chunks = (n + kDwTcChunk - 1) / kDwTcChunk, per = (chunks + splits - 1) / splits;
+    const uint32_t c0 = split * per, c1 = min(chunks, c0 + per);
+    const __nv_bfloat16* A = DT + (uint64_t)l * kHidden * kTrainSlice;  // row m: dY_l[., m] over the samples
+    const __nv_bfloat16* B = XT + (uint64_t)l * kHidden * kTrainSlice;  // row k: X_l[., k]
+
+    // the padding rows of A (rows .. 127) stay zero for the whole kernel
+    for (int i = tid; i < (kTcRows - rows) * (kDwTcChunk / 8); i += kTcRows) {
+        const uint32_t row = (uint32_t)(rows + i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
+        *reinterpret_cast<uint4*>(at + tc_offset(row, 8 * c)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t mb = smem_addr(mbar);
+    const uint32_t aBase = smem_addr(at), bBase = smem_addr(bt);
+    uint32_t phase = 0;
+    bool failed = false;
+    // one 16-byte group (8 samples) of one row, samples >= n zeroed
+    auto group = [&](const __nv_bfloat16* row, uint32_t s0) -> uint4 {
+        if (s0 + 8 <= n) return *reinterpret_cast<const uint4*>(row + s0);
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = s0 + k < n ? row[s0 + k] : __float2bfloat16_rn(0.0f);
+        return *reinterpret_cast<const uint4*>(v);
+    };
+    for (uint32_t ch = c0; ch < c1 && !failed; ++ch) {
+        const uint32_t sbase = ch * kDwTcChunk;
+        for (int i = tid; i < rows * (kDwTcChunk / 8); i += kTcRows) {
+            const uint32_t row = (uint32_t)(i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
+            *reinterpret_cast<uint4*>(at + tc_offset(row, 8 * c)) = group(A + (uint64_t)row * kTrainSlice, sbase + 8 * c);
+        }
+        for (int i = tid; i < kHidden * (kDwTcChunk / 8); i += kTcRows) {
+            const uint32_t row = (uint32_t)(i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
+            *reinterpret_cast<uint4*>(bt + tc_offset(row, 8 * c)) = group(B + (uint64_t)row * kTrainSlice, sbase + 8 * c);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tiles visible to the tensor cores
+        tc_sync();
+        if (tid == 0) {
+            const uint32_t idesc = tc_idesc(kTcRows, kHidden);
+#pragma unroll
+            for (int ks = 0; ks < kDwTcChunk / 16; ++ks)
+                tc_mma(tmem, tc_desc(aBase + ks * 2 * kTcLbo), tc_desc(bBase + ks * 2 * kTcLbo), idesc,
+                       (ch > c0 || ks > 0) ? 1u : 0u);
+            tc_commit(mb);
+        }
+        uint32_t tries = 0;
+        bool late = false;
+        while (!mbar_try_wait(mb, phase))
+            if (++tries >= kTcWaitLimit) {
+                late = true;
+                break;
+            }
+        phase ^= 1u;
+        failed = __syncthreads_or(late) != 0;  // the tiles are rewritten only after the MMAs read them
+    }
+    if (!failed) {
+        tc_fence_after();
+        const int inDim = layer_in(l);
+        float* out = partial + (uint64_t)split * kWeightCount + layer_offset(l);
+        if (warp < 2) {  // rows 0..63 live in lanes 0..63 (warps 0 and 1)
+            const uint32_t lane = tmem + ((warp * 32u) << 16);
+            const int row = (int)(warp * 32 + (tid & 31));
+#pragma unroll
+            for (int c16 = 0; c16 < kHidden / 16; ++c16) {
+                float v[16];
+                tc_ld16(lane + 16u * c16, v);
+                if (row < rows)
+#pragma unroll
+                    for (int k = 0; k < 16; k += 4)
+                        *reinterpret_cast<float4*>(out + row * inDim + 16 * c16 + k) =
+                            c1 > c0 ? make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    } else if (status) {
+        atomicOr(status, kErrTensorWait);
+    }
+    tc_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+}
+
 // dW[i] += sum over blocks of the blocks' partial dW (fixed order).
 __global__ void k_reduce_dw(const float* __restrict__ partial, uint32_t blocks, float* __restrict__ dW)
 {
@@ -910,7 +1031,7 @@ void Guide::infer_queue(const Query* q, const uint32_t* count, uint32_t maxN, fl
 }
 
 void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset,
-                                 uint32_t stride)
+                                 uint32_t stride, uint32_t* status)
 {
     cudaFuncSetAttribute(k_train_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_rows_smem());
     for (uint32_t start = 0; start < n; start += kTrainSlice) {
@@ -918,9 +1039,16 @@ void Guide::accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cu
         const uint32_t chunks = (m + 31) / 32;
         k_train_rows<<<(chunks + kTrainRowWarps - 1) / kTrainRowWarps, 32 * kTrainRowWarps, train_rows_smem(), st>>>(
             params(), s, m, offset + start * stride, stride, invBatch, xt_, dt_, gridG_, loss_);
-        const uint32_t splits = std::min(kDwSplits, (m + 15) / 16);
-        k_dw<<<dim3(splits, kDwTasks), 32, 0, st>>>(xt_, dt_, m, partial_);
-        k_reduce_dw<<<(kWeightCount + 255) / 256, 256, 0, st>>>(partial_, splits, wG_);
+        if (gradKernel_ == kKernelTensorMemory) {
+            cudaFuncSetAttribute(k_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDwTcSmem);
+            const uint32_t splits = std::min(kDwSplits, (m + kDwTcChunk - 1) / kDwTcChunk);
+            k_dw_tc<<<dim3(splits, kLayers), kTcRows, kDwTcSmem, st>>>(xt_, dt_, m, partial_, status);
+            k_reduce_dw<<<(kWeightCount + 255) / 256, 256, 0, st>>>(partial_, splits, wG_);
+        } else {
+            const uint32_t splits = std::min(kDwSplits, (m + 15) / 16);
+            k_dw<<<dim3(splits, kDwTasks), 32, 0, st>>>(xt_, dt_, m, partial_);
+            k_reduce_dw<<<(kWeightCount + 255) / 256, 256, 0, st>>>(partial_, splits, wG_);
+        }
     }
 }
 

@@ -108,6 +108,15 @@ int alpine_gpu_guide_infer(alpine_gpu_ctx* c, const float* queries, uint32_t n, 
     return c->check_device_status();
 }
 
+int alpine_gpu_guide_set_gradient_kernel(alpine_gpu_ctx* c, int kernel)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (kernel == ALPINE_GPU_GUIDE_KERNEL_WARP_MMA) c->guide.set_gradient_kernel(G::Guide::kKernelWarpMma);
+    else if (kernel == ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY) c->guide.set_gradient_kernel(G::Guide::kKernelTensorMemory);
+    else return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "guide_set_gradient_kernel: unknown kernel");
+    return ALPINE_GPU_OK;
+}
+
 int alpine_gpu_guide_set_kernel(alpine_gpu_ctx* c, int kernel)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
@@ -133,7 +142,7 @@ int alpine_gpu_guide_gradients(alpine_gpu_ctx* c, const float* samples, uint32_t
     if (e == cudaSuccess) e = cudaMemsetAsync(c->guide.weight_grad(), 0, G::kWeightCount * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->guide.grid_grad(), 0, G::kGridParams * 4, st);
     if (e == cudaSuccess) {
-        c->guide.accumulate_gradients(ds.as<G::Sample>(), n, n ? 1.0f / (float)n : 0.0f, st);
+        c->guide.accumulate_gradients(ds.as<G::Sample>(), n, n ? 1.0f / (float)n : 0.0f, st, 0, 1, c->dStatus);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && dW) e = cudaMemcpyAsync(dW, c->guide.weight_grad(), G::kWeightCount * 4, cudaMemcpyDeviceToHost, st);

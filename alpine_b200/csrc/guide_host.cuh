@@ -35,7 +35,11 @@ public:
     // Adds the gradient of the batch s[offset + i * stride], i < n (mean
     // loss, scaled by invBatch) to the gradient buffers, without an update.
     void accumulate_gradients(const Sample* s, uint32_t n, float invBatch, cudaStream_t st, uint32_t offset = 0,
-                              uint32_t stride = 1);
+                              uint32_t stride = 1, uint32_t* status = nullptr);
+    // Weight-gradient kernel (dW = dY^T X per layer): warp-level mma.sync
+    // tiles, or tcgen05 MMAs with tensor-memory accumulators.
+    void set_gradient_kernel(int k) { gradKernel_ = k; }
+    int gradient_kernel() const { return gradKernel_; }
     void apply_adam(float lr, cudaStream_t st);
     // gradients + Adam; returns the batch loss (synchronises).
     float train_step(const Sample* s, uint32_t n, float lr, cudaStream_t st);
@@ -61,6 +65,7 @@ private:
     void* mem_ = nullptr;
     bool ready_ = false;
     int kernel_ = kKernelWarpMma;
+    int gradKernel_ = kKernelTensorMemory;
     uint32_t step_ = 0;
     float* gridP_ = nullptr;
     float* gridM_ = nullptr;

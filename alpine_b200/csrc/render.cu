@@ -453,7 +453,7 @@ int train_guide(alpine_gpu_ctx* c, const ag::IntegratorKernels& K, const ag::Wav
     const uint32_t stride = surplus ? kept / batch : steps;
     for (uint32_t i = 0; i < steps; ++i) {
         const uint32_t n = surplus ? batch : (kept - i + steps - 1) / steps;
-        c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, stride);
+        c->guide.accumulate_gradients(gw.out, n, 1.0f / (float)n, st, i, stride, c->dStatus);
         c->guide.apply_adam(lr, st);
     }
     c->guideLastLossSteps = steps;

@@ -161,6 +161,7 @@ def lib():
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
         L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p, C.POINTER(C.c_float)]
         L.alpine_gpu_guide_set_kernel.argtypes = [vp, C.c_int]
+        L.alpine_gpu_guide_set_gradient_kernel.argtypes = [vp, C.c_int]
         L.alpine_gpu_guide_gradients.argtypes = [vp, vp, C.c_uint32, vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_guide_train.argtypes = [vp, vp, C.c_uint32, C.c_float, f3]
         L.alpine_gpu_guide_get_weights.argtypes = [vp, vp]
@@ -528,6 +529,11 @@ class Context:
     def guide_set_kernel(self, kernel):
         """GUIDE_KERNEL_WARP_MMA (mma.sync) or GUIDE_KERNEL_TENSOR_MEMORY (tcgen05)."""
         self._check(self.L.alpine_gpu_guide_set_kernel(self.h, kernel))
+
+    def guide_set_gradient_kernel(self, kernel):
+        """Training's weight-gradient kernel: GUIDE_KERNEL_TENSOR_MEMORY
+        (tcgen05, default) or GUIDE_KERNEL_WARP_MMA (mma.sync)."""
+        self._check(self.L.alpine_gpu_guide_set_gradient_kernel(self.h, kernel))
 
     def guide_infer(self, queries):
         q = np.ascontiguousarray(queries, np.float32).reshape(-1, 12)

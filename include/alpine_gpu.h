@@ -522,6 +522,14 @@ ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* quer
 #define ALPINE_GPU_GUIDE_KERNEL_WARP_MMA 0
 #define ALPINE_GPU_GUIDE_KERNEL_TENSOR_MEMORY 1
 ALPINE_GPU_API int alpine_gpu_guide_set_kernel(alpine_gpu_ctx* ctx, int kernel);
+/* Weight-gradient kernel of the guide's training, dW_l = dY_l^T X_l over a
+ * slice of samples per layer: TENSOR_MEMORY (default) runs it as tcgen05
+ * MMAs (M 128 with the layer's output rows zero-padded, N 64, K 16 per
+ * instruction over 64-sample stages) accumulating in tensor memory, one CTA
+ * per (split of the samples, layer); WARP_MMA runs mma.sync tiles, one warp
+ * per (layer, 16 rows, split). Both sum BF16 x BF16 products in FP32; the
+ * sums differ in the last bits (order). */
+ALPINE_GPU_API int alpine_gpu_guide_set_gradient_kernel(alpine_gpu_ctx* ctx, int kernel);
 /* Adam steps taken since the last reset, waves rendered with guiding, and the
  * mean training loss (KL divergence up to a constant) of the last trained
  * wave's steps (0 before any). Any pointer may be NULL. */

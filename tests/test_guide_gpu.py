@@ -127,6 +127,30 @@ def test_gradients_match_oracle(ctx):
     assert gerr < 5e-2
 
 
+@pytest.mark.parametrize("n", [1, 37, 64, 1000, 16384, 20000])
+def test_gradient_kernels_agree(ctx, n):
+    """The tcgen05 weight-gradient kernel (tensor-memory accumulators) and
+    the mma.sync kernel compute the same dW = dY^T X (FP32 sums of BF16
+    products, in different orders), for batches that fill, straddle and
+    span more than one 16,384-sample slice."""
+    q = _queries(n, 20 + n % 7)
+    _randomise(ctx, q, 8)
+    rng = np.random.default_rng(n)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    samples = np.concatenate([q, d, rng.uniform(0.2, 3.0, (n, 1))], axis=1).astype(np.float32)
+    out = {}
+    for k in (gpu.GUIDE_KERNEL_WARP_MMA, gpu.GUIDE_KERNEL_TENSOR_MEMORY):
+        ctx.guide_set_gradient_kernel(k)
+        out[k] = ctx.guide_gradients(samples)[0].astype(np.float64)
+    ctx.guide_set_gradient_kernel(gpu.GUIDE_KERNEL_TENSOR_MEMORY)
+    a, b = out[gpu.GUIDE_KERNEL_TENSOR_MEMORY], out[gpu.GUIDE_KERNEL_WARP_MMA]
+    err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+    print(f"n={n}: tcgen05 vs mma.sync dW relative L2 difference {err:.2e}")
+    assert np.isfinite(a).all() and np.linalg.norm(b) > 0
+    assert err < 1e-5
+
+
 def test_mixture_sampling(ctx):
     rng = np.random.default_rng(6)
     raw = rng.normal(size=40).astype(np.float32)
