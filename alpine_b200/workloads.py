@@ -9,6 +9,7 @@ its NVTX range "measure").
     python -m alpine_b200.workloads guided   # glossy interior 320x180, depth 12, guided:
                                              # 16 Adam steps, then 2 x 32 spp
     python -m alpine_b200.workloads guided_tc  # the same with the tcgen05 inference kernel
+    python -m alpine_b200.workloads guided_dwmma  # the same with the mma.sync weight-gradient kernel
     python -m alpine_b200.workloads city     # many-light city 960x540, 1 + 2 spp, depth 8, light BVH
     python -m alpine_b200.workloads interior        # glossy interior 320x180, depth 12, plain MIS, 2 x 64 spp
     python -m alpine_b200.workloads interior_guided # the same guided with the time-to-relMSE schedule
@@ -33,7 +34,7 @@ def run(mode: str, device: int = 0) -> float:
         opts, sampler, spp = dict(russian_roulette_depth=3), gpu.SAMPLER_POWER, (16, 16)
         if mode == "room_queue":  # shading in traversal-queue order
             opts["shade_order"] = gpu.SHADE_ORDER_QUEUE
-    elif mode in ("guided", "guided_tc"):
+    elif mode in ("guided", "guided_tc", "guided_dwmma"):
         sc, (W, H), depth = scenes.glossy_interior_scene(), (320, 180), 12
         opts = dict(accumulate_fp64=True, guide=True, guide_spp_per_wave=2, guide_batch=65536, guide_steps_per_wave=4,
                     guide_min_roughness=0.2, guide_train_steps=16)
@@ -58,6 +59,8 @@ def run(mode: str, device: int = 0) -> float:
     c = gpu.Context(device, W, H, depth)
     if mode == "guided_tc":
         c.guide_set_kernel(gpu.GUIDE_KERNEL_TENSOR_MEMORY)
+    if mode == "guided_dwmma":  # training's weight gradients on mma.sync instead of tcgen05
+        c.guide_set_gradient_kernel(gpu.GUIDE_KERNEL_WARP_MMA)
     scenes.load_scene(c, sc, W, H)
     if sampler is not None:
         c.build_light_sampler(sampler)
