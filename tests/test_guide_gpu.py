@@ -62,7 +62,9 @@ def test_inference_matches_oracle(ctx):
     ref, _ = G.forward(X, G.unpack(w), emulate_bf16=True)
     err = np.linalg.norm(raw - ref[:, :40]) / np.linalg.norm(ref[:, :40])
     print(f"inference relative L2 error vs BF16-emulated FP64 oracle: {err:.2e}")
-    assert err < 2e-2
+    # measured about 4e-8: the oracle emulates every BF16 rounding, so only the
+    # FP32 accumulation order differs
+    assert err < 1e-5
 
 
 @pytest.mark.parametrize("n", [1000, 128, 1, 70000])
@@ -87,8 +89,8 @@ def test_tensor_memory_inference_matches(ctx, n):
     err = np.linalg.norm(tc[:m] - ref[:, :40]) / np.linalg.norm(ref[:, :40])
     diff = np.linalg.norm(tc - warp) / np.linalg.norm(warp)
     print(f"n={n}: tcgen05 vs oracle {err:.2e}, vs warp MMA {diff:.2e}")
-    assert err < 2e-2
-    assert diff < 1e-2
+    assert err < 1e-5
+    assert diff < 1e-5
 
 
 def test_gradients_match_oracle(ctx):
