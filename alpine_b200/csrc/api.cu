@@ -313,6 +313,7 @@ int alpine_gpu_build(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats)
     c->stats.wide_depth = bs.wideDepth;
     c->stats.sah_cost = bs.sahCost;
     c->stats.build_ms = bs.buildMs;
+    c->stats.child_slots = bs.childSlots;
     if (stats) *stats = c->stats;
     return check_status(c);
 }
@@ -372,6 +373,20 @@ int alpine_gpu_set_traversal_options(alpine_gpu_ctx* c, const alpine_gpu_travers
         return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT,
                        "set_traversal_options: stack_limit above " + std::to_string(ag::kTraversalStack));
     c->traversal = *o;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_set_build_options(alpine_gpu_ctx* c, const alpine_gpu_build_options* o)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (!o) return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_build_options: null options");
+    if (o->collapse != ALPINE_GPU_COLLAPSE_SAH && o->collapse != ALPINE_GPU_COLLAPSE_GREEDY)
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_build_options: unknown collapse");
+    if (!(o->triangle_cost >= 0.0f) || !(o->triangle_cost <= 1e6f))
+        return c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "set_build_options: triangle_cost outside [0, 1e6]");
+    c->builder.set_collapse(o->collapse == ALPINE_GPU_COLLAPSE_SAH ? ag::kCollapseSah : ag::kCollapseGreedy,
+                            o->triangle_cost > 0.0f ? o->triangle_cost : ag::kCollapseTriCost);
+    c->bvhDirty = true;
     return ALPINE_GPU_OK;
 }
 

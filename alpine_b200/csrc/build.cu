@@ -11,10 +11,18 @@
 // is a pure function of its input (the float min/max merges and integer counts
 // are order independent).
 //
-// Wide phase: breadth-first greedy collapse to 8 slots (open the internal
-// child of largest surface area, as src/accelerators/wide_bvh.cpp:200-243
-// does), quantised child boxes, octant-ordered slots, triangle records in leaf
-// order (src/accelerators/wide_bvh.cpp:430-472 packs TriangleN likewise).
+// Wide phase: breadth-first collapse to 8 slots, quantised child boxes,
+// octant-ordered slots, triangle records in leaf order
+// (src/accelerators/wide_bvh.cpp:430-472 packs TriangleN likewise). Which
+// binary nodes fill a wide node's slots is chosen either
+//   * SAH-optimally (the default): a bottom-up dynamic program over the
+//     binary tree gives every node its least SAH cost when it may occupy
+//     1..8 slots of its parent (the method of Ylitie, Karras and Laine,
+//     "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide
+//     BVHs", HPG 2017, restated for leaves of at most 3 triangles), and the
+//     collapse follows its choices; or
+//   * greedily, as the reference does (src/accelerators/wide_bvh.cpp:200-243):
+//     open the internal child of largest surface area until 8 slots are used.
 #include "build.cuh"
 #include "scan.cuh"
 
@@ -62,7 +70,7 @@ struct BigSplit {
     uint32_t nL;
 };
 
-enum Counter { kCntTasks = 0, kCntBig, kCntChunks, kCntInt, kCntTri, kCntBounds = 8, kCntWords = 32 };
+enum Counter { kCntTasks = 0, kCntBig, kCntChunks, kCntInt, kCntTri, kCntSlots, kCntBounds = 8, kCntWords = 32 };
 
 // --------------------------------------------------------------------------
 // Binning arithmetic. Every kernel must compute identical bin indices, so all
@@ -736,9 +744,81 @@ __global__ void k_compact(const Task* __restrict__ tasks, const Cand* __restrict
 // Collapse to the wide layout.
 AG_D float bn_area(const BinNode& b) { return area_of(b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z); }
 
+// SAH cost program of the collapse, one binary level per launch from the
+// deepest up. For binary node x of area A, count n and children l, r:
+//   leaf(x)    = A * triCost * n                       (n <= kMaxLeafTris)
+//   D(x, j)    = min over k in 1..j-1 of C(l, k) + C(r, j - k)
+//   C(x, 1)    = leaf(x) if n <= kMaxLeafTris, else A + D(x, 8)  (x in one slot:
+//                a leaf, or an internal child whose own wide node tests 8 slots)
+//   C(x, j)    = min(C(x, j - 1), D(x, j))             (x spread over at most j slots)
+// with a wide-node visit costing 1 per unit area. cost[8x + j - 1] holds
+// C(x, j) for j = 1..7 and cost[8x + 7] = A + D(x, 8); nibble j - 1 of
+// choice[x] holds the k of D(x, j) when it was taken (0: x keeps j - 1
+// slots; nibble 7: the split of x's own wide node). A binary leaf costs
+// leaf(x) for every j.
+__global__ void k_collapse_cost(const BinNode* __restrict__ bnodes, uint32_t first, uint32_t count, float triCost,
+                                float* __restrict__ cost, uint32_t* __restrict__ choice)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t x = first + t;
+    const BinNode b = bnodes[x];
+    const float A = bn_area(b);
+    float* C = cost + 8ull * x;
+    if (b.left < 0) {
+        const float leaf = b.count <= (uint32_t)kMaxLeafTris ? A * triCost * float(b.count) : INFINITY;
+        for (int j = 0; j < 8; ++j) C[j] = leaf;
+        choice[x] = 0;
+        return;
+    }
+    float L[7], R[7];
+    const float* cl = cost + 8ull * (uint32_t)b.left;
+    const float* cr = cost + 8ull * (uint32_t)b.right;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        L[j] = cl[j];
+        R[j] = cr[j];
+    }
+    float D[9];
+    uint32_t K[9];
+#pragma unroll
+    for (int j = 2; j <= 8; ++j) {
+        float best = INFINITY;
+        uint32_t bk = 1;
+#pragma unroll
+        for (int k = 1; k < j; ++k) {
+            const float v = L[k - 1] + R[j - k - 1];
+            if (v < best) {
+                best = v;
+                bk = (uint32_t)k;
+            }
+        }
+        D[j] = best;
+        K[j] = bk;
+    }
+    const float node = A + D[8];
+    float prev = b.count <= (uint32_t)kMaxLeafTris ? A * triCost * float(b.count) : node;
+    C[0] = prev;
+    uint32_t ch = K[8] << 28;
+#pragma unroll
+    for (int j = 2; j <= 7; ++j) {
+        if (D[j] < prev) {
+            prev = D[j];
+            ch |= K[j] << (4 * (j - 1));
+        }
+        C[j - 1] = prev;
+    }
+    C[7] = node;
+    choice[x] = ch;
+}
+
+// The slots of one wide node per thread. choice (the cost program's
+// decisions) selects the SAH-optimal distribution; null selects the greedy
+// rule. Slots are then assigned to octants.
 __global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
-                                  int32_t* __restrict__ slots, uint32_t* __restrict__ intCount,
-                                  uint32_t* __restrict__ triCount)
+                                  const uint32_t* __restrict__ choice, int32_t* __restrict__ slots,
+                                  uint32_t* __restrict__ intCount, uint32_t* __restrict__ triCount,
+                                  uint32_t* __restrict__ slotTotal)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= numItems) return;
@@ -748,31 +828,58 @@ __global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numI
     const BinNode root = bnodes[b];
     if (root.count <= (uint32_t)kMaxLeafTris || root.left < 0) {
         ent[n++] = (int32_t)b;
+    } else if (choice) {
+        // follow the cost program: (node, slots it may use), root split first
+        int32_t stN[kWidth];
+        uint32_t stJ[kWidth];
+        int sp = 0;
+        const uint32_t k8 = choice[b] >> 28;
+        stN[sp] = root.right;
+        stJ[sp++] = 8u - k8;
+        stN[sp] = root.left;
+        stJ[sp++] = k8;
+        while (sp > 0) {
+            const int32_t x = stN[--sp];
+            uint32_t j = stJ[sp];
+            const BinNode c = bnodes[x];
+            uint32_t k = 0;
+            if (c.left >= 0)
+                while (j > 1 && (k = (choice[x] >> (4 * (j - 1))) & 0xfu) == 0u) --j;
+            if (j <= 1 || c.left < 0 || k == 0u || k >= j || sp + 2 > kWidth || n + sp + 2 > kWidth) {
+                ent[n++] = x;  // one slot (the last tests only guard malformed input)
+                continue;
+            }
+            stN[sp] = c.right;
+            stJ[sp++] = j - k;
+            stN[sp] = c.left;
+            stJ[sp++] = k;
+        }
     } else {
         ent[n++] = root.left;
         ent[n++] = root.right;
-    }
-    // Open children until all 8 slots are used: first those too large for a
-    // leaf slot, then small internal ones (tighter leaf boxes are free since
-    // every slot box is tested anyway).
-    for (int phase = 0; phase < 2; ++phase) {
-        while (n < kWidth) {
-            int pick = -1;
-            float pa = -1.0f;
-            for (int k = 0; k < n; ++k) {
-                const BinNode& c = bnodes[ent[k]];
-                if (c.left < 0) continue;
-                bool large = c.count > (uint32_t)kMaxLeafTris;
-                if (phase == 0 ? !large : large) continue;
-                float a = bn_area(c);
-                if (a > pa) { pa = a; pick = k; }
+        // Open children until all 8 slots are used: first those too large for
+        // a leaf slot, then small internal ones (tighter leaf boxes are free
+        // since every slot box is tested anyway).
+        for (int phase = 0; phase < 2; ++phase) {
+            while (n < kWidth) {
+                int pick = -1;
+                float pa = -1.0f;
+                for (int k = 0; k < n; ++k) {
+                    const BinNode& c = bnodes[ent[k]];
+                    if (c.left < 0) continue;
+                    bool large = c.count > (uint32_t)kMaxLeafTris;
+                    if (phase == 0 ? !large : large) continue;
+                    float a = bn_area(c);
+                    if (a > pa) { pa = a; pick = k; }
+                }
+                if (pick < 0) break;
+                const BinNode& c = bnodes[ent[pick]];
+                ent[pick] = c.left;
+                ent[n++] = c.right;
             }
-            if (pick < 0) break;
-            const BinNode& c = bnodes[ent[pick]];
-            ent[pick] = c.left;
-            ent[n++] = c.right;
         }
     }
+    atomicAdd(slotTotal, (uint32_t)n);
     // Octant slot assignment: slot s prefers the child whose centre lies
     // toward corner s of the parent box (bit k of s set = + side of axis k).
     float3 pc = 0.5f * (root.lo + root.hi);
@@ -982,6 +1089,8 @@ int Builder::reserve(uint32_t n, char* err, size_t errLen)
     bytes += carve_bytes<BigSplit>(maxBig);
     bytes += 2 * carve_bytes<uint2>(N + 1);        // items x2
     bytes += carve_bytes<int32_t>((N + 1) * kWidth);
+    bytes += carve_bytes<float>(2 * N * 8);        // collapse costs
+    bytes += carve_bytes<uint32_t>(2 * N);         // collapse choices
     bytes += 4 * carve_bytes<uint32_t>(N + 1);     // intCount, intOff, triCount, triOff
     bytes += carve_bytes<uint32_t>(kCntWords);
     bytes += carve_bytes<uint32_t>(scan_scratch_words(2 * N + 2));
@@ -1019,6 +1128,8 @@ int Builder::reserve(uint32_t n, char* err, size_t errLen)
     items_[0] = reinterpret_cast<uint32_t*>(carve<uint2>(p, N + 1));
     items_[1] = reinterpret_cast<uint32_t*>(carve<uint2>(p, N + 1));
     slots_ = reinterpret_cast<uint32_t*>(carve<int32_t>(p, (N + 1) * kWidth));
+    collapseCost_ = carve<float>(p, 2 * N * 8);
+    collapseChoice_ = carve<uint32_t>(p, 2 * N);
     intCount_ = carve<uint32_t>(p, N + 1);
     intOff_ = carve<uint32_t>(p, N + 1);
     triCount_ = carve<uint32_t>(p, N + 1);
@@ -1067,6 +1178,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     uint32_t nodeCount = 1;
     int cur = 0;
     uint32_t level = 0;
+    levelStart_.assign(1, 0u);  // binary node ids of level L: [levelStart_[L], levelStart_[L + 1])
     while (numTasks > 0) {
         if (++level > kMaxLevels) {
             snprintf(err, errLen, "BVH build: more than %u levels", kMaxLevels);
@@ -1104,11 +1216,22 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         numTasks = hostCounters_[kCntTasks];
         numBig = hostCounters_[kCntBig];
         totalChunks = hostCounters_[kCntChunks];
+        levelStart_.push_back(nodeCount);
         nodeCount += numTasks;
         cur ^= 1;
     }
+    levelStart_.push_back(nodeCount);
     local.binaryNodes = nodeCount;
     local.binaryLevels = level;
+
+    // SAH cost program of the collapse, deepest level first
+    const bool sahCollapse = collapse_ == kCollapseSah;
+    if (sahCollapse)
+        for (size_t L = levelStart_.size() - 1; L-- > 0;) {
+            const uint32_t first = levelStart_[L], cnt = levelStart_[L + 1] - first;
+            if (cnt) k_collapse_cost<<<blocks_for(cnt, 128), 128, 0, st>>>(bnodes_, first, cnt, triCost_,
+                                                                          collapseCost_, collapseChoice_);
+        }
 
     // Wide collapse.
     BinNode rb;
@@ -1116,6 +1239,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     uint2 rootItem = make_uint2(0, 0);
     cudaMemcpyAsync(items_[0], &rootItem, sizeof(uint2), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(sahAccum_, 0, sizeof(float), st);
+    cudaMemsetAsync(counters_ + kCntSlots, 0, sizeof(uint32_t), st);
     cudaStreamSynchronize(st);
     float rootArea = (rb.hi.x - rb.lo.x) * (rb.hi.y - rb.lo.y) + (rb.hi.y - rb.lo.y) * (rb.hi.z - rb.lo.z) +
                      (rb.hi.z - rb.lo.z) * (rb.hi.x - rb.lo.x);
@@ -1130,8 +1254,9 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         const uint2* items = reinterpret_cast<const uint2*>(items_[ci]);
         uint2* itemsNext = reinterpret_cast<uint2*>(items_[ci ^ 1]);
         int32_t* slots = reinterpret_cast<int32_t*>(slots_);
-        k_collapse_decide<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intCount_,
-                                                                      triCount_);
+        k_collapse_decide<<<blocks_for(numItems, 128), 128, 0, st>>>(
+            items, numItems, bnodes_, sahCollapse ? collapseChoice_ : nullptr, slots, intCount_, triCount_,
+            counters_ + kCntSlots);
         exclusive_scan(intCount_, intOff_, numItems, counters_ + kCntInt, scanScratch_, st);
         exclusive_scan(triCount_, triOff_, numItems, counters_ + kCntTri, scanScratch_, st);
         k_collapse_emit<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intOff_, triOff_,
@@ -1153,6 +1278,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     cudaEventRecord(ev1_, st);
     float sah = 0.0f;
     cudaMemcpyAsync(&sah, sahAccum_, sizeof(float), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hostCounters_ + kCntSlots, counters_ + kCntSlots, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         snprintf(err, errLen, "BVH build: %s", cudaGetErrorString(cudaGetLastError()));
         return -2;
@@ -1164,6 +1290,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     local.triCount = triCount;
     local.sahCost = sah;
     local.buildMs = ms;
+    local.childSlots = hostCounters_[kCntSlots];
     if (triCount != n) {
         snprintf(err, errLen, "BVH build: %u triangles placed, expected %u", triCount, n);
         return -3;

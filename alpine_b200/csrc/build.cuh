@@ -1,10 +1,13 @@
-// GPU BVH builder: binned SAH (32 bins) binary build, then a greedy collapse to
-// the 8-wide quantised layout of bvh.cuh. Replaces the reference's CPU build
+// GPU BVH builder: binned SAH (32 bins) binary build, then a collapse
+// (SAH-optimal by default, or the reference's greedy rule) to the 8-wide
+// quantised layout of bvh.cuh. Replaces the reference's CPU build
 // (src/accelerators/bvh_common.cpp:185-391 binned SAH with 9 bins and
 // src/accelerators/wide_bvh.cpp:200-243 collapse + 290-356 flatten).
 #pragma once
 
 #include "bvh.cuh"
+
+#include <vector>
 
 namespace ag {
 
@@ -16,7 +19,13 @@ struct BuildStats {
     uint32_t triCount = 0;
     float sahCost = 0.0f;  // SAH cost of the wide tree (node + triangle tests per unit root area)
     float buildMs = 0.0f;  // device time of the whole build
+    uint32_t childSlots = 0;  // filled slots over all wide nodes
 };
+
+// Which binary nodes fill the slots of a wide node.
+constexpr uint32_t kCollapseSah = 0;     // SAH-optimal (dynamic program over the binary tree)
+constexpr uint32_t kCollapseGreedy = 1;  // largest-area child first (src/accelerators/wide_bvh.cpp:200-243)
+constexpr float kCollapseTriCost = 1.0f;  // default SAH cost of a triangle test per wide-node visit
 
 // Device buffers owned by a builder; grown on demand and reused across builds.
 class Builder {
@@ -35,11 +44,23 @@ public:
               WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t stream, BuildStats* stats,
               char* err, size_t errLen);
 
+    // Collapse rule and the SAH cost of a triangle test relative to a
+    // wide-node visit (used by kCollapseSah); applied at the next build.
+    void set_collapse(uint32_t rule, float triCost)
+    {
+        collapse_ = rule;
+        triCost_ = triCost;
+    }
+    uint32_t collapse() const { return collapse_; }
+    float triangle_cost() const { return triCost_; }
+
 private:
     int reserve(uint32_t ntris, char* err, size_t errLen);
     void release();
 
     uint32_t cap_ = 0;
+    uint32_t collapse_ = kCollapseSah;
+    float triCost_ = kCollapseTriCost;
     void* mem_ = nullptr;  // one allocation carved into the arrays below
     size_t memBytes_ = 0;
     float4* primLo_ = nullptr;
@@ -64,6 +85,9 @@ private:
     void* bigSplit_ = nullptr;
     uint32_t* items_[2] = {nullptr, nullptr};
     uint32_t* slots_ = nullptr;
+    std::vector<uint32_t> levelStart_;   // first binary node id of each level (host)
+    float* collapseCost_ = nullptr;      // 8 per binary node (k_collapse_cost)
+    uint32_t* collapseChoice_ = nullptr; // 1 per binary node
     uint32_t* intCount_ = nullptr;
     uint32_t* intOff_ = nullptr;
     uint32_t* triCount_ = nullptr;

@@ -677,47 +677,63 @@ __global__ void __launch_bounds__(32) k_dw(const __nv_bfloat16* __restrict__ XT,
 
 // k_dw_tc: the same product on the 5th-generation tensor cores. One CTA of
 // 128 threads per (split of the samples, layer) accumulates
-// dW_l = dY_l^T X_l in tensor memory: per chunk of 64 samples it stages
-// A = dY_l^T (the layer's output rows, zero-padded to M = 128 so that the
-// accumulator has the lane-per-row layout of k_infer_tc) and B = X_l^T
-// (N = 64 input rows), both K-major over the samples, in the no-swizzle
-// core-matrix layout, and one elected thread issues four tcgen05.mma
-// (K = 16 each) and commits them to an mbarrier. Samples beyond n are staged
-// as zeros. Warps 0 and 1 then read rows 0..63 back (tcgen05.ld) into the
+// dW_l = dY_l^T X_l in tensor memory over chunks of 64 samples: A = dY_l^T
+// (the layer's output rows, zero-padded to M = 128 so that the accumulator
+// has the lane-per-row layout of k_infer_tc) and B = X_l^T (N = 64 input
+// rows), both K-major over the samples in the no-swizzle core-matrix
+// layout. The chunks stream through kDwTcStages shared-memory stages:
+// cp.async copies (16 bytes, zero-filled past n) run kDwTcStages - 1 chunks
+// ahead of the MMAs, one elected thread issues each chunk's four
+// tcgen05.mma (K = 16) and commits them to the stage's mbarrier, and a
+// stage is refilled only after that mbarrier says the MMAs that read it are
+// done. Warps 0 and 1 then read rows 0..63 back (tcgen05.ld) into the
 // split's partial dW, summed by k_reduce_dw like k_dw's. Every wait is
-// bounded: a CTA that runs out records kErrTensorWait, writes nothing, and
-// still frees its tensor memory.
+// bounded: a CTA that runs out records kErrTensorWait, writes nothing,
+// waits for its own copies and still frees its tensor memory.
 constexpr int kDwTcChunk = 64;                                   // samples per stage (K)
+constexpr int kDwTcStages = 4;
 constexpr int kDwTcATile = kTcRows * kDwTcChunk * 2;             // 16 KiB
 constexpr int kDwTcBTile = kHidden * kDwTcChunk * 2;             // 8 KiB
-constexpr int kDwTcSmem = kDwTcATile + kDwTcBTile + 16;
+constexpr int kDwTcStage = kDwTcATile + kDwTcBTile;
+constexpr int kDwTcSmem = kDwTcStages * kDwTcStage + kDwTcStages * 8 + 8;  // + mbarriers + tensor-memory address
 static_assert(kTrainSlice % kDwTcChunk == 0, "whole chunks per slice");
+static_assert(kDwTcStage % 1024 == 0, "stages keep the operand tiles' alignment");
+
+// 16 bytes from global to shared memory, asynchronously; bytes past `bytes`
+// (0..16) are written as zeros and not read.
+AG_D void cp_async16(uint32_t dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+AG_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> AG_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __global__ void __launch_bounds__(kTcRows) k_dw_tc(const __nv_bfloat16* __restrict__ XT,
                                                    const __nv_bfloat16* __restrict__ DT, uint32_t n,
                                                    float* __restrict__ partial, uint32_t* __restrict__ status)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* at = smem;
-    unsigned char* bt = smem + kDwTcATile;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(bt + kDwTcBTile);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bt + kDwTcBTile + 8);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kDwTcStages * kDwTcStage);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kDwTcStages);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const int l = blockIdx.y;
     const int rows = layer_out(l);
     const uint32_t split = blockIdx.x, splits = gridDim.x;
     const uint32_t chunks = (n + kDwTcChunk - 1) / kDwTcChunk, per = (chunks + splits - 1) / splits;
-    const uint32_t c0 = split * per, c1 = min(chunks, c0 + per);
+    const uint32_t c0 = min(chunks, split * per), cnt = min(chunks, c0 + per) - c0;
     const __nv_bfloat16* A = DT + (uint64_t)l * kHidden * kTrainSlice;  // row m: dY_l[., m] over the samples
     const __nv_bfloat16* B = XT + (uint64_t)l * kHidden * kTrainSlice;  // row k: X_l[., k]
+    const uint32_t sBase = smem_addr(smem);
 
-    // the padding rows of A (rows .. 127) stay zero for the whole kernel
-    for (int i = tid; i < (kTcRows - rows) * (kDwTcChunk / 8); i += kTcRows) {
-        const uint32_t row = (uint32_t)(rows + i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
-        *reinterpret_cast<uint4*>(at + tc_offset(row, 8 * c)) = make_uint4(0u, 0u, 0u, 0u);
+    // the padding rows of every stage's A (rows .. 127) stay zero for the whole kernel
+    for (int i = tid; i < kDwTcStages * (kTcRows - rows) * (kDwTcChunk / 8); i += kTcRows) {
+        const int st = i / ((kTcRows - rows) * (kDwTcChunk / 8)), j = i % ((kTcRows - rows) * (kDwTcChunk / 8));
+        const uint32_t row = (uint32_t)(rows + j / (kDwTcChunk / 8)), c = (uint32_t)(j % (kDwTcChunk / 8));
+        *reinterpret_cast<uint4*>(smem + st * kDwTcStage + tc_offset(row, 8 * c)) = make_uint4(0u, 0u, 0u, 0u);
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
+        for (int st = 0; st < kDwTcStages; ++st)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + st)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -726,52 +742,67 @@ __global__ void __launch_bounds__(kTcRows) k_dw_tc(const __nv_bfloat16* __restri
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // chunk j (of this split) into stage j % kDwTcStages
+    auto load = [&](uint32_t j) {
+        const uint32_t sbase = (c0 + j) * kDwTcChunk;
+        const uint32_t at = sBase + (j % kDwTcStages) * kDwTcStage, bt = at + kDwTcATile;
+        for (int i = tid; i < (rows + kHidden) * (kDwTcChunk / 8); i += kTcRows) {
+            const bool isA = i < rows * (kDwTcChunk / 8);
+            const int k = isA ? i : i - rows * (kDwTcChunk / 8);
+            const uint32_t row = (uint32_t)(k / (kDwTcChunk / 8)), s0 = sbase + 8 * (uint32_t)(k % (kDwTcChunk / 8));
+            const uint32_t bytes = s0 >= n ? 0u : min(16u, (n - s0) * 2u);
+            cp_async16((isA ? at : bt) + tc_offset(row, s0 - sbase), (isA ? A : B) + (uint64_t)row * kTrainSlice + s0,
+                       bytes);
+        }
+    };
+    // bounded wait for the MMAs of chunk j
+    auto wait_mma = [&](uint32_t j) -> bool {
+        const uint32_t mb = smem_addr(mbar + j % kDwTcStages), parity = (j / kDwTcStages) & 1u;
+        for (uint32_t tries = 0; !mbar_try_wait(mb, parity);)
+            if (++tries >= kTcWaitLimit) return false;
+        return true;
+    };
+#pragma unroll
+    for (int j = 0; j < kDwTcStages - 1; ++j) {
+        if ((uint32_t)j < cnt) load(j);
+        cp_async_commit();
+    }
     tc_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t mb = smem_addr(mbar);
-    const uint32_t aBase = smem_addr(at), bBase = smem_addr(bt);
-    uint32_t phase = 0;
-    bool failed = false;
-    // one 16-byte group (8 samples) of one row, samples >= n zeroed
-    auto group = [&](const __nv_bfloat16* row, uint32_t s0) -> uint4 {
-        if (s0 + 8 <= n) return *reinterpret_cast<const uint4*>(row + s0);
-        __align__(16) __nv_bfloat16 v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = s0 + k < n ? row[s0 + k] : __float2bfloat16_rn(0.0f);
-        return *reinterpret_cast<const uint4*>(v);
-    };
-    for (uint32_t ch = c0; ch < c1 && !failed; ++ch) {
-        const uint32_t sbase = ch * kDwTcChunk;
-        for (int i = tid; i < rows * (kDwTcChunk / 8); i += kTcRows) {
-            const uint32_t row = (uint32_t)(i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
-            *reinterpret_cast<uint4*>(at + tc_offset(row, 8 * c)) = group(A + (uint64_t)row * kTrainSlice, sbase + 8 * c);
-        }
-        for (int i = tid; i < kHidden * (kDwTcChunk / 8); i += kTcRows) {
-            const uint32_t row = (uint32_t)(i / (kDwTcChunk / 8)), c = (uint32_t)(i % (kDwTcChunk / 8));
-            *reinterpret_cast<uint4*>(bt + tc_offset(row, 8 * c)) = group(B + (uint64_t)row * kTrainSlice, sbase + 8 * c);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tiles visible to the tensor cores
-        tc_sync();
+    const uint32_t idesc = tc_idesc(kTcRows, kHidden);
+    bool late = false, failed = false;
+    for (uint32_t j = 0; j < cnt; ++j) {
+        cp_async_wait<kDwTcStages - 2>();                             // chunk j has landed (this thread's copies)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+        tc_fence_before();
+        failed = __syncthreads_or(late) != 0;
+        tc_fence_after();
+        if (failed) break;
         if (tid == 0) {
-            const uint32_t idesc = tc_idesc(kTcRows, kHidden);
+            const uint32_t at = sBase + (j % kDwTcStages) * kDwTcStage, bt = at + kDwTcATile;
 #pragma unroll
             for (int ks = 0; ks < kDwTcChunk / 16; ++ks)
-                tc_mma(tmem, tc_desc(aBase + ks * 2 * kTcLbo), tc_desc(bBase + ks * 2 * kTcLbo), idesc,
-                       (ch > c0 || ks > 0) ? 1u : 0u);
-            tc_commit(mb);
+                tc_mma(tmem, tc_desc(at + ks * 2 * kTcLbo), tc_desc(bt + ks * 2 * kTcLbo), idesc,
+                       (j > 0 || ks > 0) ? 1u : 0u);
+            tc_commit(smem_addr(mbar + j % kDwTcStages));
         }
-        uint32_t tries = 0;
-        bool late = false;
-        while (!mbar_try_wait(mb, phase))
-            if (++tries >= kTcWaitLimit) {
-                late = true;
-                break;
-            }
-        phase ^= 1u;
-        failed = __syncthreads_or(late) != 0;  // the tiles are rewritten only after the MMAs read them
+        // refill the stage that chunk j - 1 read with chunk j + kDwTcStages - 1
+        const uint32_t next = j + kDwTcStages - 1;
+        if (next < cnt) {
+            if (j >= 1 && !wait_mma(j - 1)) late = true;
+            if (!late) load(next);
+        }
+        cp_async_commit();
     }
+    // the MMAs of the last chunks (the earlier ones were waited for above)
+    if (!failed)
+        for (uint32_t j = cnt > (uint32_t)kDwTcStages ? cnt - kDwTcStages : 0u; j < cnt; ++j)
+            if (!wait_mma(j)) late = true;
+    cp_async_wait<0>();
+    tc_fence_before();
+    failed = __syncthreads_or(late || failed) != 0;
+    tc_fence_after();
     if (!failed) {
-        tc_fence_after();
         const int inDim = layer_in(l);
         float* out = partial + (uint64_t)split * kWeightCount + layer_offset(l);
         if (warp < 2) {  // rows 0..63 live in lanes 0..63 (warps 0 and 1)
@@ -785,10 +816,10 @@ __global__ void __launch_bounds__(kTcRows) k_dw_tc(const __nv_bfloat16* __restri
 #pragma unroll
                     for (int k = 0; k < 16; k += 4)
                         *reinterpret_cast<float4*>(out + row * inDim + 16 * c16 + k) =
-                            c1 > c0 ? make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            cnt ? make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
             }
         }
-    } else if (status) {
+    } else if (status && tid == 0) {
         atomicOr(status, kErrTensorWait);
     }
     tc_sync();

@@ -33,6 +33,8 @@ TRIANGLE_TEST_BINARY_BVH = 1
 SHADE_ORDER_QUEUE = 0
 SHADE_ORDER_BY_MATERIAL = 1
 SHADE_ORDER_DEFAULT = SHADE_ORDER_BY_MATERIAL
+COLLAPSE_SAH = 0
+COLLAPSE_GREEDY = 1
 
 
 class GpuError(RuntimeError):
@@ -48,7 +50,7 @@ class Config(C.Structure):
 class BvhStats(C.Structure):
     _fields_ = [("triangles", C.c_uint32), ("binary_nodes", C.c_uint32), ("binary_levels", C.c_uint32),
                 ("wide_nodes", C.c_uint32), ("wide_depth", C.c_uint32), ("sah_cost", C.c_float),
-                ("build_ms", C.c_float), ("spheres", C.c_uint32)]
+                ("build_ms", C.c_float), ("spheres", C.c_uint32), ("child_slots", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -66,6 +68,10 @@ class RenderOptions(C.Structure):
 
 class TraversalOptions(C.Structure):
     _fields_ = [("triangle_test", C.c_uint32), ("max_visits", C.c_uint32), ("stack_limit", C.c_uint32)]
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [("collapse", C.c_uint32), ("triangle_cost", C.c_float)]
 
 
 class GlbInfo(C.Structure):
@@ -123,6 +129,7 @@ def lib():
         L.alpine_gpu_synchronize.argtypes = [vp]
         L.alpine_gpu_trace_noalloc.argtypes = [vp, vp, C.c_uint64, vp]
         L.alpine_gpu_set_traversal_options.argtypes = [vp, C.POINTER(TraversalOptions)]
+        L.alpine_gpu_set_build_options.argtypes = [vp, C.POINTER(BuildOptions)]
         f3 = C.POINTER(C.c_float)
         u32p = C.POINTER(C.c_uint32)
         L.alpine_gpu_set_materials.argtypes = [vp, vp, C.c_uint32]
@@ -305,6 +312,13 @@ class Context:
         BVH) and the per-ray device-side limits (0 = defaults)."""
         o = TraversalOptions(triangle_test, max_visits, stack_limit)
         self._check(self.L.alpine_gpu_set_traversal_options(self.h, C.byref(o)))
+
+    def set_build_options(self, collapse=COLLAPSE_SAH, triangle_cost=0.0):
+        """Collapse rule of the next builds (COLLAPSE_SAH: SAH-optimal, the
+        default; COLLAPSE_GREEDY: the reference's rule) and the SAH cost of a
+        triangle test per wide-node visit (0 = 1.0)."""
+        o = BuildOptions(collapse, triangle_cost)
+        self._check(self.L.alpine_gpu_set_build_options(self.h, C.byref(o)))
 
     def traversal_stats(self, rays_ptr: int, n: int, any_hit: bool):
         """(wide nodes fetched, triangles tested) summed over n device rays."""

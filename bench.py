@@ -204,9 +204,9 @@ def cpu_baseline(verts, idx, closest, shadow, budget_s):
 GUIDING_RES = (1920, 1080)
 GUIDING_DEPTH = 12
 # training schedule measured best on B200 (waves of 8 spp, up to 32 Adam
-# steps of about 16,384 samples after each, 512 steps in all)
+# steps of about 16,384 samples after each, 4,096 steps in all)
 GUIDE_OPTIONS = dict(guide=True, guide_fraction=0.5, guide_spp_per_wave=8, guide_batch=16384, guide_steps_per_wave=32,
-                     guide_lr=1e-2, guide_min_roughness=0.2, guide_train_steps=512)
+                     guide_lr=1e-2, guide_min_roughness=0.2, guide_train_steps=4096)
 
 
 def relmse(x, ref):
@@ -257,7 +257,7 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES, guided_repe
     # halves of independent samples (for a fixed guide the estimator is
     # unbiased; per unit time it has far less variance than plain MIS)
     c = context(seed=999, **GUIDE_OPTIONS)
-    c.render(64)  # trains the guide (512 Adam steps) and warms up
+    c.render(128)  # trains the guide (16 waves, 512 Adam steps) and warms up
     halves = []
     for seed in (1000, 2000):
         c.set_render_options(sampler=gpu.RNG_COUNTER, accumulate_fp64=True, seed=seed,
@@ -330,7 +330,7 @@ def guiding_benchmark(device, ref_spp, target=0.01, res=GUIDING_RES, guided_repe
         "resolution": [W, H], "reference_spp": ref_spp, "reference_s": ref_s,
         "reference_relmse_removed": ref_err,
         "relmse": "mean(((x - r)^2 - (h1 - h2)^2 / 4) / (r^2 + 0.01 mean(r)^2)), r = (h1 + h2) / 2",
-        "reference": "the guided estimator after its 512 training steps, frozen, in two independent halves",
+        "reference": "the guided estimator after 512 training steps, frozen, in two independent halves",
         "plain_extrapolated": bool(plain_at and len(plain_at) > 2),
         "guided_extrapolated": bool(guided_at and len(guided_at) > 2),
         "plain_s": plain_at[0] if plain_at else None, "plain_spp": plain_at[1] if plain_at else None,

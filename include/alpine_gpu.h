@@ -77,6 +77,7 @@ typedef struct alpine_gpu_bvh_stats {
     float sah_cost;      /* SAH cost of the wide tree, relative to the root area */
     float build_ms;      /* device time of the last build */
     uint32_t spheres;    /* analytic spheres in the BVH */
+    uint32_t child_slots; /* filled child slots over all wide nodes (of 8 each) */
 } alpine_gpu_bvh_stats;
 
 /* Creates a context on cfg->device (replaces alpine::initialize,
@@ -146,6 +147,28 @@ ALPINE_GPU_API int alpine_gpu_get_vertices(alpine_gpu_ctx* ctx, uint32_t shape_i
  * an 8-wide quantised BVH (Accelerator::updateScene, accelerator.h:31;
  * src/accelerators/wide_bvh.cpp:175-197). stats may be NULL. */
 ALPINE_GPU_API int alpine_gpu_build(alpine_gpu_ctx* ctx, alpine_gpu_bvh_stats* stats);
+
+/* How the binary SAH tree is collapsed into 8-wide nodes (the next build):
+ *   COLLAPSE_SAH (0, the default): SAH-optimal. A dynamic program over the
+ *     binary tree picks, for every wide node, the binary nodes that fill its
+ *     slots at least SAH cost (Ylitie, Karras and Laine, HPG 2017). Nodes
+ *     are fuller than under the greedy rule, and rays fetch fewer of them.
+ *   COLLAPSE_GREEDY (1): the reference's rule (src/accelerators/wide_bvh.cpp:
+ *     200-243): open the internal child of largest surface area until the
+ *     8 slots are used.
+ * triangle_cost: SAH cost of one triangle test relative to one wide-node
+ *   visit (COLLAPSE_SAH only); 0 = 1.0 (measured best on B200: a triangle
+ *   test costs about 3.6 node visits of time in the traversal kernel, but
+ *   costs above 1 change little).
+ * Hits do not depend on the collapse, except which of two triangles at
+ * exactly the same distance is reported. */
+#define ALPINE_GPU_COLLAPSE_SAH 0u
+#define ALPINE_GPU_COLLAPSE_GREEDY 1u
+typedef struct alpine_gpu_build_options {
+    uint32_t collapse;
+    float triangle_cost;
+} alpine_gpu_build_options;
+ALPINE_GPU_API int alpine_gpu_set_build_options(alpine_gpu_ctx* ctx, const alpine_gpu_build_options* options);
 
 /* Closest hit for `count` rays in HOST memory (Accelerator::intersect,
  * accelerator.h:33, batched). Pinned buffers are copied in chunks overlapped

@@ -141,6 +141,54 @@ def test_build_is_deterministic(ctx):
     assert h1.tobytes() == h2.tobytes()
 
 
+@pytest.mark.parametrize("rule", [gpu.COLLAPSE_GREEDY, gpu.COLLAPSE_SAH])
+@pytest.mark.parametrize("n,seed,cost", [(2, 71, 0.0), (5, 72, 0.0), (300, 73, 0.0), (20000, 74, 0.0),
+                                         (20000, 75, 0.05), (20000, 76, 4.0)])
+def test_collapse_rules_vs_bruteforce(ctx, rule, n, seed, cost):
+    """Both collapse rules (and SAH triangle costs from very low to very
+    high) give the exact closest and any hits."""
+    ctx.set_build_options(rule, cost)
+    try:
+        verts, idx = scenes.triangle_soup(n, seed=seed, mu=-3.0, sigma=0.5)
+        st = _load(ctx, verts, idx)
+        assert st["wide_nodes"] <= st["child_slots"] <= 8 * st["wide_nodes"]
+        tris = oracle.make_tris(verts, idx)
+        rays = np.concatenate([scenes.primary_rays(32, 32), scenes.incoherent_rays(3000, seed=seed + 100)])
+        compare_closest(rays, tris, ctx.trace(rays), *oracle.closest_brute(rays, tris)[:4])
+        sh = rays.copy()
+        sh[:, 7] = scenes.shadow_tmax(len(rays), seed=seed + 200)
+        assert (ctx.occluded(sh) == oracle.any_brute(sh, tris)).all()
+    finally:
+        ctx.set_build_options()
+
+
+def test_sah_collapse_fills_nodes(ctx):
+    """The SAH-optimal collapse fills more slots per wide node than the
+    greedy rule and rays fetch fewer nodes."""
+    import torch
+
+    verts, idx = scenes.triangle_soup(100000, seed=81, mu=-4.0, sigma=0.5)
+    rays = torch.from_numpy(scenes.incoherent_rays(20000, seed=82)).cuda()
+    res = {}
+    for rule in (gpu.COLLAPSE_GREEDY, gpu.COLLAPSE_SAH):
+        ctx.set_build_options(rule)
+        st = _load(ctx, verts, idx)
+        nodes, tris = ctx.traversal_stats(rays.data_ptr(), rays.shape[0], False)
+        res[rule] = (st["child_slots"] / st["wide_nodes"], nodes / rays.shape[0], tris / rays.shape[0])
+    ctx.set_build_options()
+    print("children per node, nodes and triangles per ray: greedy %s, SAH %s" % (res[1], res[0]))
+    assert res[gpu.COLLAPSE_SAH][0] > res[gpu.COLLAPSE_GREEDY][0]
+    assert res[gpu.COLLAPSE_SAH][1] < res[gpu.COLLAPSE_GREEDY][1]
+
+
+def test_build_options_rejected(ctx):
+    with pytest.raises(gpu.GpuError):
+        ctx.set_build_options(7)
+    with pytest.raises(gpu.GpuError):
+        ctx.set_build_options(gpu.COLLAPSE_SAH, -1.0)
+    ctx.set_build_options()
+
+
 def test_device_pointer_api(ctx):
     import torch
 
