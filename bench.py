@@ -78,6 +78,8 @@ def parse_args():
     p.add_argument("--no-room", action="store_true", help="skip the small-room render measurement")
     p.add_argument("--profile", action="store_true",
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
+    p.add_argument("--collapse-sweep", action="store_true",
+                   help="traversal workload under each wide-BVH collapse rule and SAH triangle cost (one JSON line each)")
     return p.parse_args()
 
 
@@ -789,8 +791,55 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def collapse_sweep(device=0):
+    """The traversal workload's BVH built with the reference's greedy collapse
+    and with the SAH-optimal one at several triangle costs: filled slots per
+    wide node, node visits and triangle tests per closest-hit ray, and the
+    device Mrays/s of each half of the workload (traversal_split). Hits are
+    compared with the greedy build's (they differ only on exact ties)."""
+    import torch
+
+    from alpine_b200 import gpu, scenes
+
+    verts, idx, closest, shadow = scenes.traversal_workload()
+    n = closest.shape[0]
+    half = n // 2
+    ctx = gpu.Context(device)
+    ctx.add_mesh(verts, idx)
+    d_closest = torch.from_numpy(closest).cuda()
+    d_shadow = torch.from_numpy(shadow).cuda()
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    d_occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    first = None
+    for name, rule, cost in [("greedy", gpu.COLLAPSE_GREEDY, 0.0)] + [
+            (f"sah_{c}", gpu.COLLAPSE_SAH, c) for c in (0.3, 0.5, 1.0, 2.0)]:
+        ctx.set_build_options(rule, cost)
+        st = ctx.build()
+        r = {"collapse": name, "wide_nodes": st["wide_nodes"], "children_per_node": st["child_slots"] / st["wide_nodes"],
+             "wide_depth": st["wide_depth"], "build_ms": min(ctx.build()["build_ms"] for _ in range(2))}
+        for hn, off in (("coherent", 0), ("incoherent", half)):
+            nv, tv = ctx.traversal_stats(d_closest.data_ptr() + off * RAY_BYTES, half, False)
+            r[f"{hn}_closest_nodes_per_ray"] = nv / half
+            r[f"{hn}_closest_tris_per_ray"] = tv / half
+        r["mrays_s"] = traversal_split(ctx, d_closest, d_shadow, d_hits, d_occ, stream, half, reps=10)
+        ctx.trace_device(d_closest.data_ptr(), n, d_hits.data_ptr(), stream.cuda_stream)
+        ctx.synchronize()
+        h = d_hits.cpu().numpy()
+        first = h.copy() if first is None else first
+        r["prims_differing_from_greedy"] = int((h[:, 0] != first[:, 0]).sum())
+        r["t_differing_from_greedy"] = int((h[:, 1] != first[:, 1]).sum())
+        print(json.dumps(r), flush=True)
+    ctx.set_build_options()
+    ctx.close()
+
+
 def main():
     args = parse_args()
+    if args.collapse_sweep:
+        collapse_sweep()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
