@@ -3,6 +3,7 @@
 #include "guide_host.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -56,8 +57,10 @@ AG_D void encode_row(const Params& g, const Query& q, __nv_bfloat16* row)
 {
     const float3 p = normalise_position(g, mk3(q.pos[0], q.pos[1], q.pos[2]));
 #pragma unroll
+    // one corner's kFeatures fp16 values in one load
+    using Corner = typename std::conditional<kFeatures == 4, uint2, uint32_t>::type;
     for (int l0 = 0; l0 < kLevels; l0 += kEncodeLevels) {
-        __half2 v[kEncodeLevels][8];
+        Corner v[kEncodeLevels][8];
 #pragma unroll
         for (int j = 0; j < kEncodeLevels; ++j)
 #pragma unroll
@@ -65,20 +68,26 @@ AG_D void encode_row(const Params& g, const Query& q, __nv_bfloat16* row)
                 uint32_t idx;
                 float w;
                 grid_corner(g.res[l0 + j], p, c, idx, w);
-                v[j][c] = *reinterpret_cast<const __half2*>(g.grid + ((uint64_t)(l0 + j) * kTableSize + idx) * kFeatures);
+                v[j][c] = *reinterpret_cast<const Corner*>(g.grid + ((uint64_t)(l0 + j) * kTableSize + idx) * kFeatures);
             }
 #pragma unroll
         for (int j = 0; j < kEncodeLevels; ++j) {
-            float f0 = 0.0f, f1 = 0.0f;
+            float f[kFeatures] = {};
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 uint32_t idx;
                 float w;
                 grid_corner(g.res[l0 + j], p, c, idx, w);
-                f0 += w * __low2float(v[j][c]);
-                f1 += w * __high2float(v[j][c]);
+                const __half2* h = reinterpret_cast<const __half2*>(&v[j][c]);
+#pragma unroll
+                for (int k = 0; k < kFeatures / 2; ++k) {
+                    f[2 * k] += w * __low2float(h[k]);
+                    f[2 * k + 1] += w * __high2float(h[k]);
+                }
             }
-            *reinterpret_cast<uint32_t*>(row + 2 * (l0 + j)) = pack_bf2(f0, f1);
+#pragma unroll
+            for (int k = 0; k < kFeatures; k += 2)
+                *reinterpret_cast<uint32_t*>(row + kFeatures * (l0 + j) + k) = pack_bf2(f[k], f[k + 1]);
         }
     }
     float ex[8];
@@ -620,14 +629,17 @@ __global__ void __launch_bounds__(32 * kTrainRowWarps) k_train_rows(Params g, co
         if (valid) {
             const float3 p = normalise_position(g, mk3(smp.q.pos[0], smp.q.pos[1], smp.q.pos[2]));
             for (int lv = 0; lv < kLevels; ++lv) {
-                const float d0 = dIn[lane * kGridDims + 2 * lv], d1 = dIn[lane * kGridDims + 2 * lv + 1];
+                float d[kFeatures];
+#pragma unroll
+                for (int k = 0; k < kFeatures; ++k) d[k] = dIn[lane * kGridDims + kFeatures * lv + k];
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
                     uint32_t idx;
                     float w;
                     grid_corner(g.res[lv], p, c, idx, w);
                     float2* dst = reinterpret_cast<float2*>(dGrid + ((uint64_t)lv * kTableSize + idx) * kFeatures);
-                    atomicAdd(dst, make_float2(w * d0, w * d1));
+#pragma unroll
+                    for (int k = 0; k < kFeatures / 2; ++k) atomicAdd(dst + k, make_float2(w * d[2 * k], w * d[2 * k + 1]));
                 }
             }
         }

@@ -22,8 +22,12 @@
 namespace ag {
 namespace guide {
 
-constexpr int kLevels = 16;
-constexpr int kFeatures = 2;                 // per level
+#ifndef AG_GUIDE_FEATURES
+#define AG_GUIDE_FEATURES 2
+#endif
+constexpr int kFeatures = AG_GUIDE_FEATURES;  // per level (2 or 4)
+constexpr int kLevels = 32 / kFeatures;
+static_assert(kFeatures == 2 || kFeatures == 4, "2 or 4 features per level");
 constexpr uint32_t kTableLog2 = 19;
 constexpr uint32_t kTableSize = 1u << kTableLog2;
 constexpr int kGridDims = kLevels * kFeatures;  // 32

@@ -50,7 +50,8 @@ def _check_spheres(rays, sph, hits, tri_t=None, tri_prim=None):
     assert ok.all(), f"{(~ok).sum()} rays disagree on hit / miss"
     both = exp_hit & got_hit & ~near_tangent
     assert (np.abs(g_t[both] - exp_t[both]) <= tol[both]).all(), "t outside the FP64 tolerance"
-    sphere_expected = both & (bt < tri_t - tol) & (second > bt + 2 * tol)
+    with np.errstate(invalid="ignore"):  # inf - inf where no triangle or second sphere is hit
+        sphere_expected = both & (bt < tri_t - tol) & (second > bt + 2 * tol)
     assert (g_prim[sphere_expected] == (SPH | best[sphere_expected])).all(), "wrong sphere reported"
     tri_expected = both & (tri_t < bt - tol)
     if tri_prim is not None:

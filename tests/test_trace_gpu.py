@@ -164,7 +164,8 @@ def test_collapse_rules_vs_bruteforce(ctx, rule, n, seed, cost):
 
 def test_sah_collapse_fills_nodes(ctx):
     """The SAH-optimal collapse fills more slots per wide node than the
-    greedy rule and rays fetch fewer nodes."""
+    greedy rule, and lowers what it minimises: node visits plus triangle
+    tests (at the default triangle cost of 1 node visit) per ray."""
     import torch
 
     verts, idx = scenes.triangle_soup(100000, seed=81, mu=-4.0, sigma=0.5)
@@ -178,7 +179,8 @@ def test_sah_collapse_fills_nodes(ctx):
     ctx.set_build_options()
     print("children per node, nodes and triangles per ray: greedy %s, SAH %s" % (res[1], res[0]))
     assert res[gpu.COLLAPSE_SAH][0] > res[gpu.COLLAPSE_GREEDY][0]
-    assert res[gpu.COLLAPSE_SAH][1] < res[gpu.COLLAPSE_GREEDY][1]
+    cost = {k: v[1] + 1.0 * v[2] for k, v in res.items()}
+    assert cost[gpu.COLLAPSE_SAH] < 0.95 * cost[gpu.COLLAPSE_GREEDY]
 
 
 def test_build_options_rejected(ctx):
