@@ -528,7 +528,7 @@ class Context:
         wc, gp, ts = C.c_uint32(), C.c_uint64(), C.c_uint32()
         res = (C.c_uint32 * 16)()
         self._check(self.L.alpine_gpu_guide_dims(C.byref(wc), C.byref(gp), C.byref(ts), res))
-        return {"weights": wc.value, "grid_params": gp.value, "table_size": ts.value, "res": list(res)}
+        return {"weights": wc.value, "grid_params": gp.value, "table_size": ts.value, "res": [r for r in res if r]}
 
     def guide_reset(self, seed, lo, hi):
         self._check(self.L.alpine_gpu_guide_reset(self.h, seed, _f3(lo), _f3(hi)))

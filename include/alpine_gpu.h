@@ -530,7 +530,10 @@ ALPINE_GPU_API int alpine_gpu_post_process(alpine_gpu_ctx* ctx, int tonemap, flo
  * the integrator uses it when alpine_gpu_render_options.guide is set.
  * Query record: 12 floats {pos[3], roughness, wo[3], 0, normal[3], 0}.
  * Sample record: 16 floats {query[12], dir[3], weight}.
- * Raw output: 40 floats = 8 lobes x {direction[3], log kappa, logit}. */
+ * Raw output: 40 floats = 8 lobes x {direction[3], log kappa, logit}.
+ * alpine_gpu_guide_dims: resolutions receives one grid resolution per level
+ * (16 levels of 2 features; room for 16 entries), the grid parameters are
+ * [level][entry][feature]. */
 ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_params, uint32_t* table_size,
                                          uint32_t* resolutions);
 ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],

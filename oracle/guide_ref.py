@@ -94,8 +94,8 @@ def grid_flat_indices(queries, lo, hi, res):
     out = []
     for l in range(LEVELS):
         idx, _ = corners(p, res[l])
-        base = (np.uint64(l) * np.uint64(T) + idx) * np.uint64(2)
-        out += [base.reshape(-1), (base + np.uint64(1)).reshape(-1)]
+        base = (np.uint64(l) * np.uint64(T) + idx) * np.uint64(FEAT)
+        out += [(base + np.uint64(f)).reshape(-1) for f in range(FEAT)]
     return np.unique(np.concatenate(out))
 
 
@@ -107,14 +107,12 @@ def encode(queries, lo, hi, res, grid_lookup, half=True):
     X = np.zeros((n, IN))
     for l in range(LEVELS):
         idx, w = corners(p, res[l])
-        base = (np.uint64(l) * np.uint64(T) + idx) * np.uint64(2)
-        v0 = np.asarray(grid_lookup(base.reshape(-1)), np.float64).reshape(n, 8)
-        v1 = np.asarray(grid_lookup((base + np.uint64(1)).reshape(-1)), np.float64).reshape(n, 8)
-        if half:
-            v0 = v0.astype(np.float16).astype(np.float64)
-            v1 = v1.astype(np.float16).astype(np.float64)
-        X[:, 2 * l] = (w * v0).sum(1)
-        X[:, 2 * l + 1] = (w * v1).sum(1)
+        base = (np.uint64(l) * np.uint64(T) + idx) * np.uint64(FEAT)
+        for f in range(FEAT):
+            v = np.asarray(grid_lookup((base + np.uint64(f)).reshape(-1)), np.float64).reshape(n, 8)
+            if half:
+                v = v.astype(np.float16).astype(np.float64)
+            X[:, FEAT * l + f] = (w * v).sum(1)
     nrm = q[:, 8:11]
     nl = np.linalg.norm(nrm, axis=1, keepdims=True)
     nrm = np.where(nl > 0, nrm / np.maximum(nl, 1e-30), np.array([0, 0, 1.0]))

@@ -121,9 +121,9 @@ def test_gradients_match_oracle(ctx):
     gref = {}
     for l in range(G.LEVELS):
         idx, cw = G.corners(p, res[l])
-        base = (np.uint64(l) * np.uint64(G.T) + idx) * np.uint64(2)
-        for f in range(2):
-            contrib = cw * dX[:, 2 * l + f][:, None]
+        base = (np.uint64(l) * np.uint64(G.T) + idx) * np.uint64(G.FEAT)
+        for f in range(G.FEAT):
+            contrib = cw * dX[:, G.FEAT * l + f][:, None]
             for i, c in zip((base + np.uint64(f)).reshape(-1).tolist(), contrib.reshape(-1).tolist()):
                 gref[i] = gref.get(i, 0.0) + c
     gr = np.array([gref.get(int(i), 0.0) for i in gidx])
