@@ -732,7 +732,7 @@ def run_ours(args):
         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_from_profile(),
         "traffic_source": "DRAM bytes of one full-size launch from the committed ncu summary of this workload "
                           "(profiles/trace_closest_soup1M.md); not captured in this run",
-        "limiter": "instruction issue and SIMD divergence: the BVH (about 57 MB) is served from L2, so DRAM "
+        "limiter": "instruction issue and SIMD divergence: the BVH (about 65 MB) is served from L2, so DRAM "
                    "traffic is a small fraction of the algorithmic bytes",
         "l2": {"achieved": achieved, "peak": l2_gbs, "frac": achieved / l2_gbs if l2_gbs else None,
                "peak_source": "L2-resident device copy (best of 4-24 MiB buffers) measured in this run"},
