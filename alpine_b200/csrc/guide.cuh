@@ -23,7 +23,7 @@ namespace ag {
 namespace guide {
 
 #ifndef AG_GUIDE_FEATURES
-#define AG_GUIDE_FEATURES 2
+#define AG_GUIDE_FEATURES 4
 #endif
 constexpr int kFeatures = AG_GUIDE_FEATURES;  // per level (2 or 4)
 constexpr int kLevels = 32 / kFeatures;

@@ -532,7 +532,7 @@ ALPINE_GPU_API int alpine_gpu_post_process(alpine_gpu_ctx* ctx, int tonemap, flo
  * Sample record: 16 floats {query[12], dir[3], weight}.
  * Raw output: 40 floats = 8 lobes x {direction[3], log kappa, logit}.
  * alpine_gpu_guide_dims: resolutions receives one grid resolution per level
- * (16 levels of 2 features; room for 16 entries), the grid parameters are
+ * (8 levels of 4 features; room for 16 entries), the grid parameters are
  * [level][entry][feature]. */
 ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_params, uint32_t* table_size,
                                          uint32_t* resolutions);

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-LEVELS, FEAT, T_LOG2 = 16, 2, 19
+LEVELS, FEAT, T_LOG2 = 8, 4, 19
 T = 1 << T_LOG2
 GRID_DIMS = LEVELS * FEAT
 IN, HID, OUT, LOBES, LAYERS = 64, 64, 48, 8, 5
