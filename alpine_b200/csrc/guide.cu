@@ -80,9 +80,9 @@ AG_D void encode_row(const Params& g, const Query& q, __nv_bfloat16* row)
                 grid_corner(g.res[l0 + j], p, c, idx, w);
                 const __half2* h = reinterpret_cast<const __half2*>(&v[j][c]);
 #pragma unroll
-                for (int k = 0; k < kFeatures / 2; ++k) {
-                    f[2 * k] += w * __low2float(h[k]);
-                    f[2 * k + 1] += w * __high2float(h[k]);
+                for (int k = 0; k < kFeatures / 2; ++k) {  // one rounding per corner, in corner order
+                    f[2 * k] = __fmaf_rn(w, __low2float(h[k]), f[2 * k]);
+                    f[2 * k + 1] = __fmaf_rn(w, __high2float(h[k]), f[2 * k + 1]);
                 }
             }
 #pragma unroll

@@ -99,8 +99,21 @@ def grid_flat_indices(queries, lo, hi, res):
     return np.unique(np.concatenate(out))
 
 
+def fma32(a, b, c):
+    """FP32 fused multiply-add of FP32 arrays, through FP64: a * b is exact
+    there for the encoding's operands (a 24-bit weight times an 11-bit FP16
+    value), and the sum is rounded once to FP32 (twice only when the
+    exponents of the product and c differ by more than 18)."""
+    return (np.asarray(a, np.float64) * np.asarray(b, np.float64) + np.asarray(c, np.float64)).astype(np.float32)
+
+
 def encode(queries, lo, hi, res, grid_lookup, half=True):
-    """Inputs (n, 64). grid_lookup(flat_indices) -> fp32 parameter values."""
+    """Inputs (n, 64). grid_lookup(flat_indices) -> fp32 parameter values.
+    half=True reproduces the GPU's encoding: FP16 grid values, each feature
+    summed over the 8 corners in corner order by FP32 fused multiply-adds
+    (src: alpine_b200/csrc/guide.cu, encode_row), so that the BF16 rounding
+    of an input that lands near a rounding boundary goes the same way.
+    half=False sums the FP32 values in FP64."""
     q = np.asarray(queries, np.float64)
     p = normalise(q[:, 0:3], lo, hi)
     n = q.shape[0]
@@ -111,8 +124,13 @@ def encode(queries, lo, hi, res, grid_lookup, half=True):
         for f in range(FEAT):
             v = np.asarray(grid_lookup((base + np.uint64(f)).reshape(-1)), np.float64).reshape(n, 8)
             if half:
-                v = v.astype(np.float16).astype(np.float64)
-            X[:, FEAT * l + f] = (w * v).sum(1)
+                v = v.astype(np.float16).astype(np.float32)
+                acc = np.zeros(n, np.float32)
+                for c in range(8):
+                    acc = fma32(w[:, c], v[:, c], acc)
+                X[:, FEAT * l + f] = acc
+            else:
+                X[:, FEAT * l + f] = (w * v).sum(1)
     nrm = q[:, 8:11]
     nl = np.linalg.norm(nrm, axis=1, keepdims=True)
     nrm = np.where(nl > 0, nrm / np.maximum(nl, 1e-30), np.array([0, 0, 1.0]))
