@@ -108,6 +108,18 @@ int alpine_gpu_guide_infer(alpine_gpu_ctx* c, const float* queries, uint32_t n, 
     return c->check_device_status();
 }
 
+int alpine_gpu_guide_infer_device(alpine_gpu_ctx* c, const float* queries, uint32_t n, float* raw, void* stream)
+{
+    if (!c || (n && (!queries || !raw))) return c ? c->fail(ALPINE_GPU_ERR_INVALID_ARGUMENT, "null buffer") : -1;
+    if (int rc = ensure_guide(c)) return rc;
+    if (n == 0) return ALPINE_GPU_OK;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    c->guide.infer(reinterpret_cast<const G::Query*>(queries), n, raw, st, c->dStatus);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(ALPINE_GPU_ERR_CUDA, std::string("guide_infer_device: ") + cudaGetErrorString(e));
+    return ALPINE_GPU_OK;
+}
+
 int alpine_gpu_guide_set_gradient_kernel(alpine_gpu_ctx* c, int kernel)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;

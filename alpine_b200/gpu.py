@@ -166,6 +166,7 @@ def lib():
         L.alpine_gpu_guide_dims.argtypes = [u32p, C.POINTER(C.c_uint64), u32p, u32p]
         L.alpine_gpu_guide_reset.argtypes = [vp, C.c_uint32, f3, f3]
         L.alpine_gpu_guide_infer.argtypes = [vp, vp, C.c_uint32, vp]
+        L.alpine_gpu_guide_infer_device.argtypes = [vp, vp, C.c_uint32, vp, vp]
         L.alpine_gpu_guide_steps.argtypes = [vp, u32p, u32p, C.POINTER(C.c_float)]
         L.alpine_gpu_guide_set_kernel.argtypes = [vp, C.c_int]
         L.alpine_gpu_guide_set_gradient_kernel.argtypes = [vp, C.c_int]
@@ -554,6 +555,12 @@ class Context:
         raw = np.empty((q.shape[0], 40), np.float32)
         self._check(self.L.alpine_gpu_guide_infer(self.h, _ptr(q), q.shape[0], _ptr(raw)))
         return raw
+
+    def guide_infer_device(self, queries_ptr: int, n: int, raw_ptr: int, stream: int = 0):
+        """Inference on device buffers (float32[n, 12] in, float32[n, 40] out)
+        on `stream`, without synchronising."""
+        self._check(self.L.alpine_gpu_guide_infer_device(self.h, C.c_void_p(queries_ptr), n, C.c_void_p(raw_ptr),
+                                                         C.c_void_p(stream or None)))
 
     def guide_gradients(self, samples, grid_index=None):
         s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)

@@ -745,11 +745,13 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(verts, idx, closest, shadow, args.cpu_seconds)
-    guiding = batched = many = room = None
+    guiding = batched = many = room = ginfer = None
     if rank == 0 and world == 1 and (not args.no_guiding or args.batch_frames or not args.no_many_lights
                                      or not args.no_room):
         ctx.close()
         ctx = None
+    if rank == 0 and world == 1 and not args.no_guiding:
+        ginfer = guide_inference_benchmark(local, l2_gbs)
     if rank == 0 and world == 1 and not args.no_room:
         room = room_benchmark(local)
     if rank == 0 and world == 1 and not args.no_many_lights:
@@ -783,12 +785,79 @@ def run_ours(args):
             "batch": batched,
             "many_lights": many,
             "room": room,
+            "guide_inference": ginfer,
         }
         print(json.dumps(line), flush=True)
     if ctx is not None:
         ctx.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def guide_inference_benchmark(device, l2_gbs, n=1 << 21, reps=10):
+    """Device throughput of the guide's inference (`alpine_gpu_guide_infer_device`,
+    the render's k_infer with raw outputs) on n queries, both inference
+    kernels, CUDA events on the launching stream (mean of `reps` launches
+    after 3 warm-ups). Queries are uniform in the unit scene box with random
+    directions and normals: a harsher gather pattern than a render's, whose
+    queries lie on surfaces. The model is freshly initialised (the time does
+    not depend on the parameter values).
+    Roofline quantities per query: MLP FLOPs 2 x (4 x 64 x 64 + 64 x 48)
+    (inputs padded to 64, outputs to 48), against the measured BF16 GEMM peak;
+    bytes: the hash-grid corner gathers (levels x 8 corners x features x 2 B
+    of FP16) plus 48 B of query in and 160 B of outputs, against the L2 copy
+    bandwidth measured in this run (the grid is L2-resident)."""
+    import torch
+
+    from alpine_b200 import gpu
+
+    ctx = gpu.Context(device)
+    ctx.guide_reset(1, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    dims = ctx.guide_dims()
+    levels = len(dims["res"])
+    features = dims["grid_params"] // (levels * dims["table_size"])
+    g = torch.Generator(device="cuda").manual_seed(7)
+    q = torch.zeros((n, 12), dtype=torch.float32, device="cuda")
+    q[:, 0:3] = torch.rand((n, 3), generator=g, device="cuda")
+    q[:, 3] = 0.02 + 0.98 * torch.rand(n, generator=g, device="cuda")
+    for a, b in ((4, 7), (8, 11)):
+        v = torch.randn((n, 3), generator=g, device="cuda")
+        q[:, a:b] = v / v.norm(dim=1, keepdim=True)
+    raw = torch.empty((n, 40), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    flops = 2.0 * (4 * 64 * 64 + 64 * 48)
+    gather = levels * 8 * features * 2
+    io = 48 + 160
+    bf16_peak = None
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        bf16_peak = float(json.load(open(path))["bf16_tflops"])
+    out = {"queries": n, "levels": levels, "features_per_level": features,
+           "flops_per_query": flops, "gather_bytes_per_query": gather, "io_bytes_per_query": io}
+    for name, kernel in (("warp_mma", gpu.GUIDE_KERNEL_WARP_MMA), ("tensor_memory", gpu.GUIDE_KERNEL_TENSOR_MEMORY)):
+        ctx.guide_set_kernel(kernel)
+        for _ in range(3):
+            ctx.guide_infer_device(q.data_ptr(), n, raw.data_ptr(), sp)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(reps):
+            ctx.guide_infer_device(q.data_ptr(), n, raw.data_ptr(), sp)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        s = ev[0].elapsed_time(ev[1]) / 1e3 / reps
+        tflops = n * flops / s / 1e12
+        gbs = n * (gather + io) / s / 1e9
+        out[name] = {"ms": s * 1e3, "gqueries_per_s": n / s / 1e9, "tflops": tflops,
+                     "tflops_frac": tflops / bf16_peak if bf16_peak else None, "gbs": gbs,
+                     "l2_frac": gbs / l2_gbs if l2_gbs else None}
+    ctx.guide_set_kernel(gpu.GUIDE_KERNEL_WARP_MMA)
+    out["peaks"] = {"bf16_tflops": bf16_peak, "bf16_source": "of measured (burst)" if bf16_peak else None,
+                    "l2_gbs": l2_gbs}
+    out["bound"] = "gathers (L1/L2 latency and throughput), not the tensor cores"
+    ctx.close()
+    return out
 
 
 def collapse_sweep(device=0):

@@ -539,6 +539,11 @@ ALPINE_GPU_API int alpine_gpu_guide_dims(uint32_t* weight_count, uint64_t* grid_
 ALPINE_GPU_API int alpine_gpu_guide_reset(alpine_gpu_ctx* ctx, uint32_t seed, const float scene_lo[3],
                                           const float scene_hi[3]);
 ALPINE_GPU_API int alpine_gpu_guide_infer(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw);
+/* The same on DEVICE buffers (queries: 12 floats each, raw: 40 floats each),
+ * launched on `stream` (NULL: the context's stream) without synchronising;
+ * device-side errors are reported by the next alpine_gpu_synchronize. */
+ALPINE_GPU_API int alpine_gpu_guide_infer_device(alpine_gpu_ctx* ctx, const float* queries, uint32_t count, float* raw,
+                                                 void* stream);
 /* Inference kernel of the guide (rendering and alpine_gpu_guide_infer):
  * WARP_MMA (default): each warp runs 32 queries through the MLP with
  *   warp-level mma.sync tiles; TENSOR_MEMORY: tiles of 128 queries run

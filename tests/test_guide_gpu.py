@@ -67,6 +67,24 @@ def test_inference_matches_oracle(ctx):
     assert err < 1e-5
 
 
+def test_device_inference_equals_host(ctx):
+    """alpine_gpu_guide_infer_device on device buffers gives the host entry
+    point's outputs bit for bit."""
+    import torch
+
+    q = _queries(5000, 31)
+    _randomise(ctx, q, 32)
+    host = ctx.guide_infer(q)
+    dq = torch.from_numpy(q).cuda()
+    draw = torch.full((q.shape[0], 40), float("nan"), dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream()
+    ctx.guide_infer_device(dq.data_ptr(), q.shape[0], draw.data_ptr(), s.cuda_stream)
+    ctx.synchronize()
+    s.synchronize()
+    assert draw.cpu().numpy().tobytes() == host.tobytes()
+    ctx.guide_infer_device(dq.data_ptr(), 0, draw.data_ptr(), 0)  # empty: nothing launched
+
+
 @pytest.mark.parametrize("n", [1000, 128, 1, 70000])
 def test_tensor_memory_inference_matches(ctx, n):
     """The tcgen05 kernel (tiles of 128 queries, accumulators in tensor
