@@ -65,18 +65,21 @@ __global__ void __launch_bounds__(kBlock) k_trace_dyn(BvhView bvh, const float4*
 {
     static_assert(kTraversalStack * kBlock * sizeof(uint2) <= 48 * 1024, "static shared memory");
     __shared__ uint2 stack[kTraversalStack * kBlock];
+    // the grid covers the queue's capacity: one ray per thread (a count above
+    // the capacity would be a queue overflow upstream: reported, not traced)
     const uint32_t n = *count;
-    for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        float4 a = rays[2ull * i];
-        float4 b = rays[2ull * i + 1];
-        TraceResult r;
-        uint32_t err = 0, nv = 0, tv = 0;
-        bool hit = trace<kAny, kBinary>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r,
-                                        stack + threadIdx.x, kBlock, err, nv, tv);
-        if (kAny) static_cast<uint8_t*>(out)[i] = hit ? 1 : 0;
-        else static_cast<uint4*>(out)[i] = make_uint4(r.prim, __float_as_uint(r.t), __float_as_uint(r.b1), __float_as_uint(r.b2));
-        if (err) atomicOr(status, err);
-    }
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i == 0 && n > gridDim.x * kBlock) atomicOr(status, kErrQueueOverflow);
+    if (i >= n) return;
+    float4 a = rays[2ull * i];
+    float4 b = rays[2ull * i + 1];
+    TraceResult r;
+    uint32_t err = 0, nv = 0, tv = 0;
+    bool hit = trace<kAny, kBinary>(bvh, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w, r, stack + threadIdx.x,
+                                    kBlock, err, nv, tv);
+    if (kAny) static_cast<uint8_t*>(out)[i] = hit ? 1 : 0;
+    else static_cast<uint4*>(out)[i] = make_uint4(r.prim, __float_as_uint(r.t), __float_as_uint(r.b1), __float_as_uint(r.b2));
+    if (err) atomicOr(status, err);
 }
 
 template <bool kAny>
