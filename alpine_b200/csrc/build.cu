@@ -833,7 +833,7 @@ __global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numI
         int32_t stN[kWidth];
         uint32_t stJ[kWidth];
         int sp = 0;
-        const uint32_t k8 = choice[b] >> 28;
+        const uint32_t k8 = min(max(choice[b] >> 28, 1u), 7u);  // 1..7 by construction; clamped so j stays <= 8
         stN[sp] = root.right;
         stJ[sp++] = 8u - k8;
         stN[sp] = root.left;
