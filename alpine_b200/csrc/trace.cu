@@ -60,17 +60,18 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(BvhView bvh, const 
 // with the block size as a parameter (chosen by the autotuner).
 template <bool kAny, int kBlock, bool kBinary>
 __global__ void __launch_bounds__(kBlock) k_trace_dyn(BvhView bvh, const float4* __restrict__ rays,
-                                                      const uint32_t* __restrict__ count, void* __restrict__ out,
-                                                      uint32_t* __restrict__ status)
+                                                      const uint32_t* __restrict__ count, uint32_t cap,
+                                                      void* __restrict__ out, uint32_t* __restrict__ status)
 {
     static_assert(kTraversalStack * kBlock * sizeof(uint2) <= 48 * 1024, "static shared memory");
     __shared__ uint2 stack[kTraversalStack * kBlock];
     // the grid covers the queue's capacity: one ray per thread (a count above
-    // the capacity would be a queue overflow upstream: reported, not traced)
+    // the capacity would be a queue overflow upstream: reported, and no ray
+    // beyond the capacity is read)
     const uint32_t n = *count;
     const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-    if (i == 0 && n > gridDim.x * kBlock) atomicOr(status, kErrQueueOverflow);
-    if (i >= n) return;
+    if (i == 0 && n > cap) atomicOr(status, kErrQueueOverflow);
+    if (i >= n || i >= cap) return;
     float4 a = rays[2ull * i];
     float4 b = rays[2ull * i + 1];
     TraceResult r;
@@ -105,10 +106,10 @@ void launch_dyn(const BvhView& bvh, const float4* r, const uint32_t* count, uint
 {
     const unsigned blocks = (maxCount + kBlock - 1) / kBlock;
     const bool bin = bvh.triTest == kTriTestBinary;
-    if (any && bin) k_trace_dyn<true, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
-    else if (any) k_trace_dyn<true, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
-    else if (bin) k_trace_dyn<false, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
-    else k_trace_dyn<false, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, out, status);
+    if (any && bin) k_trace_dyn<true, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, maxCount, out, status);
+    else if (any) k_trace_dyn<true, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, maxCount, out, status);
+    else if (bin) k_trace_dyn<false, kBlock, true><<<blocks, kBlock, 0, st>>>(bvh, r, count, maxCount, out, status);
+    else k_trace_dyn<false, kBlock, false><<<blocks, kBlock, 0, st>>>(bvh, r, count, maxCount, out, status);
 }
 }  // namespace
 
