@@ -11,9 +11,14 @@ with a per-object phase, keyed at 60 frames. The BVH is rebuilt every frame.
 graph) per scene. A frame morphs and rebuilds every scene, enqueues every
 render without waiting, then waits for all. Contexts are independent, so the
 GPU runs the renders of different scenes concurrently, overlapping them with
-the rebuilds of other scenes; the scenes' morph + rebuild + enqueue run on a
-pool of host threads, so the per-level host waits of their rebuilds overlap
-too.
+the rebuilds of other scenes. Two ways to rebuild:
+* "async" (the default): the device-driven rebuild (alpine_gpu_build_async,
+  a captured graph replayed every frame). A frame's morph, rebuild and
+  render of every scene are enqueued from one host thread with no host wait
+  until the end of the frame;
+* "sync": the host-driven rebuild, which waits on the host once per BVH
+  level; the scenes' morph + rebuild + enqueue then run on a pool of host
+  threads, so that those waits overlap.
 """
 from __future__ import annotations
 
@@ -150,18 +155,30 @@ class BatchRenderer:
                                  cuda_graph=cuda_graph)
             if autotune:
                 cfg["tuning"] = c.autotune(probe_spp=min(4, cfg["spp"]))
+            c.update_scene(0.0)  # a synchronous build sizes the buffers of the device-driven rebuild
             c.reset_accumulation()
             self.triangles += sum(m["idx"].shape[0] for m in scene["meshes"])
             self.ctxs.append(c)
 
-    def frame(self, t, threads=None):
+    def frame(self, t, threads=None, rebuild="async"):
         """Morph + rebuild + render every scene at time t; returns the summed
-        device build time (ms). A scene's rebuild waits on the host once per
-        BVH level; with threads > 1 the scenes' morph + rebuild + render
-        enqueue run on a pool of host threads (each context is used by one
-        thread at a time; the C calls release the GIL), so those waits
-        overlap instead of adding up."""
+        device build time (ms).
+
+        rebuild="async": every scene's morph, device-driven rebuild and
+        render are enqueued from this thread, then all are waited for.
+        rebuild="sync": a scene's rebuild waits on the host once per BVH
+        level; with threads > 1 the scenes' morph + rebuild + render enqueue
+        run on a pool of host threads (each context is used by one thread at
+        a time; the C calls release the GIL), so those waits overlap instead
+        of adding up."""
         threads = self.threads if threads is None else threads
+        if rebuild == "async":
+            for c, cfg in zip(self.ctxs, self.configs):
+                c.update_scene_async(t)
+                c.render_async(cfg["spp"])
+            for c in self.ctxs:
+                c.render_wait()
+            return sum(c.read_build_stats()["build_ms"] for c in self.ctxs)
 
         def one(i):
             c, cfg = self.ctxs[i], self.configs[i]
@@ -177,12 +194,12 @@ class BatchRenderer:
             c.render_wait()
         return build_ms
 
-    def run(self, frames, start=0, threads=None):
+    def run(self, frames, start=0, threads=None, rebuild="async"):
         """Renders `frames` frames; returns wall time, build time and rates."""
         t0 = time.perf_counter()
         build = 0.0
         for f in range(start, start + frames):
-            build += self.frame(float(f), threads)
+            build += self.frame(float(f), threads, rebuild)
         dt = time.perf_counter() - t0
         samples = frames * sum(c["width"] * c["height"] * c["spp"] for c in self.configs)
         return {"frames": frames, "seconds": dt, "frames_per_s": frames / dt, "samples_per_s": samples / dt,

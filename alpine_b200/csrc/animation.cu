@@ -160,9 +160,11 @@ int alpine_gpu_add_animation_channel(alpine_gpu_ctx* c, uint32_t shape, const fl
     return ALPINE_GPU_OK;
 }
 
-int alpine_gpu_update_scene(alpine_gpu_ctx* c, float time, alpine_gpu_bvh_stats* stats)
+namespace {
+// Alpine::updateScene's morph (src/alpine.cpp:204-212) on the context stream,
+// without waiting.
+int morph_all(alpine_gpu_ctx* c, float time)
 {
-    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     // device copies of the geometry and the attributes first: the morph
     // writes into them
@@ -187,7 +189,22 @@ int alpine_gpu_update_scene(alpine_gpu_ctx* c, float time, alpine_gpu_bvh_stats*
     }
     c->geometryDirty = false;  // the device copy is the newest
     c->bvhDirty = true;
+    return ALPINE_GPU_OK;
+}
+}  // namespace
+
+int alpine_gpu_update_scene(alpine_gpu_ctx* c, float time, alpine_gpu_bvh_stats* stats)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (int rc = morph_all(c, time)) return rc;
     return alpine_gpu_build(c, stats);  // Accelerator::updateScene
+}
+
+int alpine_gpu_update_scene_async(alpine_gpu_ctx* c, float time)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    if (int rc = morph_all(c, time)) return rc;
+    return alpine_gpu_build_async(c, 0u, 0u);
 }
 
 int alpine_gpu_get_vertices(alpine_gpu_ctx* c, uint32_t shape, float* vertices, float* normals)

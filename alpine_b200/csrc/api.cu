@@ -314,7 +314,61 @@ int alpine_gpu_build(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats)
     c->stats.sah_cost = bs.sahCost;
     c->stats.build_ms = bs.buildMs;
     c->stats.child_slots = bs.childSlots;
+    c->stats.big_levels = bs.bigLevels;
+    c->syncBuildPrims = (uint32_t)prims;
     if (stats) *stats = c->stats;
+    return check_status(c);
+}
+
+int alpine_gpu_build_async(alpine_gpu_ctx* c, uint32_t max_binary_levels, uint32_t max_wide_levels)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (int rc = upload_geometry_now(c)) return rc;
+    const uint32_t n = (uint32_t)(c->idx.size() / 3);
+    const uint32_t ns = (uint32_t)c->spheres.size();
+    const uint32_t prims = n + ns;
+    if (prims == 0 || prims != c->syncBuildPrims)
+        return c->fail(ALPINE_GPU_ERR_INVALID_STATE,
+                       "build_async: run alpine_gpu_build first with this scene's primitive count");
+    // default caps: the last synchronous build's depths with a margin for
+    // moving geometry (a deeper tree is reported, not built)
+    const uint32_t lb = c->stats.binary_levels, wd = c->stats.wide_depth;
+    const uint32_t L = max_binary_levels ? max_binary_levels : std::min<uint32_t>(1024u, lb + std::max(4u, lb / 4));
+    const uint32_t W = max_wide_levels ? max_wide_levels : std::min<uint32_t>(64u, wd + 2u);
+    char err[256] = {0};
+    int rc = c->builder.enqueue(c->dVerts.as<float>(), c->dIdx.as<uint32_t>(), n, c->dSpheres.as<float4>(), ns,
+                                c->dNodes.as<ag::WideNode>(), c->dTris.as<ag::TriRecord>(), c->dStatus, c->stream, L,
+                                W, err, sizeof err);
+    if (rc) return c->fail(rc == -2 ? ALPINE_GPU_ERR_CUDA : ALPINE_GPU_ERR_INVALID_ARGUMENT, err);
+    // the node count of the new tree stays on the device: traversals check
+    // child indices against the node array's capacity
+    c->nodeCount = prims + 1;
+    c->triCount = prims;
+    c->bvhDirty = false;
+    return ALPINE_GPU_OK;
+}
+
+int alpine_gpu_read_build_stats(alpine_gpu_ctx* c, alpine_gpu_bvh_stats* stats, uint32_t* graph_captures,
+                                uint32_t* graph_launches)
+{
+    if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (graph_captures) *graph_captures = c->builder.graph_captures();
+    if (graph_launches) *graph_launches = c->builder.graph_launches();
+    if (!stats) return check_status(c);
+    ag::BuildStats bs;
+    char err[256] = {0};
+    if (int rc = c->builder.enqueued_stats(c->stream, &bs, err, sizeof err))
+        return c->fail(rc == -2 ? ALPINE_GPU_ERR_CUDA : ALPINE_GPU_ERR_INVALID_STATE, err);
+    *stats = c->stats;
+    stats->binary_nodes = bs.binaryNodes;
+    stats->binary_levels = bs.binaryLevels;
+    stats->wide_nodes = bs.wideNodes;
+    stats->wide_depth = bs.wideDepth;
+    stats->sah_cost = bs.sahCost;
+    stats->build_ms = bs.buildMs;
+    stats->child_slots = bs.childSlots;
     return check_status(c);
 }
 

@@ -26,6 +26,7 @@
 #include "build.cuh"
 #include "scan.cuh"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -71,6 +72,27 @@ struct BigSplit {
 };
 
 enum Counter { kCntTasks = 0, kCntBig, kCntChunks, kCntInt, kCntTri, kCntSlots, kCntBounds = 8, kCntWords = 32 };
+
+// Device-driven build (Builder::enqueue): the state the host loop keeps,
+// held in counter words instead, so that no kernel needs a host value.
+enum DevCounter {
+    kDevTasks = 20,  // tasks of the current binary level
+    kDevBig,         // big tasks of the current level
+    kDevChunks,      // chunks of the big tasks
+    kDevNodes,       // binary nodes so far (first id of the next level)
+    kDevLevels,      // binary levels that had tasks
+    kDevItems,       // wide nodes of the current collapse level
+    kDevWide,        // wide nodes so far
+    kDevTris,        // triangle records placed so far
+    kDevDepth,       // collapse levels that had items
+    kDevRootAreaInv, // float bits: 1 / half-area of the root box
+};
+static_assert((int)kDevRootAreaInv < (int)kCntWords, "counter words");
+
+// Work-item count of a level kernel: the host's count, or, in a
+// device-driven build, mult times the count a previous kernel left in
+// device memory.
+AG_D uint32_t level_count(const uint32_t* dn, uint32_t n, uint32_t mult = 1u) { return dn ? *dn * mult : n; }
 
 // --------------------------------------------------------------------------
 // Binning arithmetic. Every kernel must compute identical bin indices, so all
@@ -352,10 +374,13 @@ __global__ void k_root(uint32_t n, const uint32_t* __restrict__ bounds, Task* ta
 
 // --------------------------------------------------------------------------
 // Big tasks.
-__global__ void k_bins_clear(uint32_t* bins, uint32_t numBig)
+__global__ void k_bins_clear(uint32_t* bins, uint32_t numBig, const uint32_t* dBig)
 {
-    uint32_t* b = bins + size_t(blockIdx.x) * kTaskBinWords;
-    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(b + k, k);
+    const uint32_t nb = level_count(dBig, numBig);
+    for (uint32_t bi = blockIdx.x; bi < nb; bi += gridDim.x) {
+        uint32_t* b = bins + size_t(bi) * kTaskBinWords;
+        for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(b + k, k);
+    }
 }
 
 struct ChunkRange {
@@ -378,90 +403,98 @@ AG_D ChunkRange chunk_range(uint32_t c, const Task* tasks, const uint32_t* bigLi
 __global__ void __launch_bounds__(kChunkThreads) k_bin_big(const Task* __restrict__ tasks, const uint32_t* __restrict__ refs,
                                                            const float4* __restrict__ primLo, const float4* __restrict__ primHi,
                                                            const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
-                                                           const uint32_t* __restrict__ chunkTask, uint32_t* __restrict__ bigBins)
+                                                           const uint32_t* __restrict__ chunkTask, uint32_t* __restrict__ bigBins,
+                                                           uint32_t numChunks, const uint32_t* __restrict__ dChunks)
 {
     __shared__ uint32_t sb[kTaskBinWords];
-    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(sb + k, k);
-    __syncthreads();
-    Task task;
-    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
-    float sc[3];
+    const uint32_t nc = level_count(dChunks, numChunks);
+    for (uint32_t cb = blockIdx.x; cb < nc; cb += gridDim.x) {
+        for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) bin_init_word(sb + k, k);
+        __syncthreads();
+        Task task;
+        ChunkRange r = chunk_range(cb, tasks, bigList, chunkOff, chunkTask, task);
+        float sc[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) sc[a] = axis_scale(task.clo[a], task.chi[a]);
-    for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) {
-        uint32_t p = refs[i];
-        float4 lo = primLo[p], hi = primHi[p];
-        float cx = centroid(lo.x, hi.x), cy = centroid(lo.y, hi.y), cz = centroid(lo.z, hi.z);
-        float cc[3] = {cx, cy, cz};
+        for (int a = 0; a < 3; ++a) sc[a] = axis_scale(task.clo[a], task.chi[a]);
+        for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) {
+            uint32_t p = refs[i];
+            float4 lo = primLo[p], hi = primHi[p];
+            float cx = centroid(lo.x, hi.x), cy = centroid(lo.y, hi.y), cz = centroid(lo.z, hi.z);
+            float cc[3] = {cx, cy, cz};
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            if (sc[a] == 0.0f) continue;
-            int b = bin_of(cc[a], task.clo[a], sc[a]);
-            bin_accumulate(sb + a * kAxisBinWords + b * kBinWords, lo, hi, cx, cy, cz);
+            for (int a = 0; a < 3; ++a) {
+                if (sc[a] == 0.0f) continue;
+                int b = bin_of(cc[a], task.clo[a], sc[a]);
+                bin_accumulate(sb + a * kAxisBinWords + b * kBinWords, lo, hi, cx, cy, cz);
+            }
         }
-    }
-    __syncthreads();
-    uint32_t* g = bigBins + size_t(r.bi) * kTaskBinWords;
-    for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) {
-        int binBase = k - k % kBinWords;
-        if (sb[binBase + 12] == 0) continue;  // empty bin: nothing to merge
-        int f = k % kBinWords;
-        if (f == 12) atomicAdd(g + k, sb[k]);
-        else if (f < 3 || (f >= 6 && f < 9)) atomicMin(g + k, sb[k]);
-        else atomicMax(g + k, sb[k]);
+        __syncthreads();
+        uint32_t* g = bigBins + size_t(r.bi) * kTaskBinWords;
+        for (int k = threadIdx.x; k < kTaskBinWords; k += blockDim.x) {
+            int binBase = k - k % kBinWords;
+            if (sb[binBase + 12] == 0) continue;  // empty bin: nothing to merge
+            int f = k % kBinWords;
+            if (f == 12) atomicAdd(g + k, sb[k]);
+            else if (f < 3 || (f >= 6 && f < 9)) atomicMin(g + k, sb[k]);
+            else atomicMax(g + k, sb[k]);
+        }
+        __syncthreads();  // sb is cleared again for the next chunk
     }
 }
 
 __global__ void k_split_big(const Task* __restrict__ tasks, const uint32_t* __restrict__ bigList,
                             const uint32_t* __restrict__ bigBins, BigSplit* __restrict__ splits,
-                            Cand* __restrict__ cands, uint32_t* __restrict__ candFlag)
+                            Cand* __restrict__ cands, uint32_t* __restrict__ candFlag, uint32_t numBig,
+                            const uint32_t* __restrict__ dBig)
 {
-    uint32_t bi = blockIdx.x;
-    uint32_t t = bigList[bi];
-    Task task = tasks[t];
-    SplitChoice best;
-    best.cost = FLT_MAX;
-    best.axis = -1;
-    best.bin = 0;
-    best.nL = 0;
-    for (int a = 0; a < 3; ++a) {
-        if (axis_scale(task.clo[a], task.chi[a]) == 0.0f) continue;
-        float v[12];
-        uint32_t cnt;
-        load_bin(bigBins + size_t(bi) * kTaskBinWords + a * kAxisBinWords + lane_id() * kBinWords, v, cnt);
-        eval_axis(a, v, cnt, true, best);
-    }
-    if (lane_id() == 0) {
-        BigSplit s;
-        if (best.axis >= 0) {
-            s.axis = best.axis;
-            s.bin = best.bin;
-            s.mode = 0;
-            s.nL = best.nL;
-            write_cand(cands + 2 * t, best.L, task.begin, best.nL);
-            write_cand(cands + 2 * t + 1, best.R, task.begin + best.nL, task.count - best.nL);
-        } else {
-            // All centroids coincide: split by position. The children inherit
-            // the parent's node box (a NaN in lo marks this for k_compact) and
-            // its point-sized centroid box.
-            float pb[12];
-            const float nan = __uint_as_float(0x7fc00000u);
-            for (int k = 0; k < 3; ++k) {
-                pb[k] = nan;
-                pb[3 + k] = nan;
-                pb[6 + k] = task.clo[k];
-                pb[9 + k] = task.chi[k];
-            }
-            s.axis = 0;
-            s.bin = 0;
-            s.mode = 1;
-            s.nL = task.count / 2;
-            write_cand(cands + 2 * t, pb, task.begin, s.nL);
-            write_cand(cands + 2 * t + 1, pb, task.begin + s.nL, task.count - s.nL);
+    const uint32_t nb = level_count(dBig, numBig);
+    for (uint32_t bi = blockIdx.x; bi < nb; bi += gridDim.x) {
+        uint32_t t = bigList[bi];
+        Task task = tasks[t];
+        SplitChoice best;
+        best.cost = FLT_MAX;
+        best.axis = -1;
+        best.bin = 0;
+        best.nL = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (axis_scale(task.clo[a], task.chi[a]) == 0.0f) continue;
+            float v[12];
+            uint32_t cnt;
+            load_bin(bigBins + size_t(bi) * kTaskBinWords + a * kAxisBinWords + lane_id() * kBinWords, v, cnt);
+            eval_axis(a, v, cnt, true, best);
         }
-        splits[bi] = s;
-        candFlag[2 * t] = 1;
-        candFlag[2 * t + 1] = 1;
+        if (lane_id() == 0) {
+            BigSplit s;
+            if (best.axis >= 0) {
+                s.axis = best.axis;
+                s.bin = best.bin;
+                s.mode = 0;
+                s.nL = best.nL;
+                write_cand(cands + 2 * t, best.L, task.begin, best.nL);
+                write_cand(cands + 2 * t + 1, best.R, task.begin + best.nL, task.count - best.nL);
+            } else {
+                // All centroids coincide: split by position. The children inherit
+                // the parent's node box (a NaN in lo marks this for k_compact) and
+                // its point-sized centroid box.
+                float pb[12];
+                const float nan = __uint_as_float(0x7fc00000u);
+                for (int k = 0; k < 3; ++k) {
+                    pb[k] = nan;
+                    pb[3 + k] = nan;
+                    pb[6 + k] = task.clo[k];
+                    pb[9 + k] = task.chi[k];
+                }
+                s.axis = 0;
+                s.bin = 0;
+                s.mode = 1;
+                s.nL = task.count / 2;
+                write_cand(cands + 2 * t, pb, task.begin, s.nL);
+                write_cand(cands + 2 * t + 1, pb, task.begin + s.nL, task.count - s.nL);
+            }
+            splits[bi] = s;
+            candFlag[2 * t] = 1;
+            candFlag[2 * t + 1] = 1;
+        }
     }
 }
 
@@ -479,22 +512,27 @@ __global__ void __launch_bounds__(kChunkThreads) k_part_count(const Task* __rest
                                                               const float4* __restrict__ primLo, const float4* __restrict__ primHi,
                                                               const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
                                                               const uint32_t* __restrict__ chunkTask, const BigSplit* __restrict__ splits,
-                                                              uint32_t* __restrict__ chunkLeft)
+                                                              uint32_t* __restrict__ chunkLeft, uint32_t numChunks,
+                                                              const uint32_t* __restrict__ dChunks)
 {
-    Task task;
-    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
-    BigSplit s = splits[r.bi];
-    uint32_t c = 0;
-    for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) c += goes_left(s, task, i, refs[i], primLo, primHi);
-#pragma unroll
-    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     __shared__ uint32_t ws[kChunkThreads / 32];
-    if (lane_id() == 0) ws[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t s2 = 0;
-        for (int w = 0; w < kChunkThreads / 32; ++w) s2 += ws[w];
-        chunkLeft[blockIdx.x] = s2;
+    const uint32_t nc = level_count(dChunks, numChunks);
+    for (uint32_t cb = blockIdx.x; cb < nc; cb += gridDim.x) {
+        Task task;
+        ChunkRange r = chunk_range(cb, tasks, bigList, chunkOff, chunkTask, task);
+        BigSplit s = splits[r.bi];
+        uint32_t c = 0;
+        for (uint32_t i = r.begin + threadIdx.x; i < r.end; i += blockDim.x) c += goes_left(s, task, i, refs[i], primLo, primHi);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane_id() == 0) ws[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t s2 = 0;
+            for (int w = 0; w < kChunkThreads / 32; ++w) s2 += ws[w];
+            chunkLeft[cb] = s2;
+        }
+        __syncthreads();  // ws is written again for the next chunk
     }
 }
 
@@ -504,70 +542,75 @@ __global__ void __launch_bounds__(kChunkThreads) k_part_scatter(const Task* __re
                                                                 const uint32_t* __restrict__ bigList, const uint32_t* __restrict__ chunkOff,
                                                                 const uint32_t* __restrict__ chunkTask, const BigSplit* __restrict__ splits,
                                                                 const uint32_t* __restrict__ chunkLeftOff,
-                                                                uint32_t* __restrict__ status)
+                                                                uint32_t* __restrict__ status, uint32_t numChunks,
+                                                                const uint32_t* __restrict__ dChunks)
 {
-    Task task;
-    ChunkRange r = chunk_range(blockIdx.x, tasks, bigList, chunkOff, chunkTask, task);
-    BigSplit s = splits[r.bi];
-    uint32_t leftBefore = chunkLeftOff[blockIdx.x] - chunkLeftOff[chunkOff[r.bi]];
-    uint32_t rightBefore = r.local * kChunk - leftBefore;
-    // each thread owns 4 consecutive references: stable order inside the chunk
-    uint32_t base = r.begin + threadIdx.x * 4;
-    uint32_t p[4];
-    bool f[4];
-    uint32_t nl = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        uint32_t i = base + k;
-        f[k] = false;
-        p[k] = 0;
-        if (i < r.end) {
-            p[k] = refs[i];
-            f[k] = goes_left(s, task, i, p[k], primLo, primHi);
-            nl += f[k];
-        }
-    }
-    uint32_t nvalid = base < r.end ? min(4u, r.end - base) : 0u;
-    // block exclusive scan of (left count, valid count)
     __shared__ uint32_t wl[kChunkThreads / 32], wv[kChunkThreads / 32];
-    uint32_t il = nl, iv = nvalid;
+    const uint32_t nc = level_count(dChunks, numChunks);
+    for (uint32_t cb = blockIdx.x; cb < nc; cb += gridDim.x) {
+        Task task;
+        ChunkRange r = chunk_range(cb, tasks, bigList, chunkOff, chunkTask, task);
+        BigSplit s = splits[r.bi];
+        uint32_t leftBefore = chunkLeftOff[cb] - chunkLeftOff[chunkOff[r.bi]];
+        uint32_t rightBefore = r.local * kChunk - leftBefore;
+        // each thread owns 4 consecutive references: stable order inside the chunk
+        uint32_t base = r.begin + threadIdx.x * 4;
+        uint32_t p[4];
+        bool f[4];
+        uint32_t nl = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t yl = __shfl_up_sync(0xffffffffu, il, o);
-        uint32_t yv = __shfl_up_sync(0xffffffffu, iv, o);
-        if (lane_id() >= (uint32_t)o) { il += yl; iv += yv; }
-    }
-    if (lane_id() == 31) { wl[threadIdx.x >> 5] = il; wv[threadIdx.x >> 5] = iv; }
-    __syncthreads();
-    uint32_t pl = 0, pv = 0;
-    for (uint32_t w = 0; w < (threadIdx.x >> 5); ++w) { pl += wl[w]; pv += wv[w]; }
-    uint32_t leftRank = pl + il - nl;
-    uint32_t rightRank = (pv + iv - nvalid) - leftRank;
+        for (int k = 0; k < 4; ++k) {
+            uint32_t i = base + k;
+            f[k] = false;
+            p[k] = 0;
+            if (i < r.end) {
+                p[k] = refs[i];
+                f[k] = goes_left(s, task, i, p[k], primLo, primHi);
+                nl += f[k];
+            }
+        }
+        uint32_t nvalid = base < r.end ? min(4u, r.end - base) : 0u;
+        // block exclusive scan of (left count, valid count)
+        uint32_t il = nl, iv = nvalid;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        uint32_t i = base + k;
-        if (i >= r.end) break;
-        uint32_t dst = f[k] ? task.begin + leftBefore + leftRank++ : task.begin + s.nL + rightBefore + rightRank++;
-        if (dst >= task.begin + task.count) { atomicOr(status, kErrBadIndex); continue; }
-        refsNext[dst] = p[k];
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t yl = __shfl_up_sync(0xffffffffu, il, o);
+            uint32_t yv = __shfl_up_sync(0xffffffffu, iv, o);
+            if (lane_id() >= (uint32_t)o) { il += yl; iv += yv; }
+        }
+        if (lane_id() == 31) { wl[threadIdx.x >> 5] = il; wv[threadIdx.x >> 5] = iv; }
+        __syncthreads();
+        uint32_t pl = 0, pv = 0;
+        for (uint32_t w = 0; w < (threadIdx.x >> 5); ++w) { pl += wl[w]; pv += wv[w]; }
+        uint32_t leftRank = pl + il - nl;
+        uint32_t rightRank = (pv + iv - nvalid) - leftRank;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t i = base + k;
+            if (i >= r.end) break;
+            uint32_t dst = f[k] ? task.begin + leftBefore + leftRank++ : task.begin + s.nL + rightBefore + rightRank++;
+            if (dst >= task.begin + task.count) { atomicOr(status, kErrBadIndex); continue; }
+            refsNext[dst] = p[k];
+        }
+        __syncthreads();  // wl / wv are written again for the next chunk
     }
 }
 
 // --------------------------------------------------------------------------
 // Small tasks: one warp does bin + split + partition.
-__global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restrict__ tasks, uint32_t numTasks,
-                                                          const uint32_t* __restrict__ refs, uint32_t* __restrict__ refsNext,
-                                                          const float4* __restrict__ primLo, const float4* __restrict__ primHi,
-                                                          const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
-                                                          uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order,
-                                                          uint32_t* __restrict__ status)
+// Task t by one warp; sb: the warp's bins in shared memory.
+AG_D void small_task(uint32_t t, const Task* __restrict__ tasks, const uint32_t* __restrict__ refs,
+                     uint32_t* __restrict__ refsNext, const float4* __restrict__ primLo,
+                     const float4* __restrict__ primHi, const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
+                     uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order, uint32_t* __restrict__ status,
+                     uint32_t* sb, bool bigHandled)
 {
-    __shared__ uint32_t sbins[kSmallWarps][kTaskBinWords];
-    uint32_t w = threadIdx.x >> 5;
-    uint32_t t = blockIdx.x * kSmallWarps + w;
-    if (t >= numTasks) return;
     Task task = tasks[t];
-    if (task.count > kSmallMax) return;  // handled by the big-task kernels
+    if (task.count > kSmallMax) {  // handled by the big-task kernels
+        // a device-driven build runs those kernels on its first levels only
+        if (!bigHandled && lane_id() == 0) atomicOr(status, kErrBuildDepth);
+        return;
+    }
     uint32_t lane = lane_id();
     const uint32_t b0 = task.begin, n = task.count;
 
@@ -594,7 +637,7 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restri
         sc[k] = axis_scale(clo[k], chi[k]);
     }
 
-    uint32_t* sb = sbins[w];
+    __syncwarp();  // the warp's previous task has finished reading sb
     for (int k = lane; k < kTaskBinWords; k += 32) bin_init_word(sb + k, k);
     __syncwarp();
     for (uint32_t i = lane; i < n; i += 32) {
@@ -686,57 +729,79 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restri
     }
 }
 
+__global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restrict__ tasks, uint32_t numTasks,
+                                                          const uint32_t* __restrict__ refs, uint32_t* __restrict__ refsNext,
+                                                          const float4* __restrict__ primLo, const float4* __restrict__ primHi,
+                                                          const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
+                                                          uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order,
+                                                          uint32_t* __restrict__ status, const uint32_t* __restrict__ dTasks,
+                                                          uint32_t bigHandled)
+{
+    __shared__ uint32_t sbins[kSmallWarps][kTaskBinWords];
+    const uint32_t w = threadIdx.x >> 5;
+    const uint32_t nt = level_count(dTasks, numTasks);
+    for (uint32_t t = blockIdx.x * kSmallWarps + w; t < nt; t += gridDim.x * kSmallWarps)
+        small_task(t, tasks, refs, refsNext, primLo, primHi, bnodes, cands, candFlag, order, status, sbins[w],
+                   bigHandled != 0u);
+}
+
 // --------------------------------------------------------------------------
 // Compaction of the children into the next level's task list.
-__global__ void k_cand_keys(const Cand* __restrict__ cands, const uint32_t* __restrict__ candFlag, uint32_t n,
-                            uint32_t* __restrict__ bigFlag, uint32_t* __restrict__ chunkCnt)
+__global__ void k_cand_keys(const Cand* __restrict__ cands, const uint32_t* __restrict__ candFlag, uint32_t nHost,
+                            uint32_t* __restrict__ bigFlag, uint32_t* __restrict__ chunkCnt,
+                            const uint32_t* __restrict__ dTasks)
 {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    bool v = candFlag[j] != 0;
-    bigFlag[j] = v ? cands[j].big : 0u;
-    chunkCnt[j] = v ? cands[j].chunks : 0u;
+    const uint32_t n = level_count(dTasks, nHost, 2u);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        bool v = candFlag[j] != 0;
+        bigFlag[j] = v ? cands[j].big : 0u;
+        chunkCnt[j] = v ? cands[j].chunks : 0u;
+    }
 }
 
 __global__ void k_compact(const Task* __restrict__ tasks, const Cand* __restrict__ cands,
                           const uint32_t* __restrict__ candFlag, const uint32_t* __restrict__ candPos,
-                          const uint32_t* __restrict__ bigPos, const uint32_t* __restrict__ chunkOffSparse, uint32_t n,
-                          uint32_t nodeBase, Task* __restrict__ next, BinNode* __restrict__ bnodes,
-                          uint32_t* __restrict__ bigList, uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ chunkTask)
+                          const uint32_t* __restrict__ bigPos, const uint32_t* __restrict__ chunkOffSparse, uint32_t nHost,
+                          uint32_t nodeBaseHost, Task* __restrict__ next, BinNode* __restrict__ bnodes,
+                          uint32_t* __restrict__ bigList, uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ chunkTask,
+                          const uint32_t* __restrict__ dTasks, const uint32_t* __restrict__ dNodes)
 {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n || !candFlag[j]) return;
-    Cand c = cands[j];
-    uint32_t p = candPos[j];
-    uint32_t node = nodeBase + p;
-    uint32_t parent = tasks[j >> 1].node;
-    if (j & 1) bnodes[parent].right = (int32_t)node;
-    else bnodes[parent].left = (int32_t)node;
-    BinNode b;
-    if (c.lo[0] != c.lo[0]) {  // median split of coincident centroids: inherit parent box
-        b.lo = bnodes[parent].lo;
-        b.hi = bnodes[parent].hi;
-    } else {
-        b.lo = mk3(c.lo[0], c.lo[1], c.lo[2]);
-        b.hi = mk3(c.hi[0], c.hi[1], c.hi[2]);
-    }
-    b.begin = c.begin;
-    b.count = c.count;
-    b.left = -1;
-    b.right = -1;
-    bnodes[node] = b;
-    Task t;
-    for (int k = 0; k < 3; ++k) { t.clo[k] = c.clo[k]; t.chi[k] = c.chi[k]; }
-    t.node = node;
-    t.begin = c.begin;
-    t.count = c.count;
-    next[p] = t;
-    if (c.big) {
-        uint32_t bi = bigPos[j];
-        bigList[bi] = p;
-        uint32_t off = chunkOffSparse[j];
-        chunkOff[bi] = off;
-        for (uint32_t k = 0; k < c.chunks; ++k) chunkTask[off + k] = bi;
+    const uint32_t n = level_count(dTasks, nHost, 2u);
+    const uint32_t nodeBase = level_count(dNodes, nodeBaseHost);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        if (!candFlag[j]) continue;
+        Cand c = cands[j];
+        uint32_t p = candPos[j];
+        uint32_t node = nodeBase + p;
+        uint32_t parent = tasks[j >> 1].node;
+        if (j & 1) bnodes[parent].right = (int32_t)node;
+        else bnodes[parent].left = (int32_t)node;
+        BinNode b;
+        if (c.lo[0] != c.lo[0]) {  // median split of coincident centroids: inherit parent box
+            b.lo = bnodes[parent].lo;
+            b.hi = bnodes[parent].hi;
+        } else {
+            b.lo = mk3(c.lo[0], c.lo[1], c.lo[2]);
+            b.hi = mk3(c.hi[0], c.hi[1], c.hi[2]);
+        }
+        b.begin = c.begin;
+        b.count = c.count;
+        b.left = -1;
+        b.right = -1;
+        bnodes[node] = b;
+        Task t;
+        for (int k = 0; k < 3; ++k) { t.clo[k] = c.clo[k]; t.chi[k] = c.chi[k]; }
+        t.node = node;
+        t.begin = c.begin;
+        t.count = c.count;
+        next[p] = t;
+        if (c.big) {
+            uint32_t bi = bigPos[j];
+            bigList[bi] = p;
+            uint32_t off = chunkOffSparse[j];
+            chunkOff[bi] = off;
+            for (uint32_t k = 0; k < c.chunks; ++k) chunkTask[off + k] = bi;
+        }
     }
 }
 
@@ -756,12 +821,9 @@ AG_D float bn_area(const BinNode& b) { return area_of(b.lo.x, b.lo.y, b.lo.z, b.
 // choice[x] holds the k of D(x, j) when it was taken (0: x keeps j - 1
 // slots; nibble 7: the split of x's own wide node). A binary leaf costs
 // leaf(x) for every j.
-__global__ void k_collapse_cost(const BinNode* __restrict__ bnodes, uint32_t first, uint32_t count, float triCost,
-                                float* __restrict__ cost, uint32_t* __restrict__ choice)
+AG_D void collapse_cost_node(const BinNode* __restrict__ bnodes, uint32_t x, float triCost, float* __restrict__ cost,
+                             uint32_t* __restrict__ choice)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const uint32_t x = first + t;
     const BinNode b = bnodes[x];
     const float A = bn_area(b);
     float* C = cost + 8ull * x;
@@ -812,16 +874,26 @@ __global__ void k_collapse_cost(const BinNode* __restrict__ bnodes, uint32_t fir
     choice[x] = ch;
 }
 
+// One binary level per launch: nodes [first, first + count), or, in a
+// device-driven build, [levelStart[level], levelStart[level + 1]).
+__global__ void k_collapse_cost(const BinNode* __restrict__ bnodes, uint32_t firstHost, uint32_t countHost,
+                                float triCost, float* __restrict__ cost, uint32_t* __restrict__ choice,
+                                const uint32_t* __restrict__ levelStart, uint32_t level)
+{
+    const uint32_t first = levelStart ? levelStart[level] : firstHost;
+    const uint32_t count = levelStart ? levelStart[level + 1] - first : countHost;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x)
+        collapse_cost_node(bnodes, first + t, triCost, cost, choice);
+}
+
 // The slots of one wide node per thread. choice (the cost program's
 // decisions) selects the SAH-optimal distribution; null selects the greedy
 // rule. Slots are then assigned to octants.
-__global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
-                                  const uint32_t* __restrict__ choice, int32_t* __restrict__ slots,
-                                  uint32_t* __restrict__ intCount, uint32_t* __restrict__ triCount,
-                                  uint32_t* __restrict__ slotTotal)
+AG_D void collapse_decide_item(uint32_t i, const uint2* __restrict__ items, const BinNode* __restrict__ bnodes,
+                               const uint32_t* __restrict__ choice, int32_t* __restrict__ slots,
+                               uint32_t* __restrict__ intCount, uint32_t* __restrict__ triCount,
+                               uint32_t* __restrict__ slotTotal)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= numItems) return;
     uint32_t b = items[i].x;
     int32_t ent[kWidth];
     int n = 0;
@@ -919,6 +991,16 @@ __global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numI
     triCount[i] = nt;
 }
 
+__global__ void k_collapse_decide(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
+                                  const uint32_t* __restrict__ choice, int32_t* __restrict__ slots,
+                                  uint32_t* __restrict__ intCount, uint32_t* __restrict__ triCount,
+                                  uint32_t* __restrict__ slotTotal, const uint32_t* __restrict__ dItems)
+{
+    const uint32_t n = level_count(dItems, numItems);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        collapse_decide_item(i, items, bnodes, choice, slots, intCount, triCount, slotTotal);
+}
+
 __host__ __device__ inline uint32_t quant_exponent(float extent)
 {
     // smallest power of two q with 255 * q >= extent (biased exponent byte)
@@ -932,17 +1014,15 @@ __host__ __device__ inline uint32_t quant_exponent(float extent)
     return (uint32_t)biased;
 }
 
-__global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
-                                const int32_t* __restrict__ slots, const uint32_t* __restrict__ intOff,
-                                const uint32_t* __restrict__ triOff, uint32_t wideBase, uint32_t triBase0,
-                                const uint32_t* __restrict__ order, const float* __restrict__ verts,
-                                const uint32_t* __restrict__ idx, uint32_t ntris, const float4* __restrict__ spheres,
-                                WideNode* __restrict__ nodes,
-                                TriRecord* __restrict__ tris, uint2* __restrict__ itemsNext, float* sahAccum,
-                                float rootAreaInv, uint32_t nodeCap, uint32_t triCap, uint32_t* __restrict__ status)
+AG_D void collapse_emit_item(uint32_t i, const uint2* __restrict__ items, const BinNode* __restrict__ bnodes,
+                             const int32_t* __restrict__ slots, const uint32_t* __restrict__ intOff,
+                             const uint32_t* __restrict__ triOff, uint32_t wideBase, uint32_t triBase0,
+                             const uint32_t* __restrict__ order, const float* __restrict__ verts,
+                             const uint32_t* __restrict__ idx, uint32_t ntris, const float4* __restrict__ spheres,
+                             WideNode* __restrict__ nodes, TriRecord* __restrict__ tris, uint2* __restrict__ itemsNext,
+                             float* sahAccum, float rootAreaInv, uint32_t nodeCap, uint32_t triCap,
+                             uint32_t* __restrict__ status)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= numItems) return;
     uint2 it = items[i];
     const BinNode nb = bnodes[it.x];
     WideNode w;
@@ -1035,6 +1115,104 @@ __global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numIte
     atomicAdd(sahAccum, sah);
 }
 
+// One collapse level: the counts and bases are the host's, or, in a
+// device-driven build, counter words (dDev != null: items, wide nodes and
+// triangle records so far, and the root's inverse area).
+__global__ void k_collapse_emit(const uint2* __restrict__ items, uint32_t numItems, const BinNode* __restrict__ bnodes,
+                                const int32_t* __restrict__ slots, const uint32_t* __restrict__ intOff,
+                                const uint32_t* __restrict__ triOff, uint32_t wideBase, uint32_t triBase0,
+                                const uint32_t* __restrict__ order, const float* __restrict__ verts,
+                                const uint32_t* __restrict__ idx, uint32_t ntris, const float4* __restrict__ spheres,
+                                WideNode* __restrict__ nodes,
+                                TriRecord* __restrict__ tris, uint2* __restrict__ itemsNext, float* sahAccum,
+                                float rootAreaInv, uint32_t nodeCap, uint32_t triCap, uint32_t* __restrict__ status,
+                                const uint32_t* __restrict__ dDev)
+{
+    const uint32_t n = dDev ? dDev[kDevItems] : numItems;
+    const uint32_t wb = dDev ? dDev[kDevWide] : wideBase;
+    const uint32_t tb = dDev ? dDev[kDevTris] : triBase0;
+    const float ria = dDev ? __uint_as_float(dDev[kDevRootAreaInv]) : rootAreaInv;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        collapse_emit_item(i, items, bnodes, slots, intOff, triOff, wb, tb, order, verts, idx, ntris, spheres, nodes,
+                           tris, itemsNext, sahAccum, ria, nodeCap, triCap, status);
+}
+
+// --------------------------------------------------------------------------
+// Device-driven build: the host loop's bookkeeping as single-thread kernels.
+__global__ void k_dev_begin(uint32_t n, uint32_t* __restrict__ dv, uint32_t* __restrict__ levelStart)
+{
+    const uint32_t big = n > kSmallMax ? 1u : 0u;
+    dv[kDevTasks] = 1u;
+    dv[kDevBig] = big;
+    dv[kDevChunks] = big ? (n + kChunk - 1) / kChunk : 0u;
+    dv[kDevNodes] = 1u;
+    dv[kDevLevels] = 0u;
+    levelStart[0] = 0u;
+}
+
+// After binary level L: the next level's counts (the scans' totals) become
+// current, the next level's nodes start at the node count so far. Counts
+// beyond the buffers' capacities (impossible for a consistent build) stop
+// the build with an error instead of reaching past the buffers.
+__global__ void k_dev_level_end(uint32_t* __restrict__ dv, uint32_t* __restrict__ levelStart, uint32_t L,
+                                uint32_t capTasks, uint32_t capBig, uint32_t capChunks, uint32_t* __restrict__ status)
+{
+    if (dv[kDevTasks] > 0u) dv[kDevLevels] += 1u;
+    levelStart[L + 1] = dv[kDevNodes];
+    uint32_t t = dv[kCntTasks], b = dv[kCntBig], c = dv[kCntChunks];
+    if (t > capTasks || b > capBig || c > capChunks || dv[kDevNodes] + t > 2u * capTasks) {
+        atomicOr(status, kErrBadIndex);
+        t = b = c = 0u;
+    }
+    dv[kDevNodes] += t;
+    dv[kDevTasks] = t;
+    dv[kDevBig] = b;
+    dv[kDevChunks] = c;
+}
+
+// Before the collapse: the root item, the counters, the root's inverse area
+// (in the host build's order of rounded operations). Tasks left over mean
+// the level cap was too small: the collapse is then skipped (the previous
+// tree stays in place) and the status word says so.
+__global__ void k_dev_collapse_begin(uint32_t* __restrict__ dv, const BinNode* __restrict__ bnodes,
+                                     uint2* __restrict__ items, float* __restrict__ sahAccum,
+                                     uint32_t* __restrict__ status)
+{
+    const bool failed = dv[kDevTasks] != 0u;
+    if (failed) atomicOr(status, kErrBuildDepth);
+    items[0] = make_uint2(0u, 0u);
+    dv[kDevItems] = failed ? 0u : 1u;
+    dv[kDevWide] = 1u;
+    dv[kDevTris] = 0u;
+    dv[kDevDepth] = 0u;
+    dv[kCntSlots] = 0u;
+    *sahAccum = 0.0f;
+    const BinNode rb = bnodes[0];
+    const float ex = __fsub_rn(rb.hi.x, rb.lo.x), ey = __fsub_rn(rb.hi.y, rb.lo.y), ez = __fsub_rn(rb.hi.z, rb.lo.z);
+    const float area = __fadd_rn(__fadd_rn(__fmul_rn(ex, ey), __fmul_rn(ey, ez)), __fmul_rn(ez, ex));
+    dv[kDevRootAreaInv] = __float_as_uint(area > 0.0f ? __fdiv_rn(1.0f, area) : 0.0f);
+}
+
+__global__ void k_dev_wide_end(uint32_t* __restrict__ dv, uint32_t capItems, uint32_t* __restrict__ status)
+{
+    if (dv[kDevItems] > 0u) dv[kDevDepth] += 1u;
+    uint32_t items = dv[kCntInt];
+    if (items > capItems || dv[kDevWide] + items > capItems) {
+        atomicOr(status, kErrBadIndex);
+        items = 0u;
+    }
+    dv[kDevItems] = items;
+    dv[kDevWide] += items;
+    dv[kDevTris] += dv[kCntTri];
+}
+
+__global__ void k_dev_end(const uint32_t* __restrict__ dv, uint32_t n, uint32_t* __restrict__ status)
+{
+    const bool skipped = dv[kDevWide] == 1u && dv[kDevTris] == 0u && dv[kDevDepth] == 0u;
+    if (dv[kDevItems] != 0u || dv[kDevDepth] > (uint32_t)kTraversalStack || (!skipped && dv[kDevTris] != n))
+        atomicOr(status, kErrBuildDepth);
+}
+
 template <typename T>
 T* carve(char*& p, size_t count)
 {
@@ -1057,6 +1235,9 @@ Builder::~Builder() { release(); }
 
 void Builder::release()
 {
+    if (graphExec_) cudaGraphExecDestroy(graphExec_);
+    graphExec_ = nullptr;
+    graphKey_.clear();
     if (mem_) cudaFree(mem_);
     if (hostCounters_) cudaFreeHost(hostCounters_);
     if (ev0_) cudaEventDestroy(ev0_);
@@ -1093,8 +1274,10 @@ int Builder::reserve(uint32_t n, char* err, size_t errLen)
     bytes += carve_bytes<uint32_t>(2 * N);         // collapse choices
     bytes += 4 * carve_bytes<uint32_t>(N + 1);     // intCount, intOff, triCount, triOff
     bytes += carve_bytes<uint32_t>(kCntWords);
-    bytes += carve_bytes<uint32_t>(scan_scratch_words(2 * N + 2));
+    const size_t scanWords = std::max(scan_scratch_words(2 * N + 2), scan3_scratch_words(2 * N + 2));
+    bytes += carve_bytes<uint32_t>(scanWords);
     bytes += carve_bytes<float>(1);
+    bytes += carve_bytes<uint32_t>(kMaxLevels + 2);  // level starts of a device-driven build
     if (cudaMalloc(&mem_, bytes) != cudaSuccess) {
         snprintf(err, errLen, "BVH build: cudaMalloc of %zu bytes failed", bytes);
         mem_ = nullptr;
@@ -1135,8 +1318,9 @@ int Builder::reserve(uint32_t n, char* err, size_t errLen)
     triCount_ = carve<uint32_t>(p, N + 1);
     triOff_ = carve<uint32_t>(p, N + 1);
     counters_ = carve<uint32_t>(p, kCntWords);
-    scanScratch_ = carve<uint32_t>(p, scan_scratch_words(2 * N + 2));
+    scanScratch_ = carve<uint32_t>(p, scanWords);
     sahAccum_ = carve<float>(p, 1);
+    levelStartDev_ = carve<uint32_t>(p, kMaxLevels + 2);
     if (cudaMallocHost(&hostCounters_, kCntWords * sizeof(uint32_t)) != cudaSuccess) {
         snprintf(err, errLen, "BVH build: cudaMallocHost failed");
         cudaGetLastError();
@@ -1178,6 +1362,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     uint32_t nodeCount = 1;
     int cur = 0;
     uint32_t level = 0;
+    bigLevels_ = 0;
     levelStart_.assign(1, 0u);  // binary node ids of level L: [levelStart_[L], levelStart_[L + 1])
     while (numTasks > 0) {
         if (++level > kMaxLevels) {
@@ -1186,28 +1371,29 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         }
         Task* tk = tasks[cur];
         if (numBig > 0) {
-            k_bins_clear<<<numBig, 256, 0, st>>>(bigBins_, numBig);
+            bigLevels_ = level;
+            k_bins_clear<<<numBig, 256, 0, st>>>(bigBins_, numBig, nullptr);
             k_bin_big<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
-                                                             chunkTask_, bigBins_);
-            k_split_big<<<numBig, 32, 0, st>>>(tk, bigList_, bigBins_, splits, cands, candFlag_);
+                                                             chunkTask_, bigBins_, totalChunks, nullptr);
+            k_split_big<<<numBig, 32, 0, st>>>(tk, bigList_, bigBins_, splits, cands, candFlag_, numBig, nullptr);
             k_part_count<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
-                                                                chunkTask_, splits, chunkLeft_);
+                                                                chunkTask_, splits, chunkLeft_, totalChunks, nullptr);
             exclusive_scan(chunkLeft_, chunkLeftOff_, totalChunks, nullptr, scanScratch_, st);
             k_part_scatter<<<totalChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], refs_[cur ^ 1], primLo_, primHi_,
                                                                   bigList_, chunkOff_, chunkTask_, splits,
-                                                                  chunkLeftOff_, deviceStatus);
+                                                                  chunkLeftOff_, deviceStatus, totalChunks, nullptr);
         }
         k_small<<<blocks_for(numTasks, kSmallWarps), 32 * kSmallWarps, 0, st>>>(
             tk, numTasks, refs_[cur], refs_[cur ^ 1], primLo_, primHi_, bnodes_, cands, candFlag_, order_,
-            deviceStatus);
+            deviceStatus, nullptr, 1u);
         const uint32_t nc = 2 * numTasks;
-        k_cand_keys<<<blocks_for(nc, 256), 256, 0, st>>>(cands, candFlag_, nc, bigFlag_, bigChunks_);
+        k_cand_keys<<<blocks_for(nc, 256), 256, 0, st>>>(cands, candFlag_, nc, bigFlag_, bigChunks_, nullptr);
         exclusive_scan(candFlag_, candPos_, nc, counters_ + kCntTasks, scanScratch_, st);
         exclusive_scan(bigFlag_, bigPos_, nc, counters_ + kCntBig, scanScratch_, st);
         exclusive_scan(bigChunks_, chunkOffSparse, nc, counters_ + kCntChunks, scanScratch_, st);
         k_compact<<<blocks_for(nc, 256), 256, 0, st>>>(tk, cands, candFlag_, candPos_, bigPos_, chunkOffSparse, nc,
                                                        nodeCount, tasks[cur ^ 1], bnodes_, bigList_, chunkOff_,
-                                                       chunkTask_);
+                                                       chunkTask_, nullptr, nullptr);
         cudaMemcpyAsync(hostCounters_, counters_, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) {
             snprintf(err, errLen, "BVH build: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1223,6 +1409,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     levelStart_.push_back(nodeCount);
     local.binaryNodes = nodeCount;
     local.binaryLevels = level;
+    local.bigLevels = bigLevels_;
 
     // SAH cost program of the collapse, deepest level first
     const bool sahCollapse = collapse_ == kCollapseSah;
@@ -1230,7 +1417,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         for (size_t L = levelStart_.size() - 1; L-- > 0;) {
             const uint32_t first = levelStart_[L], cnt = levelStart_[L + 1] - first;
             if (cnt) k_collapse_cost<<<blocks_for(cnt, 128), 128, 0, st>>>(bnodes_, first, cnt, triCost_,
-                                                                          collapseCost_, collapseChoice_);
+                                                                          collapseCost_, collapseChoice_, nullptr, 0u);
         }
 
     // Wide collapse.
@@ -1256,14 +1443,14 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         int32_t* slots = reinterpret_cast<int32_t*>(slots_);
         k_collapse_decide<<<blocks_for(numItems, 128), 128, 0, st>>>(
             items, numItems, bnodes_, sahCollapse ? collapseChoice_ : nullptr, slots, intCount_, triCount_,
-            counters_ + kCntSlots);
+            counters_ + kCntSlots, nullptr);
         exclusive_scan(intCount_, intOff_, numItems, counters_ + kCntInt, scanScratch_, st);
         exclusive_scan(triCount_, triOff_, numItems, counters_ + kCntTri, scanScratch_, st);
         k_collapse_emit<<<blocks_for(numItems, 128), 128, 0, st>>>(items, numItems, bnodes_, slots, intOff_, triOff_,
                                                                     wideCount, triCount, order_, verts, idx, ntris,
                                                                     spheres, nodes,
                                                                     tris, itemsNext, sahAccum_, rootAreaInv, n + 1, n,
-                                                                    deviceStatus);
+                                                                    deviceStatus, nullptr);
         cudaMemcpyAsync(hostCounters_ + kCntInt, counters_ + kCntInt, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                         st);
         if (cudaStreamSynchronize(st) != cudaSuccess) {
@@ -1300,6 +1487,197 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         return -4;
     }
     if (stats) *stats = local;
+    return 0;
+}
+
+
+namespace {
+// Grids of the device-driven build: the counts are not known when the
+// launches are made, so each kernel loops over its work items on at most
+// this many blocks (a few waves of the 148 SMs).
+constexpr unsigned kDevChunkBlocks = 148 * 4;
+constexpr unsigned kDevThreadBlocks = 148 * 8;
+inline unsigned dev_blocks(size_t n, int threads, unsigned cap)
+{
+    const size_t b = (n + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+}  // namespace
+
+void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres,
+                               uint32_t n, WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t st,
+                               uint32_t maxLevels, uint32_t maxWideLevels)
+{
+    const size_t N = n;
+    const size_t maxBig = N / kSmallMax + 2;
+    const size_t maxChunks = N / kChunk + maxBig + 2;
+    Task* tasks[2] = {static_cast<Task*>(tasks_[0]), static_cast<Task*>(tasks_[1])};
+    Cand* cands = static_cast<Cand*>(cands_);
+    BigSplit* splits = static_cast<BigSplit*>(bigSplit_);
+    uint32_t* bounds = counters_ + kCntBounds;
+    uint32_t* dv = counters_;
+    const uint32_t rootChunks = n > kSmallMax ? (n + kChunk - 1) / kChunk : 0u;
+
+    k_init_bounds<<<1, 32, 0, st>>>(bounds);
+    k_prep_prims<<<blocks_for(N, 256), 256, 0, st>>>(verts, idx, ntris, spheres, n, primLo_, primHi_, refs_[0], bounds);
+    k_root<<<blocks_for(rootChunks + 1, 256), 256, 0, st>>>(n, bounds, tasks[0], bnodes_, bigList_, chunkOff_,
+                                                            chunkTask_, rootChunks);
+    k_dev_begin<<<1, 1, 0, st>>>(n, dv, levelStartDev_);
+    const unsigned gBig = dev_blocks(maxBig, 1, kDevChunkBlocks);
+    const unsigned gChunks = dev_blocks(maxChunks, 1, kDevChunkBlocks);
+    const unsigned gSmall = dev_blocks(N, kSmallWarps, kDevThreadBlocks);
+    const unsigned gCand = dev_blocks(2 * N, 256, kDevThreadBlocks);
+    // tasks above kSmallMax references occur on the top levels only: the
+    // big-task kernels run on the levels where the last host-driven build had
+    // them, plus a margin (k_small reports a big task met past them)
+    const uint32_t bigCap = std::min(maxLevels, bigLevels_ + 2u);
+    int cur = 0;
+    for (uint32_t L = 0; L < maxLevels; ++L) {
+        Task* tk = tasks[cur];
+        const bool bigLevel = L < bigCap;
+        if (bigLevel) {
+            k_bins_clear<<<gBig, 256, 0, st>>>(bigBins_, 0u, dv + kDevBig);
+            k_bin_big<<<gChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
+                                                         chunkTask_, bigBins_, 0u, dv + kDevChunks);
+            k_split_big<<<gBig, 32, 0, st>>>(tk, bigList_, bigBins_, splits, cands, candFlag_, 0u, dv + kDevBig);
+            k_part_count<<<gChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
+                                                            chunkTask_, splits, chunkLeft_, 0u, dv + kDevChunks);
+            {
+                const uint32_t* in[] = {chunkLeft_};
+                uint32_t* out[] = {chunkLeftOff_};
+                exclusive_scan_count(1, in, out, dv + kDevChunks, 1u, maxChunks, nullptr, scanScratch_, st);
+            }
+            k_part_scatter<<<gChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], refs_[cur ^ 1], primLo_, primHi_,
+                                                              bigList_, chunkOff_, chunkTask_, splits, chunkLeftOff_,
+                                                              deviceStatus, 0u, dv + kDevChunks);
+        }
+        k_small<<<gSmall, 32 * kSmallWarps, 0, st>>>(tk, 0u, refs_[cur], refs_[cur ^ 1], primLo_, primHi_, bnodes_,
+                                                     cands, candFlag_, order_, deviceStatus, dv + kDevTasks,
+                                                     bigLevel ? 1u : 0u);
+        k_cand_keys<<<gCand, 256, 0, st>>>(cands, candFlag_, 0u, bigFlag_, bigChunks_, dv + kDevTasks);
+        {
+            const uint32_t* in[] = {candFlag_, bigFlag_, bigChunks_};
+            uint32_t* out[] = {candPos_, bigPos_, chunkOffSparse_};
+            uint32_t* tot[] = {counters_ + kCntTasks, counters_ + kCntBig, counters_ + kCntChunks};
+            exclusive_scan_count(3, in, out, dv + kDevTasks, 2u, 2 * N, tot, scanScratch_, st);
+        }
+        k_compact<<<gCand, 256, 0, st>>>(tk, cands, candFlag_, candPos_, bigPos_, chunkOffSparse_, 0u, 0u,
+                                         tasks[cur ^ 1], bnodes_, bigList_, chunkOff_, chunkTask_, dv + kDevTasks,
+                                         dv + kDevNodes);
+        k_dev_level_end<<<1, 1, 0, st>>>(dv, levelStartDev_, L, n, (uint32_t)maxBig, (uint32_t)maxChunks,
+                                         deviceStatus);
+        cur ^= 1;
+    }
+
+    k_dev_collapse_begin<<<1, 1, 0, st>>>(dv, bnodes_, reinterpret_cast<uint2*>(items_[0]), sahAccum_, deviceStatus);
+    const bool sahCollapse = collapse_ == kCollapseSah;
+    if (sahCollapse) {
+        const unsigned gCost = dev_blocks(N, 128, kDevThreadBlocks);
+        for (uint32_t L = maxLevels; L-- > 0;)
+            k_collapse_cost<<<gCost, 128, 0, st>>>(bnodes_, 0u, 0u, triCost_, collapseCost_, collapseChoice_,
+                                                   levelStartDev_, L);
+    }
+    const unsigned gItems = dev_blocks(N + 1, 128, kDevThreadBlocks);
+    int ci = 0;
+    for (uint32_t D = 0; D < maxWideLevels; ++D) {
+        const uint2* items = reinterpret_cast<const uint2*>(items_[ci]);
+        uint2* itemsNext = reinterpret_cast<uint2*>(items_[ci ^ 1]);
+        int32_t* slots = reinterpret_cast<int32_t*>(slots_);
+        k_collapse_decide<<<gItems, 128, 0, st>>>(items, 0u, bnodes_, sahCollapse ? collapseChoice_ : nullptr, slots,
+                                                  intCount_, triCount_, counters_ + kCntSlots, dv + kDevItems);
+        {
+            const uint32_t* in[] = {intCount_, triCount_};
+            uint32_t* out[] = {intOff_, triOff_};
+            uint32_t* tot[] = {counters_ + kCntInt, counters_ + kCntTri};
+            exclusive_scan_count(2, in, out, dv + kDevItems, 1u, N + 1, tot, scanScratch_, st);
+        }
+        k_collapse_emit<<<gItems, 128, 0, st>>>(items, 0u, bnodes_, slots, intOff_, triOff_, 0u, 0u, order_, verts, idx,
+                                                ntris, spheres, nodes, tris, itemsNext, sahAccum_, 0.0f, n + 1, n,
+                                                deviceStatus, dv);
+        k_dev_wide_end<<<1, 1, 0, st>>>(dv, n + 1, deviceStatus);
+        ci ^= 1;
+    }
+    k_dev_end<<<1, 1, 0, st>>>(dv, n, deviceStatus);
+}
+
+int Builder::enqueue(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres,
+                     uint32_t nspheres, WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t st,
+                     uint32_t maxLevels, uint32_t maxWideLevels, char* err, size_t errLen)
+{
+    const uint32_t n = ntris + nspheres;
+    if (n == 0) return 0;
+    if (!mem_ || n > cap_) {
+        snprintf(err, errLen, "BVH enqueue: no buffers for %u primitives (run a build of this size first)", n);
+        return -6;
+    }
+    if (maxLevels == 0 || maxLevels > kMaxLevels || maxWideLevels == 0 || maxWideLevels > 64) {
+        snprintf(err, errLen, "BVH enqueue: level caps must be 1-%u (binary) and 1-64 (wide)", kMaxLevels);
+        return -6;
+    }
+    const uint64_t key[] = {(uint64_t)(uintptr_t)verts, (uint64_t)(uintptr_t)idx, (uint64_t)(uintptr_t)spheres,
+                            (uint64_t)(uintptr_t)nodes, (uint64_t)(uintptr_t)tris, (uint64_t)(uintptr_t)deviceStatus,
+                            (uint64_t)(uintptr_t)mem_, ntris, nspheres, maxLevels, maxWideLevels, bigLevels_, collapse_,
+                            (uint64_t)__builtin_bit_cast(uint32_t, triCost_)};
+    const std::vector<uint64_t> k(key, key + sizeof key / sizeof key[0]);
+    if (!graphExec_ || k != graphKey_) {
+        if (graphExec_) cudaGraphExecDestroy(graphExec_);
+        graphExec_ = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            snprintf(err, errLen, "BVH enqueue: stream capture could not begin: %s",
+                     cudaGetErrorString(cudaGetLastError()));
+            return -2;
+        }
+        enqueue_launches(verts, idx, ntris, spheres, n, nodes, tris, deviceStatus, st, maxLevels, maxWideLevels);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&graphExec_, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            graphExec_ = nullptr;
+            cudaGetLastError();
+            snprintf(err, errLen, "BVH enqueue: graph capture: %s", cudaGetErrorString(e));
+            return -2;
+        }
+        graphKey_ = k;
+        ++graphCaptures_;
+    }
+    cudaEventRecord(ev0_, st);
+    cudaError_t e = cudaGraphLaunch(graphExec_, st);
+    cudaEventRecord(ev1_, st);
+    if (e != cudaSuccess) {
+        snprintf(err, errLen, "BVH enqueue: graph launch: %s", cudaGetErrorString(e));
+        return -2;
+    }
+    ++graphLaunches_;
+    return 0;
+}
+
+int Builder::enqueued_stats(cudaStream_t st, BuildStats* stats, char* err, size_t errLen)
+{
+    if (!mem_) {
+        snprintf(err, errLen, "BVH stats: nothing built");
+        return -6;
+    }
+    uint32_t h[kCntWords];
+    float sah = 0.0f;
+    cudaMemcpyAsync(h, counters_, sizeof h, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&sah, sahAccum_, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        snprintf(err, errLen, "BVH stats: %s", cudaGetErrorString(cudaGetLastError()));
+        return -2;
+    }
+    BuildStats s;
+    s.binaryNodes = h[kDevNodes];
+    s.binaryLevels = h[kDevLevels];
+    s.wideNodes = h[kDevWide];
+    s.wideDepth = h[kDevDepth];
+    s.triCount = h[kDevTris];
+    s.sahCost = sah;
+    s.childSlots = h[kCntSlots];
+    float ms = 0.0f;
+    if (graphLaunches_ && cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess) s.buildMs = ms;
+    cudaGetLastError();
+    *stats = s;
     return 0;
 }
 

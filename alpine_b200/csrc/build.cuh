@@ -20,6 +20,7 @@ struct BuildStats {
     float sahCost = 0.0f;  // SAH cost of the wide tree (node + triangle tests per unit root area)
     float buildMs = 0.0f;  // device time of the whole build
     uint32_t childSlots = 0;  // filled slots over all wide nodes
+    uint32_t bigLevels = 0;   // leading binary levels with tasks above kSmallMax references
 };
 
 // Which binary nodes fill the slots of a wide node.
@@ -44,6 +45,24 @@ public:
               WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t stream, BuildStats* stats,
               char* err, size_t errLen);
 
+    // Device-driven build: the same tree as build(), bit for bit, with every
+    // count kept in device memory, so that nothing waits on the host and the
+    // sequence of launches is fixed. It runs maxLevels binary levels and
+    // maxWideLevels collapse levels (a level past the tree's depth costs a
+    // few short launches), captured in a CUDA graph on the first call and
+    // replayed while the arguments stay the same. Needs buffers for
+    // ntris + nspheres primitives (a build() of at least that size first).
+    // A tree deeper than the caps leaves the previous tree in place and sets
+    // kErrBuildDepth in deviceStatus. Returns 0, or a negative code with a
+    // message in err.
+    int enqueue(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres, uint32_t nspheres,
+                WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t stream, uint32_t maxLevels,
+                uint32_t maxWideLevels, char* err, size_t errLen);
+    // Statistics of the last enqueue(), read from device memory (synchronous).
+    int enqueued_stats(cudaStream_t stream, BuildStats* stats, char* err, size_t errLen);
+    uint32_t graph_captures() const { return graphCaptures_; }
+    uint32_t graph_launches() const { return graphLaunches_; }
+
     // Collapse rule and the SAH cost of a triangle test relative to a
     // wide-node visit (used by kCollapseSah); applied at the next build.
     void set_collapse(uint32_t rule, float triCost)
@@ -57,6 +76,9 @@ public:
 private:
     int reserve(uint32_t ntris, char* err, size_t errLen);
     void release();
+    void enqueue_launches(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres, uint32_t n,
+                          WideNode* nodes, TriRecord* tris, uint32_t* deviceStatus, cudaStream_t stream,
+                          uint32_t maxLevels, uint32_t maxWideLevels);
 
     uint32_t cap_ = 0;
     uint32_t collapse_ = kCollapseSah;
@@ -97,6 +119,11 @@ private:
     uint32_t* scanScratch_ = nullptr;
     float* sahAccum_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    uint32_t* levelStartDev_ = nullptr;  // first binary node id of each level (device-driven build)
+    uint32_t bigLevels_ = 0;             // leading binary levels with big tasks in the last build()
+    cudaGraphExec_t graphExec_ = nullptr;  // the captured device-driven build
+    std::vector<uint64_t> graphKey_;
+    uint32_t graphCaptures_ = 0, graphLaunches_ = 0;
 };
 
 }  // namespace ag

@@ -107,6 +107,7 @@ struct alpine_gpu_ctx {
     ag::DeviceBuffer dNodes, dTris;
     uint32_t nodeCount = 0, triCount = 0;
     alpine_gpu_bvh_stats stats{};
+    uint32_t syncBuildPrims = 0;  // primitives of the last alpine_gpu_build (buffers for alpine_gpu_build_async)
 
     // device status word (DeviceError bits) and its pinned host mirror
     // (16 words: [0] status, [1..] small read-backs)

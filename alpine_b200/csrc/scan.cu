@@ -38,8 +38,31 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
     return r;
 }
 
-__global__ void k_tile_sums(const uint32_t* __restrict__ in, size_t n, uint32_t* __restrict__ sums)
+// Element count of a scan launch: n, or (device-count scans) *count * mult
+// clamped to the capacity n.
+__device__ __forceinline__ size_t scan_count(size_t n, const uint32_t* count, uint32_t mult)
 {
+    if (!count) return n;
+    const size_t c = size_t(*count) * mult;
+    return c < n ? c : n;
+}
+
+// Up to three arrays scanned by the same launches: blockIdx.y selects one.
+struct ScanArrays {
+    const uint32_t* in[3];
+    uint32_t* out[3];
+    uint32_t* total[3];
+};
+
+__global__ void k_tile_sums(ScanArrays a, size_t nCap, const uint32_t* __restrict__ count, uint32_t mult,
+                            uint32_t* __restrict__ sums, size_t sumStride)
+{
+    const size_t n = scan_count(nCap, count, mult);
+    if (size_t(blockIdx.x) * kTile >= n) {  // a tile past the count (device-count scans): its sum is 0
+        if (threadIdx.x == 0) sums[blockIdx.y * sumStride + blockIdx.x] = 0u;
+        return;
+    }
+    const uint32_t* in = a.in[blockIdx.y];
     size_t base = size_t(blockIdx.x) * kTile + size_t(threadIdx.x) * kPerThread;
     uint32_t s = 0;
 #pragma unroll
@@ -49,12 +72,21 @@ __global__ void k_tile_sums(const uint32_t* __restrict__ in, size_t n, uint32_t*
     }
     __shared__ uint32_t tot;
     block_excl_scan(s, &tot);
-    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+    if (threadIdx.x == 0) sums[blockIdx.y * sumStride + blockIdx.x] = tot;
 }
 
-__global__ void k_tile_scan(const uint32_t* in, uint32_t* out, size_t n, const uint32_t* __restrict__ offsets,
-                            uint32_t* total)
+__global__ void k_tile_scan(ScanArrays a, size_t nCap, const uint32_t* __restrict__ count, uint32_t mult,
+                            const uint32_t* __restrict__ offsets, size_t offStride)
 {
+    const size_t n = scan_count(nCap, count, mult);
+    uint32_t* total = a.total[blockIdx.y];
+    if (size_t(blockIdx.x) * kTile >= n) {  // a tile past the count: nothing to write but the total
+        if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+            *total = offsets ? offsets[blockIdx.y * offStride + blockIdx.x] : 0u;
+        return;
+    }
+    const uint32_t* in = a.in[blockIdx.y];
+    uint32_t* out = a.out[blockIdx.y];
     size_t base = size_t(blockIdx.x) * kTile + size_t(threadIdx.x) * kPerThread;
     uint32_t v[kPerThread];
     uint32_t s = 0;
@@ -65,7 +97,7 @@ __global__ void k_tile_scan(const uint32_t* in, uint32_t* out, size_t n, const u
         s += v[k];
     }
     __shared__ uint32_t tot;
-    uint32_t p = block_excl_scan(s, &tot) + (offsets ? offsets[blockIdx.x] : 0u);
+    uint32_t p = block_excl_scan(s, &tot) + (offsets ? offsets[blockIdx.y * offStride + blockIdx.x] : 0u);
 #pragma unroll
     for (int k = 0; k < kPerThread; ++k) {
         size_t i = base + k;
@@ -73,6 +105,11 @@ __global__ void k_tile_scan(const uint32_t* in, uint32_t* out, size_t n, const u
         p += v[k];
     }
     if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) *total = p;
+}
+
+ScanArrays one_array(const uint32_t* in, uint32_t* out, uint32_t* total)
+{
+    return ScanArrays{{in, nullptr, nullptr}, {out, nullptr, nullptr}, {total, nullptr, nullptr}};
 }
 }  // namespace
 
@@ -95,14 +132,55 @@ void exclusive_scan(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total
     }
     size_t nb = (n + kTile - 1) / kTile;
     if (nb == 1) {
-        k_tile_scan<<<1, kThreads, 0, stream>>>(in, out, n, nullptr, total);
+        k_tile_scan<<<1, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, nullptr, 0);
         return;
     }
     uint32_t* sums = scratch;
-    k_tile_sums<<<(unsigned)nb, kThreads, 0, stream>>>(in, n, sums);
+    k_tile_sums<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0);
     // Scan the tile sums in place (recursively), then the tiles with offsets.
     exclusive_scan(sums, sums, nb, nullptr, scratch + nb, stream);
-    k_tile_scan<<<(unsigned)nb, kThreads, 0, stream>>>(in, out, n, sums, total);
+    k_tile_scan<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0);
+}
+
+size_t scan3_scratch_words(size_t n)
+{
+    const size_t nb = (n + kTile - 1) / kTile;
+    return 3 * nb + scan_scratch_words(nb);
+}
+
+void exclusive_scan_count(int arrays, const uint32_t* const* in, uint32_t* const* out, const uint32_t* count,
+                          uint32_t mult, size_t nCap, uint32_t* const* total, uint32_t* scratch, cudaStream_t stream)
+{
+    // Launch sizes follow the capacity only; tiles past the count see zeros,
+    // so the tile sums, their scan and the totals are those of the count.
+    ScanArrays a{};
+    for (int y = 0; y < arrays; ++y) {
+        a.in[y] = in[y];
+        a.out[y] = out[y];
+        a.total[y] = total ? total[y] : nullptr;
+    }
+    if (nCap == 0) {
+        for (int y = 0; y < arrays; ++y)
+            if (a.total[y]) cudaMemsetAsync(a.total[y], 0, sizeof(uint32_t), stream);
+        return;
+    }
+    const size_t nb = (nCap + kTile - 1) / kTile;
+    const dim3 one(1, (unsigned)arrays), all((unsigned)nb, (unsigned)arrays);
+    if (nb == 1) {
+        k_tile_scan<<<one, kThreads, 0, stream>>>(a, nCap, count, mult, nullptr, 0);
+        return;
+    }
+    uint32_t* sums = scratch;  // arrays x nb tile sums
+    k_tile_sums<<<all, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb);
+    if (nb <= kTile) {  // every array's tile sums in one tile: one launch scans them all
+        ScanArrays t{};
+        for (int y = 0; y < arrays; ++y) t.in[y] = t.out[y] = sums + y * nb;
+        k_tile_scan<<<one, kThreads, 0, stream>>>(t, nb, nullptr, 1u, nullptr, 0);
+    } else {
+        for (int y = 0; y < arrays; ++y)
+            exclusive_scan(sums + y * nb, sums + y * nb, nb, nullptr, scratch + 3 * nb, stream);
+    }
+    k_tile_scan<<<all, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb);
 }
 
 }  // namespace ag

@@ -50,7 +50,8 @@ class Config(C.Structure):
 class BvhStats(C.Structure):
     _fields_ = [("triangles", C.c_uint32), ("binary_nodes", C.c_uint32), ("binary_levels", C.c_uint32),
                 ("wide_nodes", C.c_uint32), ("wide_depth", C.c_uint32), ("sah_cost", C.c_float),
-                ("build_ms", C.c_float), ("spheres", C.c_uint32), ("child_slots", C.c_uint32)]
+                ("build_ms", C.c_float), ("spheres", C.c_uint32), ("child_slots", C.c_uint32),
+                ("big_levels", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -121,6 +122,10 @@ def lib():
         L.alpine_gpu_set_morph_targets.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint32]
         L.alpine_gpu_add_animation_channel.argtypes = [vp, C.c_uint32, vp, vp, C.c_uint32]
         L.alpine_gpu_update_scene.argtypes = [vp, C.c_float, C.POINTER(BvhStats)]
+        L.alpine_gpu_build_async.argtypes = [vp, C.c_uint32, C.c_uint32]
+        L.alpine_gpu_update_scene_async.argtypes = [vp, C.c_float]
+        L.alpine_gpu_read_build_stats.argtypes = [vp, C.POINTER(BvhStats), C.POINTER(C.c_uint32),
+                                                  C.POINTER(C.c_uint32)]
         L.alpine_gpu_get_vertices.argtypes = [vp, C.c_uint32, vp, vp]
         L.alpine_gpu_trace.argtypes = [vp, vp, C.c_uint64, vp]
         L.alpine_gpu_occluded.argtypes = [vp, vp, C.c_uint64, vp]
@@ -279,6 +284,27 @@ class Context:
         self._check(self.L.alpine_gpu_build(self.h, C.byref(s)))
         self.stats = s.as_dict()
         return self.stats
+
+    def build_async(self, max_binary_levels=0, max_wide_levels=0):
+        """Rebuild enqueued on the context stream with no host wait (the same
+        tree as build(); a captured graph replayed). 0 = the last build()'s
+        depths plus a margin. Device-side errors surface at synchronize()."""
+        self._check(self.L.alpine_gpu_build_async(self.h, max_binary_levels, max_wide_levels))
+
+    def update_scene_async(self, time):
+        """update_scene's morph and build_async, enqueued without a host wait."""
+        self._check(self.L.alpine_gpu_update_scene_async(self.h, float(time)))
+
+    def read_build_stats(self) -> dict:
+        """Statistics of the last build_async (waits for the stream), with the
+        number of captures and replays of its graph."""
+        s = BvhStats()
+        cap, lau = C.c_uint32(), C.c_uint32()
+        self._check(self.L.alpine_gpu_read_build_stats(self.h, C.byref(s), C.byref(cap), C.byref(lau)))
+        d = s.as_dict()
+        d["graph_captures"] = cap.value
+        d["graph_launches"] = lau.value
+        return d
 
     def trace(self, rays: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
         r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)

@@ -380,27 +380,41 @@ def batch_benchmark(device, frames):
     """48 independent animated scenes (BASELINE cfg4 shapes; alpine_b200.batch):
     every frame morphs and rebuilds every BVH and renders every scene at its
     resolution and spp, the renders of all scenes in flight together, each a
-    replayed CUDA graph. One warm-up frame (graph capture) is not timed."""
+    replayed CUDA graph. Timed with the device-driven rebuild (one host
+    thread, no host wait within a frame) and with the host-driven rebuild
+    (one host thread, and a pool of host threads). Warm-up frames (graph
+    captures) are not timed."""
     from alpine_b200 import batch
 
     cfgs = batch.batch_configs()
     t0 = time.perf_counter()
     br = batch.BatchRenderer(cfgs, device=device, cuda_graph=True)
     setup = time.perf_counter() - t0
-    br.run(1, start=0)
-    serial = br.run(frames, start=1, threads=1)
-    r = br.run(frames, start=1 + frames)
-    r["one_host_thread"] = {k: serial[k] for k in ("seconds", "frames_per_s", "samples_per_s", "build_ms_per_frame")}
-    r["host_threads"] = br.threads
-    r["build_ms_per_frame_note"] = ("sum over scenes of each rebuild's device time; with host threads the "
-                                    "rebuilds overlap one another and the renders, so the sum exceeds the wall time")
+    keys = ("seconds", "frames_per_s", "samples_per_s", "build_ms_per_frame")
+    br.run(1, start=0, rebuild="sync")
+    serial = br.run(frames, start=1, threads=1, rebuild="sync")
+    threaded = br.run(frames, start=1 + frames, rebuild="sync")
+    br.run(1, start=1 + 2 * frames)  # warm-up of the device-driven rebuild (graph capture)
+    r = br.run(frames, start=2 + 2 * frames)
+    r["rebuild"] = "device-driven (alpine_gpu_update_scene_async, a replayed graph), one host thread, no host wait"
+    r["sync_rebuild_one_host_thread"] = {k: serial[k] for k in keys}
+    r["sync_rebuild_host_threads"] = {**{k: threaded[k] for k in keys}, "host_threads": br.threads}
+    r["build_ms_per_frame_note"] = ("sum over scenes of each rebuild's device time; the rebuilds overlap one another "
+                                    "and the renders, so the sum exceeds the wall time")
     # the rebuilds alone (morph + BVH build of all 48 scenes, no rendering), wall clock
-    rb = []
+    rb, rba = [], []
     for f in range(frames):
         t1 = time.perf_counter()
         list(br._pool.map(lambda c: c.update_scene(float(100 + f)), br.ctxs))
         rb.append(1e3 * (time.perf_counter() - t1))
-    r["rebuild_only_wall_ms_per_frame"] = statistics.mean(rb)
+        t1 = time.perf_counter()
+        for c in br.ctxs:
+            c.update_scene_async(float(200 + f))
+        for c in br.ctxs:
+            c.synchronize()
+        rba.append(1e3 * (time.perf_counter() - t1))
+    r["rebuild_only_wall_ms_per_frame"] = statistics.mean(rba)
+    r["rebuild_only_wall_ms_per_frame_sync_threads"] = statistics.mean(rb)
     r.update({"scenes": len(cfgs), "triangles": br.triangles, "setup_s": setup,
               "samples_per_frame": sum(c["width"] * c["height"] * c["spp"] for c in cfgs),
               "workload": "48 scenes, tris log-uniform 1k-500k, res 128^2-1024^2, spp 4/16/64, 1-64 quad lights, "
@@ -548,6 +562,31 @@ def traversal_split(ctx, d_closest, d_shadow, d_hits, d_occ, stream, half, reps=
             torch.cuda.synchronize()
             out[f"{name}_{kind}"] = half * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e6
     ctx.synchronize()
+    return out
+
+
+def host_link_bandwidth(h_rays, d_rays, h_hits, d_hits, stream, h2d_bytes_per_step, reps=5):
+    """GB/s of plain pinned-host copies over the host link, timed with CUDA
+    events on the stream: the ray buffer host -> device and the hit buffer
+    device -> host, each alone. `h2d_ms_per_step` is the time the link needs
+    for one step's ray bytes, the floor under the end-to-end step."""
+    import torch
+
+    src = torch.from_numpy(h_rays)
+    back = torch.from_numpy(h_hits.view(np.uint8)).view(-1)
+    dh = d_hits.view(torch.uint8).view(-1)
+    assert src.is_pinned() and back.is_pinned()
+    out = {}
+    for name, dst, s_ in (("h2d_gbs", d_rays, src), ("d2h_gbs", back, dh)):
+        dst.copy_(s_, non_blocking=True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(reps):
+            dst.copy_(s_, non_blocking=True)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        out[name] = s_.numel() * s_.element_size() * reps / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9
+    out["h2d_ms_per_step"] = h2d_bytes_per_step / (out["h2d_gbs"] * 1e9) * 1e3
     return out
 
 
@@ -722,6 +761,7 @@ def run_ours(args):
     e2e_value, e2e_ms = replicas.job_rate(2 * n, 1e3 * (time.perf_counter() - t0) / args.steps, world, dist, "cuda")
     barrier()
     e2e_value /= 1e6
+    link = host_link_bandwidth(h_closest, d_closest, h_hits, d_hits, stream, 2 * n * RAY_BYTES)
 
     peak, peak_kind = peaks()
     bytes_closest = n * (RAY_BYTES + HIT_BYTES) + nv_c * NODE_BYTES + tv_c * TRI_BYTES
@@ -775,7 +815,8 @@ def run_ours(args):
                 "parallelism": f"replicas x{world}",
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * RAY_BYTES,
-                    "d2h_bytes_per_step": n * (HIT_BYTES + 1), "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": n * (HIT_BYTES + 1), "ms_per_step": e2e_ms,
+                    "host_link": {**link, "link_bound_mrays_s": 2 * n / (link["h2d_ms_per_step"] / 1e3) / 1e6}},
             "roofline": roofline,
             "traversal_split_mrays_s": split,
             "cpu_baseline": base,

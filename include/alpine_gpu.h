@@ -78,6 +78,8 @@ typedef struct alpine_gpu_bvh_stats {
     float build_ms;      /* device time of the last build */
     uint32_t spheres;    /* analytic spheres in the BVH */
     uint32_t child_slots; /* filled child slots over all wide nodes (of 8 each) */
+    uint32_t big_levels;  /* leading binary levels with a node of more than 512 primitives (split by the
+                             block-wide kernels; the rest are split one warp per node) */
 } alpine_gpu_bvh_stats;
 
 /* Creates a context on cfg->device (replaces alpine::initialize,
@@ -147,6 +149,37 @@ ALPINE_GPU_API int alpine_gpu_get_vertices(alpine_gpu_ctx* ctx, uint32_t shape_i
  * an 8-wide quantised BVH (Accelerator::updateScene, accelerator.h:31;
  * src/accelerators/wide_bvh.cpp:175-197). stats may be NULL. */
 ALPINE_GPU_API int alpine_gpu_build(alpine_gpu_ctx* ctx, alpine_gpu_bvh_stats* stats);
+
+/* Rebuild without host round trips (no counterpart in the reference, which
+ * rebuilds synchronously in Accelerator::updateScene): the same tree as
+ * alpine_gpu_build, bit for bit, enqueued on the context stream. Every count
+ * of the level-by-level build stays in device memory, so nothing waits on
+ * the host, and the fixed sequence of launches is captured in a CUDA graph
+ * on the first call and replayed by later calls. It runs max_binary_levels
+ * binned-SAH levels and max_wide_levels collapse levels; 0 takes the last
+ * alpine_gpu_build's depths plus a margin (binary: +max(4, levels / 4); wide:
+ * +2). A tree deeper than a cap is reported by the next alpine_gpu_synchronize
+ * / render_wait as ALPINE_GPU_ERR_LIMIT ("BVH build level cap reached"): past
+ * the binary cap nothing is written and the previous tree stays in place;
+ * past the wide cap the tree is partly rewritten, so queries and renders
+ * until the next build are not to be trusted. A synchronous build recovers
+ * in both cases. Needs an alpine_gpu_build of the same scene first (it sizes
+ * the buffers; the primitive count may not change).
+ * alpine_gpu_update_scene_async: alpine_gpu_update_scene's morph followed by
+ *   this rebuild with the default caps, all on the context stream, so that a
+ *   frame's morph, rebuild and alpine_gpu_render_async are enqueued without
+ *   any host wait.
+ * alpine_gpu_read_build_stats: waits for the stream and reads the statistics
+ *   of the last alpine_gpu_build_async from device memory (build_ms: its
+ *   device time; triangles, spheres and big_levels: those of the last
+ *   alpine_gpu_build); graph_captures / graph_launches (either may be NULL)
+ *   count the captures and replays of its graph. The block-wide kernels for
+ *   nodes of more than 512 primitives run on the first big_levels + 2 levels
+ *   only; a larger node met below them is reported like a level cap. */
+ALPINE_GPU_API int alpine_gpu_build_async(alpine_gpu_ctx* ctx, uint32_t max_binary_levels, uint32_t max_wide_levels);
+ALPINE_GPU_API int alpine_gpu_update_scene_async(alpine_gpu_ctx* ctx, float time);
+ALPINE_GPU_API int alpine_gpu_read_build_stats(alpine_gpu_ctx* ctx, alpine_gpu_bvh_stats* stats,
+                                               uint32_t* graph_captures, uint32_t* graph_launches);
 
 /* How the binary SAH tree is collapsed into 8-wide nodes (the next build):
  *   COLLAPSE_SAH (0, the default): SAH-optimal. A dynamic program over the
