@@ -86,8 +86,9 @@ enum DevCounter {
     kDevTris,        // triangle records placed so far
     kDevDepth,       // collapse levels that had items
     kDevRootAreaInv, // float bits: 1 / half-area of the root box
+    kDevFailed,      // nonzero: the binary phase met a task it could not split (the build stops)
 };
-static_assert((int)kDevRootAreaInv < (int)kCntWords, "counter words");
+static_assert((int)kDevFailed < (int)kCntWords, "counter words");
 
 // Work-item count of a level kernel: the host's count, or, in a
 // device-driven build, mult times the count a previous kernel left in
@@ -603,12 +604,19 @@ AG_D void small_task(uint32_t t, const Task* __restrict__ tasks, const uint32_t*
                      uint32_t* __restrict__ refsNext, const float4* __restrict__ primLo,
                      const float4* __restrict__ primHi, const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
                      uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order, uint32_t* __restrict__ status,
-                     uint32_t* sb, bool bigHandled)
+                     uint32_t* sb, uint32_t* failed)
 {
     Task task = tasks[t];
     if (task.count > kSmallMax) {  // handled by the big-task kernels
-        // a device-driven build runs those kernels on its first levels only
-        if (!bigHandled && lane_id() == 0) atomicOr(status, kErrBuildDepth);
+        // A device-driven build runs those kernels on its first levels only
+        // (failed != null below them): the task gets no children, and the
+        // build is stopped and reported.
+        if (failed && lane_id() == 0) {
+            candFlag[2 * t] = 0;
+            candFlag[2 * t + 1] = 0;
+            atomicOr(failed, 1u);
+            atomicOr(status, kErrBuildDepth);
+        }
         return;
     }
     uint32_t lane = lane_id();
@@ -735,14 +743,14 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_small(const Task* __restri
                                                           const BinNode* __restrict__ bnodes, Cand* __restrict__ cands,
                                                           uint32_t* __restrict__ candFlag, uint32_t* __restrict__ order,
                                                           uint32_t* __restrict__ status, const uint32_t* __restrict__ dTasks,
-                                                          uint32_t bigHandled)
+                                                          uint32_t* __restrict__ failed)
 {
     __shared__ uint32_t sbins[kSmallWarps][kTaskBinWords];
     const uint32_t w = threadIdx.x >> 5;
     const uint32_t nt = level_count(dTasks, numTasks);
     for (uint32_t t = blockIdx.x * kSmallWarps + w; t < nt; t += gridDim.x * kSmallWarps)
         small_task(t, tasks, refs, refsNext, primLo, primHi, bnodes, cands, candFlag, order, status, sbins[w],
-                   bigHandled != 0u);
+                   failed);
 }
 
 // --------------------------------------------------------------------------
@@ -764,7 +772,8 @@ __global__ void k_compact(const Task* __restrict__ tasks, const Cand* __restrict
                           const uint32_t* __restrict__ bigPos, const uint32_t* __restrict__ chunkOffSparse, uint32_t nHost,
                           uint32_t nodeBaseHost, Task* __restrict__ next, BinNode* __restrict__ bnodes,
                           uint32_t* __restrict__ bigList, uint32_t* __restrict__ chunkOff, uint32_t* __restrict__ chunkTask,
-                          const uint32_t* __restrict__ dTasks, const uint32_t* __restrict__ dNodes)
+                          const uint32_t* __restrict__ dTasks, const uint32_t* __restrict__ dNodes, uint32_t capTasks,
+                          uint32_t capBig, uint32_t capChunks, uint32_t* __restrict__ status)
 {
     const uint32_t n = level_count(dTasks, nHost, 2u);
     const uint32_t nodeBase = level_count(dNodes, nodeBaseHost);
@@ -773,6 +782,13 @@ __global__ void k_compact(const Task* __restrict__ tasks, const Cand* __restrict
         Cand c = cands[j];
         uint32_t p = candPos[j];
         uint32_t node = nodeBase + p;
+        // capacities: never exceeded by a consistent build; checked so that
+        // inconsistent input cannot write past the buffers
+        if (p >= capTasks || node >= 2u * capTasks ||
+            (c.big && (bigPos[j] >= capBig || chunkOffSparse[j] + c.chunks > capChunks))) {
+            atomicOr(status, kErrBadIndex);
+            continue;
+        }
         uint32_t parent = tasks[j >> 1].node;
         if (j & 1) bnodes[parent].right = (int32_t)node;
         else bnodes[parent].left = (int32_t)node;
@@ -1147,6 +1163,7 @@ __global__ void k_dev_begin(uint32_t n, uint32_t* __restrict__ dv, uint32_t* __r
     dv[kDevChunks] = big ? (n + kChunk - 1) / kChunk : 0u;
     dv[kDevNodes] = 1u;
     dv[kDevLevels] = 0u;
+    dv[kDevFailed] = 0u;
     levelStart[0] = 0u;
 }
 
@@ -1162,8 +1179,9 @@ __global__ void k_dev_level_end(uint32_t* __restrict__ dv, uint32_t* __restrict_
     uint32_t t = dv[kCntTasks], b = dv[kCntBig], c = dv[kCntChunks];
     if (t > capTasks || b > capBig || c > capChunks || dv[kDevNodes] + t > 2u * capTasks) {
         atomicOr(status, kErrBadIndex);
-        t = b = c = 0u;
+        dv[kDevFailed] = 1u;
     }
+    if (dv[kDevFailed]) t = b = c = 0u;  // the build stops; the collapse is skipped
     dv[kDevNodes] += t;
     dv[kDevTasks] = t;
     dv[kDevBig] = b;
@@ -1178,7 +1196,7 @@ __global__ void k_dev_collapse_begin(uint32_t* __restrict__ dv, const BinNode* _
                                      uint2* __restrict__ items, float* __restrict__ sahAccum,
                                      uint32_t* __restrict__ status)
 {
-    const bool failed = dv[kDevTasks] != 0u;
+    const bool failed = dv[kDevTasks] != 0u || dv[kDevFailed] != 0u;
     if (failed) atomicOr(status, kErrBuildDepth);
     items[0] = make_uint2(0u, 0u);
     dv[kDevItems] = failed ? 0u : 1u;
@@ -1345,6 +1363,8 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     }
     if (int rc = reserve(n, err, errLen)) return rc;
     const size_t N = n;
+    const size_t maxBig = N / kSmallMax + 2;              // as reserve() sizes the buffers
+    const size_t maxChunks = N / kChunk + maxBig + 2;
     uint32_t* chunkOffSparse = chunkOffSparse_;
     Task* tasks[2] = {static_cast<Task*>(tasks_[0]), static_cast<Task*>(tasks_[1])};
     Cand* cands = static_cast<Cand*>(cands_);
@@ -1363,6 +1383,9 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
     int cur = 0;
     uint32_t level = 0;
     bigLevels_ = 0;
+    levelCounts_.clear();
+    wideCounts_.clear();
+    ++buildGeneration_;
     levelStart_.assign(1, 0u);  // binary node ids of level L: [levelStart_[L], levelStart_[L + 1])
     while (numTasks > 0) {
         if (++level > kMaxLevels) {
@@ -1370,6 +1393,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
             return -4;
         }
         Task* tk = tasks[cur];
+        levelCounts_.push_back({numTasks, numBig, totalChunks});
         if (numBig > 0) {
             bigLevels_ = level;
             k_bins_clear<<<numBig, 256, 0, st>>>(bigBins_, numBig, nullptr);
@@ -1385,7 +1409,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         }
         k_small<<<blocks_for(numTasks, kSmallWarps), 32 * kSmallWarps, 0, st>>>(
             tk, numTasks, refs_[cur], refs_[cur ^ 1], primLo_, primHi_, bnodes_, cands, candFlag_, order_,
-            deviceStatus, nullptr, 1u);
+            deviceStatus, nullptr, nullptr);
         const uint32_t nc = 2 * numTasks;
         k_cand_keys<<<blocks_for(nc, 256), 256, 0, st>>>(cands, candFlag_, nc, bigFlag_, bigChunks_, nullptr);
         exclusive_scan(candFlag_, candPos_, nc, counters_ + kCntTasks, scanScratch_, st);
@@ -1393,7 +1417,8 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         exclusive_scan(bigChunks_, chunkOffSparse, nc, counters_ + kCntChunks, scanScratch_, st);
         k_compact<<<blocks_for(nc, 256), 256, 0, st>>>(tk, cands, candFlag_, candPos_, bigPos_, chunkOffSparse, nc,
                                                        nodeCount, tasks[cur ^ 1], bnodes_, bigList_, chunkOff_,
-                                                       chunkTask_, nullptr, nullptr);
+                                                       chunkTask_, nullptr, nullptr, n, (uint32_t)maxBig,
+                                                       (uint32_t)maxChunks, deviceStatus);
         cudaMemcpyAsync(hostCounters_, counters_, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) {
             snprintf(err, errLen, "BVH build: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1441,6 +1466,7 @@ int Builder::build(const float* verts, const uint32_t* idx, uint32_t ntris, cons
         const uint2* items = reinterpret_cast<const uint2*>(items_[ci]);
         uint2* itemsNext = reinterpret_cast<uint2*>(items_[ci ^ 1]);
         int32_t* slots = reinterpret_cast<int32_t*>(slots_);
+        wideCounts_.push_back(numItems);
         k_collapse_decide<<<blocks_for(numItems, 128), 128, 0, st>>>(
             items, numItems, bnodes_, sahCollapse ? collapseChoice_ : nullptr, slots, intCount_, triCount_,
             counters_ + kCntSlots, nullptr);
@@ -1523,10 +1549,17 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
     k_root<<<blocks_for(rootChunks + 1, 256), 256, 0, st>>>(n, bounds, tasks[0], bnodes_, bigList_, chunkOff_,
                                                             chunkTask_, rootChunks);
     k_dev_begin<<<1, 1, 0, st>>>(n, dv, levelStartDev_);
-    const unsigned gBig = dev_blocks(maxBig, 1, kDevChunkBlocks);
-    const unsigned gChunks = dev_blocks(maxChunks, 1, kDevChunkBlocks);
-    const unsigned gSmall = dev_blocks(N, kSmallWarps, kDevThreadBlocks);
-    const unsigned gCand = dev_blocks(2 * N, 256, kDevThreadBlocks);
+    // Grids: the kernels loop over their work items, so any grid is correct.
+    // Each level's grid is sized for 1.5 times the count the last host-driven
+    // build had there (animated geometry keeps them close), capped by the
+    // buffers' capacities, instead of the capacity itself: far fewer idle
+    // blocks are dispatched.
+    auto expect = [](uint32_t recorded, size_t cap) {
+        return std::min(cap, size_t(recorded) + recorded / 2 + 32);
+    };
+    auto level_expect = [&](uint32_t L) {
+        return L < levelCounts_.size() ? levelCounts_[L] : (levelCounts_.empty() ? LevelCounts{1, 1, 1} : levelCounts_.back());
+    };
     // tasks above kSmallMax references occur on the top levels only: the
     // big-task kernels run on the levels where the last host-driven build had
     // them, plus a margin (k_small reports a big task met past them)
@@ -1535,6 +1568,11 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
     for (uint32_t L = 0; L < maxLevels; ++L) {
         Task* tk = tasks[cur];
         const bool bigLevel = L < bigCap;
+        const LevelCounts e = level_expect(L);
+        const unsigned gBig = dev_blocks(expect(e.big, maxBig), 1, kDevChunkBlocks);
+        const unsigned gChunks = dev_blocks(expect(e.chunks, maxChunks), 1, kDevChunkBlocks);
+        const unsigned gSmall = dev_blocks(expect(e.tasks, N), kSmallWarps, kDevThreadBlocks);
+        const unsigned gCand = dev_blocks(2 * expect(e.tasks, N), 256, kDevThreadBlocks);
         if (bigLevel) {
             k_bins_clear<<<gBig, 256, 0, st>>>(bigBins_, 0u, dv + kDevBig);
             k_bin_big<<<gChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], primLo_, primHi_, bigList_, chunkOff_,
@@ -1545,7 +1583,8 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
             {
                 const uint32_t* in[] = {chunkLeft_};
                 uint32_t* out[] = {chunkLeftOff_};
-                exclusive_scan_count(1, in, out, dv + kDevChunks, 1u, maxChunks, nullptr, scanScratch_, st);
+                exclusive_scan_count(1, in, out, dv + kDevChunks, 1u, maxChunks, nullptr, scanScratch_, st,
+                                     expect(e.chunks, maxChunks));
             }
             k_part_scatter<<<gChunks, kChunkThreads, 0, st>>>(tk, refs_[cur], refs_[cur ^ 1], primLo_, primHi_,
                                                               bigList_, chunkOff_, chunkTask_, splits, chunkLeftOff_,
@@ -1553,17 +1592,18 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
         }
         k_small<<<gSmall, 32 * kSmallWarps, 0, st>>>(tk, 0u, refs_[cur], refs_[cur ^ 1], primLo_, primHi_, bnodes_,
                                                      cands, candFlag_, order_, deviceStatus, dv + kDevTasks,
-                                                     bigLevel ? 1u : 0u);
+                                                     bigLevel ? nullptr : dv + kDevFailed);
         k_cand_keys<<<gCand, 256, 0, st>>>(cands, candFlag_, 0u, bigFlag_, bigChunks_, dv + kDevTasks);
         {
             const uint32_t* in[] = {candFlag_, bigFlag_, bigChunks_};
             uint32_t* out[] = {candPos_, bigPos_, chunkOffSparse_};
             uint32_t* tot[] = {counters_ + kCntTasks, counters_ + kCntBig, counters_ + kCntChunks};
-            exclusive_scan_count(3, in, out, dv + kDevTasks, 2u, 2 * N, tot, scanScratch_, st);
+            exclusive_scan_count(3, in, out, dv + kDevTasks, 2u, 2 * N, tot, scanScratch_, st,
+                                 2 * expect(e.tasks, N));
         }
         k_compact<<<gCand, 256, 0, st>>>(tk, cands, candFlag_, candPos_, bigPos_, chunkOffSparse_, 0u, 0u,
                                          tasks[cur ^ 1], bnodes_, bigList_, chunkOff_, chunkTask_, dv + kDevTasks,
-                                         dv + kDevNodes);
+                                         dv + kDevNodes, n, (uint32_t)maxBig, (uint32_t)maxChunks, deviceStatus);
         k_dev_level_end<<<1, 1, 0, st>>>(dv, levelStartDev_, L, n, (uint32_t)maxBig, (uint32_t)maxChunks,
                                          deviceStatus);
         cur ^= 1;
@@ -1572,14 +1612,17 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
     k_dev_collapse_begin<<<1, 1, 0, st>>>(dv, bnodes_, reinterpret_cast<uint2*>(items_[0]), sahAccum_, deviceStatus);
     const bool sahCollapse = collapse_ == kCollapseSah;
     if (sahCollapse) {
-        const unsigned gCost = dev_blocks(N, 128, kDevThreadBlocks);
-        for (uint32_t L = maxLevels; L-- > 0;)
+        for (uint32_t L = maxLevels; L-- > 0;) {
+            // the nodes of binary level L are the tasks split at level L
+            const unsigned gCost = dev_blocks(expect(level_expect(L).tasks, N), 128, kDevThreadBlocks);
             k_collapse_cost<<<gCost, 128, 0, st>>>(bnodes_, 0u, 0u, triCost_, collapseCost_, collapseChoice_,
                                                    levelStartDev_, L);
+        }
     }
-    const unsigned gItems = dev_blocks(N + 1, 128, kDevThreadBlocks);
     int ci = 0;
     for (uint32_t D = 0; D < maxWideLevels; ++D) {
+        const uint32_t we = D < wideCounts_.size() ? wideCounts_[D] : (wideCounts_.empty() ? 1u : wideCounts_.back());
+        const unsigned gItems = dev_blocks(expect(we, N + 1), 128, kDevThreadBlocks);
         const uint2* items = reinterpret_cast<const uint2*>(items_[ci]);
         uint2* itemsNext = reinterpret_cast<uint2*>(items_[ci ^ 1]);
         int32_t* slots = reinterpret_cast<int32_t*>(slots_);
@@ -1589,7 +1632,7 @@ void Builder::enqueue_launches(const float* verts, const uint32_t* idx, uint32_t
             const uint32_t* in[] = {intCount_, triCount_};
             uint32_t* out[] = {intOff_, triOff_};
             uint32_t* tot[] = {counters_ + kCntInt, counters_ + kCntTri};
-            exclusive_scan_count(2, in, out, dv + kDevItems, 1u, N + 1, tot, scanScratch_, st);
+            exclusive_scan_count(2, in, out, dv + kDevItems, 1u, N + 1, tot, scanScratch_, st, expect(we, N + 1));
         }
         k_collapse_emit<<<gItems, 128, 0, st>>>(items, 0u, bnodes_, slots, intOff_, triOff_, 0u, 0u, order_, verts, idx,
                                                 ntris, spheres, nodes, tris, itemsNext, sahAccum_, 0.0f, n + 1, n,
@@ -1616,7 +1659,8 @@ int Builder::enqueue(const float* verts, const uint32_t* idx, uint32_t ntris, co
     }
     const uint64_t key[] = {(uint64_t)(uintptr_t)verts, (uint64_t)(uintptr_t)idx, (uint64_t)(uintptr_t)spheres,
                             (uint64_t)(uintptr_t)nodes, (uint64_t)(uintptr_t)tris, (uint64_t)(uintptr_t)deviceStatus,
-                            (uint64_t)(uintptr_t)mem_, ntris, nspheres, maxLevels, maxWideLevels, bigLevels_, collapse_,
+                            (uint64_t)(uintptr_t)mem_, ntris, nspheres, maxLevels, maxWideLevels, bigLevels_,
+                            buildGeneration_, collapse_,
                             (uint64_t)__builtin_bit_cast(uint32_t, triCost_)};
     const std::vector<uint64_t> k(key, key + sizeof key / sizeof key[0]);
     if (!graphExec_ || k != graphKey_) {

@@ -121,6 +121,12 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     uint32_t* levelStartDev_ = nullptr;  // first binary node id of each level (device-driven build)
     uint32_t bigLevels_ = 0;             // leading binary levels with big tasks in the last build()
+    struct LevelCounts {
+        uint32_t tasks, big, chunks;
+    };
+    std::vector<LevelCounts> levelCounts_;  // per binary level of the last build(): sizes enqueue()'s grids
+    std::vector<uint32_t> wideCounts_;      // wide nodes per collapse level of the last build()
+    uint64_t buildGeneration_ = 0;          // build() calls so far (part of the graph key)
     cudaGraphExec_t graphExec_ = nullptr;  // the captured device-driven build
     std::vector<uint64_t> graphKey_;
     uint32_t graphCaptures_ = 0, graphLaunches_ = 0;

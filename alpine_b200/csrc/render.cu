@@ -1022,8 +1022,11 @@ int alpine_gpu_render_graph_stats(alpine_gpu_ctx* c, uint32_t* captures, uint32_
 }
 
 // Times probe renders over wave sizes and traversal block sizes and keeps the
-// fastest pair (samples per second). The probes add to the accumulation,
-// which is reset afterwards.
+// fastest pair (samples per second); for a guided render then also the
+// guide's inference kernels (warp MMA and tensor-memory tcgen05, whose
+// outputs are identical). Guided probes sample the guide from the first
+// probe on and do not train it, so the model is left as it was. The probes
+// add to the accumulation, which is reset afterwards.
 int alpine_gpu_autotune(alpine_gpu_ctx* c, uint32_t probe_spp, alpine_gpu_tuning* out)
 {
     if (!c) return ALPINE_GPU_ERR_INVALID_ARGUMENT;
@@ -1038,6 +1041,10 @@ int alpine_gpu_autotune(alpine_gpu_ctx* c, uint32_t probe_spp, alpine_gpu_tuning
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = ALPINE_GPU_OK;
+    if (c->options.guide) {
+        c->options.guide_train = 0;
+        c->options.guide_warmup_steps = 0;
+    }
     // warm-up: allocations, module loading
     c->options.max_paths_per_wave = waves[0];
     rc = alpine_gpu_render(c, 1);
@@ -1062,6 +1069,29 @@ int alpine_gpu_autotune(alpine_gpu_ctx* c, uint32_t probe_spp, alpine_gpu_tuning
                 best.trace_block = (uint32_t)b;
             }
         }
+    }
+    best.guide_kernel = (uint32_t)c->guide.kernel();
+    if (rc == ALPINE_GPU_OK && c->options.guide) {
+        c->options.max_paths_per_wave = best.max_paths_per_wave;
+        c->traceBlock = (int)best.trace_block;
+        float bestRate = -1.0f;
+        const int kernels[] = {ag::guide::Guide::kKernelWarpMma, ag::guide::Guide::kKernelTensorMemory};
+        for (int k : kernels) {
+            c->guide.set_kernel(k);
+            if ((rc = alpine_gpu_render(c, 1))) break;  // warm-up of this kernel
+            cudaEventRecord(e0, c->stream);
+            if ((rc = render_enqueue(c, probe_spp))) break;
+            cudaEventRecord(e1, c->stream);
+            if ((rc = render_wait(c))) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const float rate = ms > 0.0f ? (float)pixels * probe_spp / (ms * 1e-3f) : 0.0f;
+            if (rate > bestRate) {
+                bestRate = rate;
+                best.guide_kernel = (uint32_t)k;
+            }
+        }
+        c->guide.set_kernel((int)best.guide_kernel);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

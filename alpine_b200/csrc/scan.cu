@@ -1,6 +1,8 @@
 // Deterministic device-wide exclusive prefix sum (reduce-then-scan).
 #include "scan.cuh"
 
+#include <algorithm>
+
 namespace ag {
 namespace {
 constexpr int kThreads = 1024;
@@ -54,57 +56,63 @@ struct ScanArrays {
     uint32_t* total[3];
 };
 
+// Tiles are processed in a loop over the grid (tile = blockIdx.x, +gridDim.x,
+// ... below nb), so a grid smaller than nb tiles covers them all.
 __global__ void k_tile_sums(ScanArrays a, size_t nCap, const uint32_t* __restrict__ count, uint32_t mult,
-                            uint32_t* __restrict__ sums, size_t sumStride)
+                            uint32_t* __restrict__ sums, size_t sumStride, size_t nb)
 {
     const size_t n = scan_count(nCap, count, mult);
-    if (size_t(blockIdx.x) * kTile >= n) {  // a tile past the count (device-count scans): its sum is 0
-        if (threadIdx.x == 0) sums[blockIdx.y * sumStride + blockIdx.x] = 0u;
-        return;
-    }
     const uint32_t* in = a.in[blockIdx.y];
-    size_t base = size_t(blockIdx.x) * kTile + size_t(threadIdx.x) * kPerThread;
-    uint32_t s = 0;
+    for (size_t tile = blockIdx.x; tile < nb; tile += gridDim.x) {
+        if (tile * kTile >= n) {  // a tile past the count (device-count scans): its sum is 0
+            if (threadIdx.x == 0) sums[blockIdx.y * sumStride + tile] = 0u;
+            continue;
+        }
+        size_t base = tile * kTile + size_t(threadIdx.x) * kPerThread;
+        uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-        size_t i = base + k;
-        if (i < n) s += in[i];
+        for (int k = 0; k < kPerThread; ++k) {
+            size_t i = base + k;
+            if (i < n) s += in[i];
+        }
+        __shared__ uint32_t tot;
+        block_excl_scan(s, &tot);
+        if (threadIdx.x == 0) sums[blockIdx.y * sumStride + tile] = tot;
     }
-    __shared__ uint32_t tot;
-    block_excl_scan(s, &tot);
-    if (threadIdx.x == 0) sums[blockIdx.y * sumStride + blockIdx.x] = tot;
 }
 
 __global__ void k_tile_scan(ScanArrays a, size_t nCap, const uint32_t* __restrict__ count, uint32_t mult,
-                            const uint32_t* __restrict__ offsets, size_t offStride)
+                            const uint32_t* __restrict__ offsets, size_t offStride, size_t nb)
 {
     const size_t n = scan_count(nCap, count, mult);
-    uint32_t* total = a.total[blockIdx.y];
-    if (size_t(blockIdx.x) * kTile >= n) {  // a tile past the count: nothing to write but the total
-        if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
-            *total = offsets ? offsets[blockIdx.y * offStride + blockIdx.x] : 0u;
-        return;
-    }
     const uint32_t* in = a.in[blockIdx.y];
     uint32_t* out = a.out[blockIdx.y];
-    size_t base = size_t(blockIdx.x) * kTile + size_t(threadIdx.x) * kPerThread;
-    uint32_t v[kPerThread];
-    uint32_t s = 0;
+    uint32_t* total = a.total[blockIdx.y];
+    for (size_t tile = blockIdx.x; tile < nb; tile += gridDim.x) {
+        const uint32_t off = offsets ? offsets[blockIdx.y * offStride + tile] : 0u;
+        if (tile * kTile >= n) {  // a tile past the count: nothing to write but the total
+            if (total && tile == nb - 1 && threadIdx.x == 0) *total = off;
+            continue;
+        }
+        size_t base = tile * kTile + size_t(threadIdx.x) * kPerThread;
+        uint32_t v[kPerThread];
+        uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-        size_t i = base + k;
-        v[k] = i < n ? in[i] : 0u;
-        s += v[k];
-    }
-    __shared__ uint32_t tot;
-    uint32_t p = block_excl_scan(s, &tot) + (offsets ? offsets[blockIdx.y * offStride + blockIdx.x] : 0u);
+        for (int k = 0; k < kPerThread; ++k) {
+            size_t i = base + k;
+            v[k] = i < n ? in[i] : 0u;
+            s += v[k];
+        }
+        __shared__ uint32_t tot;
+        uint32_t p = block_excl_scan(s, &tot) + off;
 #pragma unroll
-    for (int k = 0; k < kPerThread; ++k) {
-        size_t i = base + k;
-        if (i < n) out[i] = p;
-        p += v[k];
+        for (int k = 0; k < kPerThread; ++k) {
+            size_t i = base + k;
+            if (i < n) out[i] = p;
+            p += v[k];
+        }
+        if (total && tile == nb - 1 && threadIdx.x == blockDim.x - 1) *total = p;
     }
-    if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) *total = p;
 }
 
 ScanArrays one_array(const uint32_t* in, uint32_t* out, uint32_t* total)
@@ -132,14 +140,14 @@ void exclusive_scan(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total
     }
     size_t nb = (n + kTile - 1) / kTile;
     if (nb == 1) {
-        k_tile_scan<<<1, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, nullptr, 0);
+        k_tile_scan<<<1, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, nullptr, 0, 1);
         return;
     }
     uint32_t* sums = scratch;
-    k_tile_sums<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0);
+    k_tile_sums<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0, nb);
     // Scan the tile sums in place (recursively), then the tiles with offsets.
     exclusive_scan(sums, sums, nb, nullptr, scratch + nb, stream);
-    k_tile_scan<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0);
+    k_tile_scan<<<(unsigned)nb, kThreads, 0, stream>>>(one_array(in, out, total), n, nullptr, 1u, sums, 0, nb);
 }
 
 size_t scan3_scratch_words(size_t n)
@@ -149,7 +157,8 @@ size_t scan3_scratch_words(size_t n)
 }
 
 void exclusive_scan_count(int arrays, const uint32_t* const* in, uint32_t* const* out, const uint32_t* count,
-                          uint32_t mult, size_t nCap, uint32_t* const* total, uint32_t* scratch, cudaStream_t stream)
+                          uint32_t mult, size_t nCap, uint32_t* const* total, uint32_t* scratch, cudaStream_t stream,
+                          size_t expected)
 {
     // Launch sizes follow the capacity only; tiles past the count see zeros,
     // so the tile sums, their scan and the totals are those of the count.
@@ -165,22 +174,25 @@ void exclusive_scan_count(int arrays, const uint32_t* const* in, uint32_t* const
         return;
     }
     const size_t nb = (nCap + kTile - 1) / kTile;
-    const dim3 one(1, (unsigned)arrays), all((unsigned)nb, (unsigned)arrays);
+    // blocks per array: the tiles of the expected count (a loop covers more)
+    size_t gb = expected ? (std::min(expected, nCap) + kTile - 1) / kTile : nb;
+    gb = gb < 1 ? 1 : (gb > nb ? nb : gb);
+    const dim3 one(1, (unsigned)arrays), grid((unsigned)gb, (unsigned)arrays);
     if (nb == 1) {
-        k_tile_scan<<<one, kThreads, 0, stream>>>(a, nCap, count, mult, nullptr, 0);
+        k_tile_scan<<<one, kThreads, 0, stream>>>(a, nCap, count, mult, nullptr, 0, 1);
         return;
     }
     uint32_t* sums = scratch;  // arrays x nb tile sums
-    k_tile_sums<<<all, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb);
+    k_tile_sums<<<grid, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb, nb);
     if (nb <= kTile) {  // every array's tile sums in one tile: one launch scans them all
         ScanArrays t{};
         for (int y = 0; y < arrays; ++y) t.in[y] = t.out[y] = sums + y * nb;
-        k_tile_scan<<<one, kThreads, 0, stream>>>(t, nb, nullptr, 1u, nullptr, 0);
+        k_tile_scan<<<one, kThreads, 0, stream>>>(t, nb, nullptr, 1u, nullptr, 0, 1);
     } else {
         for (int y = 0; y < arrays; ++y)
             exclusive_scan(sums + y * nb, sums + y * nb, nb, nullptr, scratch + 3 * nb, stream);
     }
-    k_tile_scan<<<all, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb);
+    k_tile_scan<<<grid, kThreads, 0, stream>>>(a, nCap, count, mult, sums, nb, nb);
 }
 
 }  // namespace ag

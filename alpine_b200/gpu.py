@@ -85,7 +85,8 @@ class GlbInfo(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("max_paths_per_wave", C.c_uint32), ("trace_block", C.c_uint32), ("samples_per_second", C.c_float)]
+    _fields_ = [("max_paths_per_wave", C.c_uint32), ("trace_block", C.c_uint32), ("samples_per_second", C.c_float),
+                ("guide_kernel", C.c_uint32)]
 
 
 MATERIAL_DTYPE = np.dtype([("kind", np.uint32), ("base_color", np.float32, 3), ("roughness", np.float32)])
@@ -512,11 +513,12 @@ class Context:
         return a.value, b.value
 
     def autotune(self, probe_spp=4):
-        """Picks the wave size and traversal block size for this scene; resets the accumulation."""
+        """Picks the wave size and traversal block size for this scene, and the
+        guide's inference kernel when guiding is on; resets the accumulation."""
         t = Tuning()
         self._check(self.L.alpine_gpu_autotune(self.h, probe_spp, C.byref(t)))
         return {"max_paths_per_wave": t.max_paths_per_wave, "trace_block": t.trace_block,
-                "samples_per_second": t.samples_per_second}
+                "samples_per_second": t.samples_per_second, "guide_kernel": t.guide_kernel}
 
     def read_accumulation(self, width, height, fp64=False):
         """(sums float[H, W, 9] = colour, albedo, normal sums; total samples)."""

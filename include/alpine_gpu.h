@@ -522,11 +522,16 @@ ALPINE_GPU_API int alpine_gpu_render_graph_stats(alpine_gpu_ctx* ctx, uint32_t* 
 /* Autotuner (no counterpart in the reference): renders probe_spp samples per
  * pixel (0 = 4) for each wave size (2^18 ... 2^22 paths) and traversal block
  * size (64, 128, 256 threads), keeps the fastest pair for this context and
- * writes it; then resets the accumulation. */
+ * writes it. When the render options enable guiding, it then times each of
+ * the guide's inference kernels (ALPINE_GPU_GUIDE_KERNEL_*, identical
+ * outputs) with training paused and keeps the faster (guide_kernel; otherwise
+ * guide_kernel reports the current one). The guide's weights and Adam steps
+ * are left as they were; the accumulation is reset. */
 typedef struct alpine_gpu_tuning {
     uint32_t max_paths_per_wave;
     uint32_t trace_block;
     float samples_per_second;
+    uint32_t guide_kernel;
 } alpine_gpu_tuning;
 ALPINE_GPU_API int alpine_gpu_autotune(alpine_gpu_ctx* ctx, uint32_t probe_spp, alpine_gpu_tuning* result);
 

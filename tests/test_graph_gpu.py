@@ -93,20 +93,40 @@ def test_autotune_keeps_the_image():
     tuned.close()
 
 
+def test_autotune_guided_picks_an_inference_kernel_and_keeps_the_model():
+    scene = scenes.room_scene(seed=6)
+    c = _ctx(scene, guide=True, guide_spp_per_wave=4, guide_steps_per_wave=4, guide_batch=4096)
+    try:
+        c.render(8)  # trains the guide a little
+        steps = c.guide_steps()[0]
+        weights = c.guide_get_weights()
+        assert steps > 0
+        t = c.autotune(probe_spp=4)
+        print("autotune (guided):", t)
+        assert t["guide_kernel"] in (gpu.GUIDE_KERNEL_WARP_MMA, gpu.GUIDE_KERNEL_TENSOR_MEMORY)
+        assert t["trace_block"] in (64, 128, 256)
+        assert c.guide_steps()[0] == steps
+        assert c.guide_get_weights().tobytes() == weights.tobytes()
+    finally:
+        c.close()
+
+
 def test_batch_host_threads_give_identical_frames():
-    """The batch renderer's per-scene host threads (concurrent morph +
-    rebuild + graph-replayed render enqueue) render exactly what one host
-    thread renders, scene by scene."""
+    """The batch renderer's ways of enqueueing a frame render the same
+    images, scene by scene: the host-driven rebuild from one host thread and
+    from per-scene host threads (concurrent morph + rebuild + graph-replayed
+    render enqueue), and the device-driven rebuild from one thread with no
+    host wait."""
     from alpine_b200 import batch
 
     cfgs = batch.batch_configs(n=6, seed=5, max_tris=20000, resolutions=(64, 96), spps=(4,))
     outs = []
-    for threads in (1, 6):
+    for threads, rebuild in ((1, "sync"), (6, "sync"), (1, "async")):
         br = batch.BatchRenderer(cfgs, threads=threads)
         try:
-            br.run(3)
+            br.run(3, rebuild=rebuild)
             outs.append([c.read_accumulation(cfg["width"], cfg["height"])[0].tobytes()
                          for c, cfg in zip(br.ctxs, cfgs)])
         finally:
             br.close()
-    assert outs[0] == outs[1]
+    assert outs[0] == outs[1] == outs[2]
