@@ -71,10 +71,15 @@ bool is_pinned(const void* p)
     return a.type == cudaMemoryTypeHost;
 }
 
-// Host-memory query: pinned buffers go through a chunked copy/compute
-// pipeline over several streams; pageable buffers are staged whole.
-// 32 chunks over 8 streams measured 860 Mrays/s end to end on the
-// 4M-ray traversal workload, against 845 (16 chunks), 816 (8) and 764 (64).
+// Host-memory query: pinned buffers go through a chunked three-stage
+// pipeline; pageable buffers are staged whole. The rays of all chunks are
+// copied in back to back on one stream, so the host link never waits for a
+// traversal; chunk k's traversal runs on one of six streams once its
+// copy has landed (an event), so the traversals of neighbouring chunks
+// overlap each other's tails; its results are copied out on the last stream
+// once it is done. Everything waits for the work already enqueued on the
+// context stream (an asynchronous rebuild, for instance). Up to 32 chunks of
+// at least 65,536 rays.
 template <bool kAny>
 int host_query(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, void* out)
 {
@@ -88,21 +93,30 @@ int host_query(alpine_gpu_ctx* c, const alpine_gpu_ray* rays, uint64_t n, void* 
     cudaError_t e = cudaSuccess;
     if (is_pinned(rays) && is_pinned(out)) {
         const uint64_t kMinChunk = 1ull << 16;
-        const uint64_t kChunks = 32;
-        uint64_t chunk = (n + kChunks - 1) / kChunks;
+        uint64_t chunk = (n + ag::kPipeChunks - 1) / ag::kPipeChunks;
         if (chunk < kMinChunk) chunk = kMinChunk;
+        cudaStream_t in = c->copyStreams[0], back = c->copyStreams[ag::kCopyStreams - 1];
+        e = cudaEventRecord(c->pipeStart, c->stream);
+        for (int i = 0; i < ag::kCopyStreams && e == cudaSuccess; ++i)
+            e = cudaStreamWaitEvent(c->copyStreams[i], c->pipeStart, 0);
         int k = 0;
         for (uint64_t s = 0; s < n && e == cudaSuccess; s += chunk, ++k) {
-            uint64_t m = n - s < chunk ? n - s : chunk;
-            cudaStream_t st = c->copyStreams[k % ag::kCopyStreams];
+            const uint64_t m = n - s < chunk ? n - s : chunk;
+            cudaStream_t st = c->copyStreams[1 + k % (ag::kCopyStreams - 2)];
             const char* src = reinterpret_cast<const char*>(rays) + s * sizeof(alpine_gpu_ray);
             char* dr = c->dRays.as<char>() + s * sizeof(alpine_gpu_ray);
             char* dout = c->dOut.as<char>() + s * outSize;
-            e = cudaMemcpyAsync(dr, src, m * sizeof(alpine_gpu_ray), cudaMemcpyHostToDevice, st);
+            e = cudaMemcpyAsync(dr, src, m * sizeof(alpine_gpu_ray), cudaMemcpyHostToDevice, in);
+            if (e == cudaSuccess) e = cudaEventRecord(c->pipeIn[k], in);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, c->pipeIn[k], 0);
             if (e != cudaSuccess) break;
             if (kAny) ag::launch_occluded(v, dr, m, reinterpret_cast<uint8_t*>(dout), c->dStatus, st);
             else ag::launch_trace(v, dr, m, dout, c->dStatus, st);
-            e = cudaMemcpyAsync(static_cast<char*>(out) + s * outSize, dout, m * outSize, cudaMemcpyDeviceToHost, st);
+            e = cudaEventRecord(c->pipeDone[k], st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(back, c->pipeDone[k], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(static_cast<char*>(out) + s * outSize, dout, m * outSize, cudaMemcpyDeviceToHost,
+                                    back);
         }
         for (int i = 0; i < ag::kCopyStreams; ++i) {
             cudaError_t e2 = cudaStreamSynchronize(c->copyStreams[i]);
@@ -159,6 +173,11 @@ int alpine_gpu_create(const alpine_gpu_config* cfg, alpine_gpu_ctx** out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     for (int i = 0; i < ag::kCopyStreams && e == cudaSuccess; ++i)
         e = cudaStreamCreateWithFlags(&c->copyStreams[i], cudaStreamNonBlocking);
+    for (int i = 0; i < ag::kPipeChunks && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&c->pipeIn[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pipeDone[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pipeStart, cudaEventDisableTiming);
     // 16 device words: [0] status bits, [4] the sample base of a replayed render
     if (e == cudaSuccess) e = cudaMalloc(&c->dStatus, 16 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost(&c->hStatus, 16 * sizeof(uint32_t));
@@ -180,6 +199,11 @@ void alpine_gpu_destroy(alpine_gpu_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& s : c->copyStreams)
         if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    for (int i = 0; i < ag::kPipeChunks; ++i) {
+        if (c->pipeIn[i]) cudaEventDestroy(c->pipeIn[i]);
+        if (c->pipeDone[i]) cudaEventDestroy(c->pipeDone[i]);
+    }
+    if (c->pipeStart) cudaEventDestroy(c->pipeStart);
     if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->dStatus) cudaFree(c->dStatus);

@@ -41,7 +41,8 @@ struct DeviceBuffer {
     T* as() const { return static_cast<T*>(ptr); }
 };
 
-constexpr int kCopyStreams = 8;  // host-query pipeline streams
+constexpr int kCopyStreams = 8;  // host-query pipeline streams: copies in, 6 traversal streams, copies out
+constexpr int kPipeChunks = 32;  // host-query pipeline: at most this many chunks per call
 
 // Human-readable description of DeviceError bits.
 inline std::string status_msg(uint32_t bits)
@@ -88,6 +89,9 @@ struct alpine_gpu_ctx {
     alpine_gpu_config cfg{};
     cudaStream_t stream = nullptr;
     cudaStream_t copyStreams[ag::kCopyStreams] = {};
+    cudaEvent_t pipeIn[ag::kPipeChunks] = {};    // host-query pipeline: chunk k's rays have landed
+    cudaEvent_t pipeDone[ag::kPipeChunks] = {};  // chunk k's traversal is done
+    cudaEvent_t pipeStart = nullptr;             // the context stream's work before a query
     std::string error;
 
     // scene geometry (host mirror + device copy)

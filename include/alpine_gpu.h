@@ -164,7 +164,10 @@ ALPINE_GPU_API int alpine_gpu_build(alpine_gpu_ctx* ctx, alpine_gpu_bvh_stats* s
  * past the wide cap the tree is partly rewritten, so queries and renders
  * until the next build are not to be trusted. A synchronous build recovers
  * in both cases. Needs an alpine_gpu_build of the same scene first (it sizes
- * the buffers; the primitive count may not change).
+ * the buffers; the primitive count may not change). Host-buffer queries
+ * (alpine_gpu_trace / _occluded) and renders of the context wait for it; a
+ * *_device query on a caller's stream must be ordered after it by the caller
+ * (alpine_gpu_synchronize, for instance).
  * alpine_gpu_update_scene_async: alpine_gpu_update_scene's morph followed by
  *   this rebuild with the default caps, all on the context stream, so that a
  *   frame's morph, rebuild and alpine_gpu_render_async are enqueued without
