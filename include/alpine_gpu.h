@@ -208,7 +208,8 @@ ALPINE_GPU_API int alpine_gpu_set_build_options(alpine_gpu_ctx* ctx, const alpin
 
 /* Closest hit for `count` rays in HOST memory (Accelerator::intersect,
  * accelerator.h:33, batched). Pinned buffers are copied in chunks overlapped
- * with the traversal; pageable buffers are staged. Blocks until done. */
+ * with the traversal; pageable buffers are staged. Waits for the work already
+ * enqueued on the context stream first, and blocks until done. */
 ALPINE_GPU_API int alpine_gpu_trace(alpine_gpu_ctx* ctx, const alpine_gpu_ray* rays, uint64_t count, alpine_gpu_hit* hits);
 
 /* Any hit in [tmin, tmax) for rays in HOST memory (Accelerator::intersectAny,
