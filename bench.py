@@ -80,6 +80,8 @@ def parse_args():
                    help="profiling run: one build, one warm-up and one timed step, no e2e / CPU baseline")
     p.add_argument("--collapse-sweep", action="store_true",
                    help="traversal workload under each wide-BVH collapse rule and SAH triangle cost (one JSON line each)")
+    p.add_argument("--e2e-breakdown", action="store_true",
+                   help="where the end-to-end traversal step's time goes (device, chunked, copies, each host call)")
     return p.parse_args()
 
 
@@ -945,10 +947,86 @@ def collapse_sweep(device=0):
     ctx.close()
 
 
+def e2e_breakdown(device=0, reps=8):
+    """Where the end-to-end traversal step's time goes, all on one GPU: the
+    device-resident step as two full launches and as 32 chunks on 6
+    streams, the same with the step's host->device copies running beside
+    it, the copies alone, and each host-buffer call of the library (ms per
+    step; wall time around synchronised repetitions)."""
+    import torch
+
+    from alpine_b200 import gpu, scenes
+
+    verts, idx, closest, shadow = scenes.traversal_workload()
+    n = closest.shape[0]
+    ctx = gpu.Context(device)
+    ctx.add_mesh(verts, idx)
+    ctx.build()
+    dc, ds = torch.from_numpy(closest).cuda(), torch.from_numpy(shadow).cuda()
+    dc2, ds2 = torch.empty_like(dc), torch.empty_like(ds)
+    dh = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    do = torch.empty(n, dtype=torch.uint8, device="cuda")
+    hc, hs = torch.from_numpy(closest).pin_memory(), torch.from_numpy(shadow).pin_memory()
+    hh = torch.empty((n, 4), dtype=torch.int32).pin_memory()
+    ho = torch.empty(n, dtype=torch.uint8).pin_memory()
+    streams = [torch.cuda.Stream() for _ in range(6)]
+    main, cp, back = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.set_stream(main)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return 1e3 * (time.perf_counter() - t0) / reps
+
+    def full():
+        ctx.trace_device(dc.data_ptr(), n, dh.data_ptr(), main.cuda_stream)
+        ctx.occluded_device(ds.data_ptr(), n, do.data_ptr(), main.cuda_stream)
+
+    def chunked(k_total=32):
+        c = n // k_total
+        for k in range(k_total):
+            ctx.trace_device(dc.data_ptr() + k * c * RAY_BYTES, c, dh.data_ptr() + k * c * HIT_BYTES,
+                             streams[k % 6].cuda_stream)
+        for k in range(k_total):
+            ctx.occluded_device(ds.data_ptr() + k * c * RAY_BYTES, c, do.data_ptr() + k * c,
+                                streams[k % 6].cuda_stream)
+
+    def copies():
+        with torch.cuda.stream(cp):
+            dc2.copy_(hc, non_blocking=True)
+            ds2.copy_(hs, non_blocking=True)
+        with torch.cuda.stream(back):
+            hh.copy_(dh, non_blocking=True)
+            ho.copy_(do, non_blocking=True)
+
+    def beside():
+        with torch.cuda.stream(cp):
+            dc2.copy_(hc, non_blocking=True)
+            ds2.copy_(hs, non_blocking=True)
+        full()
+
+    h_hits = torch.empty(n * HIT_BYTES, dtype=torch.uint8).pin_memory().numpy().view(gpu.HIT_DTYPE)
+    h_occ = ho.numpy()
+    out = {"device_full_ms": timed(full), "device_chunked32_ms": timed(chunked),
+           "device_full_with_h2d_beside_ms": timed(beside), "copies_only_ms": timed(copies),
+           "e2e_ms": timed(lambda: (ctx.trace(hc.numpy(), h_hits), ctx.occluded(hs.numpy(), h_occ))),
+           "e2e_trace_ms": timed(lambda: ctx.trace(hc.numpy(), h_hits)),
+           "e2e_occluded_ms": timed(lambda: ctx.occluded(hs.numpy(), h_occ))}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse_args()
     if args.collapse_sweep:
         collapse_sweep()
+        return
+    if args.e2e_breakdown:
+        e2e_breakdown()
         return
     if args.impl == "reference":
         run_reference(args)
