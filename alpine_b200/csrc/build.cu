@@ -1698,8 +1698,8 @@ int Builder::enqueue(const float* verts, const uint32_t* idx, uint32_t ntris, co
 
 int Builder::enqueued_stats(cudaStream_t st, BuildStats* stats, char* err, size_t errLen)
 {
-    if (!mem_) {
-        snprintf(err, errLen, "BVH stats: nothing built");
+    if (!mem_ || graphLaunches_ == 0) {
+        snprintf(err, errLen, "BVH stats: no device-driven build yet");
         return -6;
     }
     uint32_t h[kCntWords];

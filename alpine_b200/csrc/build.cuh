@@ -50,9 +50,12 @@ public:
     // sequence of launches is fixed. It runs maxLevels binary levels and
     // maxWideLevels collapse levels (a level past the tree's depth costs a
     // few short launches), captured in a CUDA graph on the first call and
-    // replayed while the arguments stay the same. Needs buffers for
-    // ntris + nspheres primitives (a build() of at least that size first).
-    // A tree deeper than the caps leaves the previous tree in place and sets
+    // replayed until the arguments change or a build() records new per-level
+    // counts (they size the grids and pick the levels that run the big-task
+    // kernels). Needs buffers for ntris + nspheres primitives (a build() of
+    // at least that size first). A tree deeper than the binary cap, or a big
+    // task below the big-task levels, leaves the previous tree in place; one
+    // deeper than the wide cap leaves it partly rewritten; all three set
     // kErrBuildDepth in deviceStatus. Returns 0, or a negative code with a
     // message in err.
     int enqueue(const float* verts, const uint32_t* idx, uint32_t ntris, const float4* spheres, uint32_t nspheres,
