@@ -21,7 +21,8 @@ on the host cores.
 per light sampler (uniform, power, light BVH).
 
 `batch` (rank 0, one GPU): frames/s and samples/s of 48 animated scenes
-rendered together (morph + BVH rebuild + render per scene per frame).
+rendered together (morph + BVH rebuild + render per scene per frame), with
+the device-driven rebuild and with the host-driven one.
 
 `guiding` (rank 0, one GPU): time to relMSE 0.01, guided vs plain MIS, on the
 glossy interior (20 x 4 x 12 m room, 2.0M triangles, 70% GGX with roughness
@@ -34,6 +35,8 @@ removed from every relMSE (see guiding_benchmark). relMSE = mean over pixels and
 interpolated in log-log between the curve points that bracket it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --collapse-sweep   # traversal under each wide-BVH collapse rule
+    python bench.py --e2e-breakdown    # where the end-to-end step's time goes
 Multi-GPU: one process per GPU under torchrun; each rank is an independent
 replica of the workload (weak scaling), timed as the max over ranks.
 """
